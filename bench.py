@@ -1,0 +1,368 @@
+#!/usr/bin/env python
+"""Benchmark of the Kennett reflectivity + discrete-wavenumber gather path on B200.
+
+Workload (one "step"): the 21-layer gather model (water + 19 elastic layers + half-space,
+seed 1), 2047 damped frequencies omega_k = k 2pi/64 + i pi/64 (T = 64 s, nw = 2048),
+8192 slownesses p_j = j 1.2/8192, 100 offsets 0.5..50 km, Ricker 10 Hz, free surface:
+(1) the full R(omega, p) grid, (2) the Bessel-weighted slowness sum U(r, omega),
+(3) the 100 traces of 4096 samples.  Metric: (omega, p, interface) updates per second
+(2047 x 8192 x 20 = 3.35e8 per step).
+
+Device timing: CUDA events around each step on the launching stream, L2 flushed between
+steps (256 MB write, outside the events), max over ranks.  ``e2e``: the same step through
+the public ``compute_gather_gpu(..., return_reflectivity=True)`` call with host inputs and
+pinned host outputs (R grid + traces copied back every step), wall clock.
+
+``--impl reference`` times the CPU oracle (NumPy/SciPy restatement of the reference,
+organised like the reference's process-pool gather) on a bounded slowness sample with all
+host cores; rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = dict(workload="kennett_gather_21layer", layers=21, n_sub=20, seed=1, T=64.0,
+                nw=2048, n_omega=2047, n_p=8192, p_max=1.2, n_offsets=100, dr=0.5,
+                free_surface=True, source="ricker_10Hz", dtype="complex128")
+FLOPS_PER_UPDATE = 340.0          # reference-literal count per (omega, p, interface) update
+FLOPS_PER_PAIR_FS = 25.0          # free-surface epilogue per (omega, p)
+FLOPS_PER_BESSEL_TERM = 6.0       # per (r, omega, p), J0 evaluation counted separately
+L2_FLUSH_BYTES = 256 << 20
+NOMINAL_FP64_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=0, help="slownesses in the CPU sample")
+    ap.add_argument("--profile", action="store_true",
+                    help="device steps only (no e2e, CPU baseline or peak probe): for ncu")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().strip().splitlines() if r]
+        os.unlink(self.f.name)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+                for n, v in zip(names, r[5:9]):
+                    if v.strip() == "Active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def fp64_peak(torch, dev):
+    """Measured FP64 CUDA-core peak (DFMA probe, best of 5) in TFLOP/s."""
+    from seismicinversion_b200 import _lib
+
+    h = _lib.lib()
+    blocks, iters = 148 * 8, 20000
+    out = torch.empty(blocks * 256, dtype=torch.float64, device=dev)
+    st = torch.cuda.current_stream(dev)
+    best = 0.0
+    for _ in range(6):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        _lib.check(h.kr_bench_fp64_fma(blocks, iters, out.data_ptr(), st.cuda_stream), "probe")
+        b.record(st)
+        b.synchronize()
+        best = max(best, h.kr_bench_fp64_fma_flops(blocks, iters) / (a.elapsed_time(b) * 1e-3))
+    return best / 1e12
+
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    from seismicinversion_b200 import device as D
+    from seismicinversion_b200.earth_models import random_layered_model
+    from seismicinversion_b200.kennett_gather_gpu import compute_gather_gpu
+    from seismicinversion_b200.source import ricker_10hz
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    dev = D.require_cuda(torch.device("cuda", local))
+    torch.cuda.set_device(dev)
+    W = WORKLOAD
+    model = random_layered_model(W["n_sub"], seed=W["seed"])
+    T, nw, npp, pmax = W["T"], W["nw"], W["n_p"], W["p_max"]
+    offsets = np.arange(1, W["n_offsets"] + 1) * W["dr"]
+    gamma = np.pi / T
+    dw = 2 * np.pi / T
+    om = np.arange(1, nw) * dw
+    nwm = nw - 1
+    dp = pmax / npp
+    p = np.arange(1, npp + 1) * dp
+    taper = 0.5 * (1 + np.cos(np.pi * p / pmax))
+    S = ricker_10hz(om, nw * dw)
+    time_axis = np.arange(2 * nw) * (T / (2 * nw))
+    decay = np.exp(-gamma * time_axis)
+
+    cpu_base = None
+    if rank == 0 and world == 1 and not (args.no_cpu_baseline or args.profile):
+        from oracle.cpu_baseline import GatherBaseline  # checker / baseline leg only
+
+        cores = len(os.sched_getaffinity(0))
+        n_sample = args.cpu_sample or max(256, 4 * cores)
+        cpu_base = GatherBaseline(model, offsets, T, nw, npp, pmax, True, n_sample)
+
+    tab = D.layer_table(model, dev)
+    p_t = torch.as_tensor(p, device=dev)
+    pw_t = torch.as_tensor(taper * p, device=dev)
+    w_t = torch.as_tensor(om + 1j * gamma, device=dev)
+    wr_t = torch.as_tensor(om, device=dev)
+    off_t = torch.as_tensor(offsets, device=dev)
+    S_t = torch.as_tensor(S, device=dev)
+    dec_t = torch.as_tensor(decay, device=dev)
+    R = torch.empty((npp, nwm), dtype=torch.complex128, device=dev)
+    U = torch.empty((len(offsets), nwm), dtype=torch.complex128, device=dev)
+    G = torch.empty((len(offsets), 2 * nw), dtype=torch.float64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    st = torch.cuda.current_stream(dev)
+
+    def step(ev):
+        ev[0].record(st)
+        D.reflectivity(tab, p_t, w_t, True, out=R)
+        ev[1].record(st)
+        D.bessel_sum(R, p_t, pw_t, dp, wr_t, off_t, out=U)
+        ev[2].record(st)
+        D.traces(U, nw, S=S_t, decay=dec_t, out=G)
+        ev[3].record(st)
+
+    def events():
+        return [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        step(events())
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = Clocks(local)
+    clk.start()
+    evs = []
+    for _ in range(args.steps):
+        flush.zero_()
+        ev = events()
+        step(ev)
+        evs.append(ev)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    stage = np.array([[e[i].elapsed_time(e[i + 1]) for i in range(3)] for e in evs])  # ms
+    per_step = stage.sum(axis=1)
+    ms = float(per_step.mean())
+    st_ms = stage.mean(axis=0)
+    if dist:
+        t = torch.tensor([ms, *st_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, st_ms = float(t[0]), t[1:].cpu().numpy()
+
+    upd = nwm * npp * (W["layers"] - 1)
+    value = world * upd / (ms * 1e-3)
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"profile_run": True, "ms_per_step": ms, "stage_ms": list(map(float, st_ms))}))
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    # end to end through the public API: host model in, host R grid + traces out
+    e2e_times = []
+    for k in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, _, gh, Rh = compute_gather_gpu(model, offsets, T=T, nw=nw, np_slow=npp, p_max=pmax,
+                                          source_func=ricker_10hz, free_surface=True,
+                                          return_reflectivity=True)
+        if k >= args.warmup:
+            e2e_times.append(time.perf_counter() - t0)
+    e2e_s = statistics.mean(e2e_times)
+    if dist:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t[0])
+    h2d = tab.numel() * 8 + p.nbytes + (om.nbytes * 2) + offsets.nbytes + S.nbytes + decay.nbytes
+    h2d += (taper * p).nbytes + om.nbytes
+    d2h = R.numel() * 16 + G.numel() * 8
+
+    peak = fp64_peak(torch, dev)
+    fwd_flops = FLOPS_PER_UPDATE * upd + FLOPS_PER_PAIR_FS * nwm * npp
+    bes_terms = len(offsets) * nwm * npp
+    kernels = {
+        "reflectivity": {"ms": float(st_ms[0]), "alg_tflops": fwd_flops / (st_ms[0] * 1e-3) / 1e12,
+                         "updates_per_s": upd / (st_ms[0] * 1e-3)},
+        "bessel_sum": {"ms": float(st_ms[1]), "j0_terms_per_s": bes_terms / (st_ms[1] * 1e-3),
+                       "alg_tflops": FLOPS_PER_BESSEL_TERM * bes_terms / (st_ms[1] * 1e-3) / 1e12},
+        "traces": {"ms": float(st_ms[2])},
+    }
+    dom = "reflectivity" if st_ms[0] >= st_ms[1] else "bessel_sum"
+    traffic = None
+    tf = ROOT / "profiles" / "ncu_traffic.json"
+    if tf.exists():
+        try:
+            traffic = json.loads(tf.read_text()).get(dom)
+        except Exception:
+            traffic = None
+    ach = kernels[dom]["alg_tflops"]
+    roofline = {"bound": "fp64", "kernel": dom, "achieved": round(ach, 3), "peak": round(peak, 3),
+                "unit": "TFLOP/s", "frac": round(ach / peak, 4), "traffic": traffic,
+                "peak_source": "measured: DFMA probe (kr_bench_fp64_fma), best of 6",
+                "nominal_peak": round(NOMINAL_FP64_TFLOPS, 2)}
+
+    cpu = None
+    accuracy = None
+    if cpu_base is not None:
+        samples = []
+        for i in range(2):  # one warm start, one timed
+            dt, Rc, _ = cpu_base.step()
+            samples.append(dt)
+        Rg = R[torch.as_tensor(cpu_base.rows, device=dev)].cpu().numpy()
+        accuracy = float(np.max(np.abs(Rg - Rc)) / np.max(np.abs(Rc)))
+        cpu = {"value": cpu_base.updates() / samples[-1], "unit": "updates/s",
+               "cores": cpu_base.workers, "kind": "port",
+               "sample": f"{len(cpu_base.p)} of {npp} slownesses (evenly spaced), all 2047 "
+                         f"frequencies and 100 offsets: reflectivity + J0 slowness sum, "
+                         f"multiprocessing pool of {cpu_base.workers} (oracle port)",
+               "seconds": samples[-1]}
+        cpu_base.close()
+
+    if rank == 0:
+        line = {
+            "metric": "(omega,p,interface) reflectivity updates/s, 21-layer gather workload (R grid + J0 gather + traces)",
+            "value": value, "unit": "updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 (complex128)",
+            "data": "synthetic (seeded random 21-layer model; no dataset exists)",
+            "config": {**W, "parallelism": f"replicas{world}" if world > 1 else "single",
+                       "l2": "flushed between steps (256 MB write) and R grid 268 MB > L2"},
+            "roofline": roofline, "cpu_baseline": cpu,
+            "e2e": {"value": world * upd / e2e_s, "unit": "updates/s", "seconds_per_step": e2e_s,
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": 5 * args.steps, "clocks": clocks, "kernels": kernels,
+            "max_rel_err_vs_oracle_sample": accuracy,
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from oracle.cpu_baseline import GatherBaseline
+    from seismicinversion_b200.earth_models import random_layered_model
+
+    W = WORKLOAD
+    model = random_layered_model(W["n_sub"], seed=W["seed"])
+    offsets = np.arange(1, W["n_offsets"] + 1) * W["dr"]
+    cores = len(os.sched_getaffinity(0))
+    n_sample = args.cpu_sample or max(256, 4 * cores)
+    b = GatherBaseline(model, offsets, W["T"], W["nw"], W["n_p"], W["p_max"], True, n_sample)
+    for _ in range(args.warmup):
+        b.step()
+    ts = [b.step()[0] for _ in range(args.steps)]
+    b.close()
+    sec = statistics.mean(ts)
+    v = b.updates() / sec
+    samp = (f"{len(b.p)} of {W['n_p']} slownesses per step (evenly spaced), all 2047 damped "
+            f"frequencies and 100 offsets: reflectivity + J0 slowness sum")
+    line = {
+        "impl": "reference",
+        "metric": "(omega,p,interface) reflectivity updates/s, 21-layer gather workload (R grid + J0 gather + traces)",
+        "value": v, "unit": "updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sec * 1e3 * W["n_p"] / len(b.p),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (complex128)", "data": "synthetic (seeded random 21-layer model)",
+        "config": {**W, "parallelism": "host process pool"},
+        "cpu_baseline": {"value": v, "unit": "updates/s", "cores": b.workers, "kind": "port",
+                         "sample": samp},
+        "e2e": {"value": v, "unit": "updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": "CPU oracle port (NumPy/SciPy restatement of the reference, pinned to its golden "
+                "vectors) run like the reference's multiprocessing gather; the Python reference "
+                "itself cannot travel to the GPU host",
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,122 @@
+/*
+ * kennett_b200 -- C ABI of the B200 (sm_100a) Kennett reflectivity library.
+ *
+ * Plain pointers and sizes only.  Unless stated otherwise every array argument is a DEVICE
+ * pointer owned by the caller; the library never allocates or frees caller memory, and
+ * every call is enqueued on the caller's CUDA stream (`stream`, a cudaStream_t passed as
+ * void*, NULL = legacy default stream).  Calls return a kr_status; no C++ exception
+ * crosses this boundary.  Complex numbers are interleaved (re, im) float64 pairs.
+ *
+ * Layer table: float64 [6][n_layers], rows alpha (P velocity), beta (S velocity, 0 in the
+ * acoustic ocean = layer 0), rho, thickness (+inf or >= 1e30 marks the half-space), Q_alpha,
+ * Q_beta.  Layer 0 is the ocean, layer n_layers-1 the half-space.
+ *
+ * Each entry point names the reference (tmnestor/SeismicInversion) interface it replaces.
+ */
+#ifndef KENNETT_B200_H
+#define KENNETT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t kr_status;
+
+#define KR_OK 0
+#define KR_ERR_INVALID_ARGUMENT 1   /* null pointer, negative size, unknown flag bits      */
+#define KR_ERR_INVALID_MODEL 2      /* layer table violates the model rules                 */
+#define KR_ERR_CUDA 3               /* a CUDA runtime call or kernel launch failed          */
+#define KR_ERR_CUFFT 4              /* a cuFFT call failed                                  */
+#define KR_ERR_WORKSPACE 5          /* workspace pointer NULL or smaller than required      */
+#define KR_ERR_TOO_LARGE 6          /* a size exceeds a documented limit                    */
+
+#define KR_MAX_LAYERS 256           /* layers per model (shared-memory prologue)            */
+
+/* flags */
+#define KR_FREE_SURFACE 0x1u        /* include free-surface multiples (R_fs = -1)           */
+
+/* Human-readable name of a status code (static string). */
+const char* kr_status_string(kr_status status);
+
+/* Detail of the most recent error in the calling thread ("" if none). */
+const char* kr_last_error(void);
+
+/* Library version as major*10000 + minor*100 + patch. */
+int32_t kr_version(void);
+
+/*
+ * Validates a HOST layer table against the rules of LayerModel
+ * (Kennett_Reflectivity/layer_model.py:105-123: alpha > 0, beta >= 0, rho > 0) plus what the
+ * kernels need: 2 <= n_layers <= KR_MAX_LAYERS, beta[0] == 0 (acoustic ocean,
+ * scattering_matrices.py:164-296), finite positive Q, non-negative thickness.
+ * Returns KR_OK or KR_ERR_INVALID_MODEL (detail in kr_last_error()).
+ */
+kr_status kr_validate_layers(const double* layers_host, int32_t n_layers);
+
+/*
+ * Plane-wave PP reflectivity R(p, omega) for one model on a slowness x frequency grid.
+ * Replaces kennett_reflectivity (Kennett_Reflectivity/kennett_reflectivity.py:73-78) and
+ * kennett_reflectivity_batch (Kennett_Reflectivity/kennett_reflectivity_gpu.py:88-93).
+ *   layers : device float64 [6][n_layers]
+ *   p      : device float64 [n_p] horizontal slownesses (s/km)
+ *   omega  : device complex [n_w] angular frequencies (imaginary part = damping, may be 0)
+ *   R      : device complex [n_p][n_w] output
+ *   flags  : KR_FREE_SURFACE or 0
+ * One fused kernel: slownesses, interface coefficients (shared memory, per slowness) and
+ * the Kennett sweep, one thread per (omega, p).  n_p == 0 or n_w == 0 is a no-op.
+ */
+kr_status kr_reflectivity(const double* layers, int32_t n_layers, const double* p, int32_t n_p,
+                          const double* omega, int32_t n_w, uint32_t flags, double* R,
+                          void* stream);
+
+/* Bytes of device workspace kr_bessel_sum needs for these sizes. */
+size_t kr_bessel_sum_workspace_bytes(int32_t n_p, int32_t n_w, int32_t n_r);
+
+/*
+ * Discrete-wavenumber (Bessel) summation over slowness, float64 throughout:
+ *   U[r][w] = sum_j R[j][w] * ((pw[j] * omega[w]) * dp) * J0((omega[w] * p[j]) * offsets[r])
+ * Replaces _gpu_bessel_summation (Kennett_Reflectivity/kennett_gather_gpu.py:56-166) and the
+ * per-slowness accumulation of compute_gather (Kennett_Reflectivity/kennett_gather.py:112-124,
+ * :274-288).  pw[j] is the per-slowness weight taper_j * p_j.
+ *   R       : device complex [n_p][n_w]
+ *   p, pw   : device float64 [n_p]
+ *   omega   : device float64 [n_w] (real parts of the frequencies)
+ *   offsets : device float64 [n_r] (km)
+ *   U       : device complex [n_r][n_w] output
+ *   workspace: device, >= kr_bessel_sum_workspace_bytes(n_p, n_w, n_r) bytes
+ * The slowness sum is split over blocks and reduced in a fixed order (deterministic).
+ */
+kr_status kr_bessel_sum(const double* R, const double* p, const double* pw, int32_t n_p,
+                        double dp, const double* omega, int32_t n_w, const double* offsets,
+                        int32_t n_r, double* U, void* workspace, size_t workspace_bytes,
+                        void* stream);
+
+/* Bytes of device workspace kr_traces needs. */
+size_t kr_traces_workspace_bytes(int32_t n_r, int32_t nw);
+
+/*
+ * Time traces from spectra at omega_k = k*dw, k = 1..nw-1 (nt = 2*nw samples):
+ *   traces[r][t] = Re( FFT_forward( H[r] ) )[t] * decay[t]
+ * where H[r] is the Hermitian length-nt spectrum with H[k] = U[r][k-1]*S[k-1] (k = 1..nw-1),
+ * H[0] = H[nw] = 0, H[nt-k] = conj(H[k]).  Replaces the trace assembly of compute_seismogram
+ * (Kennett_Reflectivity/kennett_seismogram.py:124-144) and the per-trace FFT loops of
+ * compute_gather / compute_gather_gpu (kennett_gather.py:294-303, kennett_gather_gpu.py:272-282).
+ * Uses a cuFFT complex-to-real transform.
+ *   U      : device complex [n_r][nw-1]
+ *   S      : device complex [nw-1] source spectrum, or NULL for S = 1
+ *   decay  : device float64 [2*nw] (e.g. exp(-gamma t)), or NULL for 1
+ *   traces : device float64 [n_r][2*nw] output
+ *   workspace: device, >= kr_traces_workspace_bytes(n_r, nw) bytes
+ */
+kr_status kr_traces(const double* U, const double* S, int32_t n_r, int32_t nw,
+                    const double* decay, double* traces, void* workspace,
+                    size_t workspace_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KENNETT_B200_H */

@@ -1,0 +1,94 @@
+"""ctypes binding of the C ABI in ``include/kennett_b200.h`` (``libkennett_b200.so``).
+
+The library is the only compute path: if it is missing, or no CUDA device is visible,
+every entry point raises.  There is no CPU fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+
+__all__ = ["lib", "check", "KennettError", "LIB_PATH", "exported_symbols"]
+
+LIB_PATH = Path(__file__).resolve().with_name("libkennett_b200.so")
+
+KR_OK = 0
+KR_ERR_INVALID_ARGUMENT = 1
+KR_ERR_INVALID_MODEL = 2
+KR_ERR_CUDA = 3
+KR_ERR_CUFFT = 4
+KR_ERR_WORKSPACE = 5
+KR_ERR_TOO_LARGE = 6
+
+KR_FREE_SURFACE = 0x1
+
+_c_double_p = ctypes.c_void_p  # device pointers travel as integers
+_size_t = ctypes.c_size_t
+_i32 = ctypes.c_int32
+_u32 = ctypes.c_uint32
+_vp = ctypes.c_void_p
+
+# name -> (restype, argtypes); kept in step with include/*.h
+_SIGNATURES = {
+    "kr_status_string": (ctypes.c_char_p, [_i32]),
+    "kr_last_error": (ctypes.c_char_p, []),
+    "kr_version": (_i32, []),
+    "kr_validate_layers": (_i32, [_vp, _i32]),
+    "kr_reflectivity": (_i32, [_vp, _i32, _vp, _i32, _vp, _i32, _u32, _vp, _vp]),
+    "kr_bessel_sum_workspace_bytes": (_size_t, [_i32, _i32, _i32]),
+    "kr_bessel_sum": (_i32, [_vp, _vp, _vp, _i32, ctypes.c_double, _vp, _i32, _vp, _i32, _vp,
+                             _vp, _size_t, _vp]),
+    "kr_traces_workspace_bytes": (_size_t, [_i32, _i32]),
+    "kr_traces": (_i32, [_vp, _vp, _i32, _i32, _vp, _vp, _vp, _size_t, _vp]),
+    # include/kennett_b200_bench.h
+    "kr_bench_fp64_fma": (_i32, [_i32, _i32, _vp, _vp]),
+    "kr_bench_fp64_fma_flops": (ctypes.c_double, [_i32, _i32]),
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+class KennettError(RuntimeError):
+    """A device-side failure reported by the library (CUDA or cuFFT)."""
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGNATURES)
+
+
+def lib() -> ctypes.CDLL:
+    """Load ``libkennett_b200.so`` once; raise ImportError if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not LIB_PATH.exists():
+                raise ImportError(
+                    f"{LIB_PATH.name} is not built; run `python -m seismicinversion_b200.build` "
+                    "(the CUDA library is the only compute path)"
+                )
+            h = ctypes.CDLL(str(LIB_PATH))
+            for name, (res, args) in _SIGNATURES.items():
+                fn = getattr(h, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = h
+    return _lib
+
+
+def check(status: int, what: str) -> None:
+    """Map a kr_status to the reference's exception style (ValueError for bad input)."""
+    if status == KR_OK:
+        return
+    h = lib()
+    name = h.kr_status_string(status).decode()
+    detail = h.kr_last_error().decode()
+    msg = f"{what}: {name}" + (f" ({detail})" if detail else "")
+    if status in (KR_ERR_INVALID_ARGUMENT, KR_ERR_INVALID_MODEL, KR_ERR_TOO_LARGE,
+                  KR_ERR_WORKSPACE):
+        raise ValueError(msg)
+    raise KennettError(msg)

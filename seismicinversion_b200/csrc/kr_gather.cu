@@ -1,0 +1,255 @@
+// Discrete-wavenumber gather: Bessel-weighted slowness sum and the omega -> t step.
+//
+// kr_bessel_sum: one thread per (offset, omega) and slowness slice.  Blocks are
+// 32 frequencies x 8 offsets; the slowness range is split over grid.z so the grid fills
+// the 148 SMs several times over; each slice writes its partial U to the workspace and a
+// second kernel adds the slices in a fixed order (bit-reproducible).  J0 is evaluated on
+// the fly in registers (FP64); R[p][omega] loads are coalesced along omega and shared by the
+// block's 8 offsets through L1.
+//
+// kr_traces: builds the half spectrum conj(U S) (DC and Nyquist zero) and runs a batched
+// cuFFT Z2D: for a Hermitian spectrum H, the forward DFT the reference applies
+// (np.fft.fft) equals the inverse real transform of conj(H).  The decay exp(-gamma t) is
+// applied by a last elementwise kernel.
+#include <cufft.h>
+
+#include <mutex>
+#include <vector>
+
+#include "kr_internal.cuh"
+
+namespace kr {
+
+constexpr int kBsW = 32;  // frequencies per block
+constexpr int kBsR = 8;   // offsets per block
+
+__global__ void __launch_bounds__(kBsW * kBsR)
+bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ p,
+                      const double* __restrict__ pw, int n_p, double dp,
+                      const double* __restrict__ omega, int n_w,
+                      const double* __restrict__ offsets, int n_r, int p_per_slice,
+                      double2* __restrict__ partial) {
+  const int iw = blockIdx.x * kBsW + threadIdx.x;
+  const int ir = blockIdx.y * kBsR + threadIdx.y;
+  const int j_begin = blockIdx.z * p_per_slice;
+  const int j_end = min(n_p, j_begin + p_per_slice);
+  if (iw >= n_w || ir >= n_r) return;
+  const double om = omega[iw];
+  const double r = offsets[ir];
+  double ax = 0.0, ay = 0.0;
+  for (int j = j_begin; j < j_end; ++j) {
+    const double pj = __ldg(p + j);
+    const double wgt = (__ldg(pw + j) * om) * dp;
+    const double2 rv = __ldg(R + (size_t)j * n_w + iw);
+    const double jv = j0((om * pj) * r);
+    ax = fma(jv, rv.x * wgt, ax);
+    ay = fma(jv, rv.y * wgt, ay);
+  }
+  partial[((size_t)blockIdx.z * n_r + ir) * n_w + iw] = make_double2(ax, ay);
+}
+
+__global__ void reduce_slices_kernel(const double2* __restrict__ partial, int n_slices,
+                                     size_t n_elem, double2* __restrict__ U) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n_elem;
+       i += (size_t)gridDim.x * blockDim.x) {
+    double x = 0.0, y = 0.0;
+    for (int s = 0; s < n_slices; ++s) {
+      double2 v = partial[(size_t)s * n_elem + i];
+      x += v.x;
+      y += v.y;
+    }
+    U[i] = make_double2(x, y);
+  }
+}
+
+struct BesselPlan {
+  int n_slices;
+  int p_per_slice;
+  size_t partial_bytes;
+};
+
+static BesselPlan bessel_plan(int n_p, int n_w, int n_r) {
+  BesselPlan b;
+  const long long tiles = (long long)((n_w + kBsW - 1) / kBsW) * ((n_r + kBsR - 1) / kBsR);
+  // About 32 blocks of 256 threads per SM in total (4 waves at 8 resident blocks per SM),
+  // but no slice shorter than 64 slownesses.
+  const long long target = 148LL * 32;
+  long long s = (target + tiles - 1) / (tiles > 0 ? tiles : 1);
+  long long smax = (n_p + 63) / 64;
+  if (s > smax) s = smax;
+  if (s < 1) s = 1;
+  if (s > 65535) s = 65535;
+  b.p_per_slice = (int)((n_p + s - 1) / s);
+  b.n_slices = (int)((n_p + b.p_per_slice - 1) / b.p_per_slice);
+  if (b.n_slices < 1) b.n_slices = 1;
+  b.partial_bytes = (size_t)b.n_slices * n_r * n_w * sizeof(double2);
+  return b;
+}
+
+// ---------------------------------------------------------------------------------------
+// Traces
+// ---------------------------------------------------------------------------------------
+__global__ void half_spectrum_kernel(const double2* __restrict__ U, const double2* __restrict__ S,
+                                     int n_r, int nw, double2* __restrict__ X) {
+  const int nh = nw + 1;
+  const size_t n = (size_t)n_r * nh;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(i / nh);
+    const int k = (int)(i % nh);
+    double2 v = make_double2(0.0, 0.0);
+    if (k >= 1 && k <= nw - 1) {
+      double2 u = U[(size_t)r * (nw - 1) + (k - 1)];
+      if (S) {
+        double2 s = S[k - 1];
+        cd y = mk(u.x, u.y) * mk(s.x, s.y);
+        u = make_double2(y.x, y.y);
+      }
+      v = make_double2(u.x, -u.y);
+    }
+    X[i] = v;
+  }
+}
+
+__global__ void decay_kernel(double* __restrict__ tr, const double* __restrict__ decay, int n_r,
+                             int nt) {
+  const size_t n = (size_t)n_r * nt;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    tr[i] *= decay[i % nt];
+}
+
+struct FftEntry {
+  int device;
+  int nt;
+  int batch;
+  cufftHandle plan;
+  size_t work;
+};
+
+static std::mutex g_fft_mu;
+static std::vector<FftEntry> g_fft;
+
+// Returns a cached C2R plan (auto work-area allocation off) for nt-point transforms.
+static kr_status get_fft_plan(int nt, int batch, FftEntry** out) {
+  int dev = 0;
+  cudaError_t ce = cudaGetDevice(&dev);
+  if (ce != cudaSuccess) {
+    set_last_error("kr_traces: cudaGetDevice", ce);
+    return KR_ERR_CUDA;
+  }
+  for (auto& e : g_fft)
+    if (e.device == dev && e.nt == nt && e.batch == batch) {
+      *out = &e;
+      return KR_OK;
+    }
+  FftEntry e;
+  e.device = dev;
+  e.nt = nt;
+  e.batch = batch;
+  if (cufftCreate(&e.plan) != CUFFT_SUCCESS) return KR_ERR_CUFFT;
+  if (cufftSetAutoAllocation(e.plan, 0) != CUFFT_SUCCESS) {
+    cufftDestroy(e.plan);
+    return KR_ERR_CUFFT;
+  }
+  int n = nt;
+  if (cufftMakePlanMany(e.plan, 1, &n, nullptr, 1, nt / 2 + 1, nullptr, 1, nt, CUFFT_Z2D, batch,
+                        &e.work) != CUFFT_SUCCESS) {
+    cufftDestroy(e.plan);
+    set_last_error_msg("kr_traces: cufftMakePlanMany failed");
+    return KR_ERR_CUFFT;
+  }
+  g_fft.push_back(e);
+  *out = &g_fft.back();
+  return KR_OK;
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace kr
+
+using namespace kr;
+
+extern "C" size_t kr_bessel_sum_workspace_bytes(int32_t n_p, int32_t n_w, int32_t n_r) {
+  if (n_p <= 0 || n_w <= 0 || n_r <= 0) return 0;
+  return bessel_plan(n_p, n_w, n_r).partial_bytes;
+}
+
+extern "C" kr_status kr_bessel_sum(const double* R, const double* p, const double* pw,
+                                   int32_t n_p, double dp, const double* omega, int32_t n_w,
+                                   const double* offsets, int32_t n_r, double* U,
+                                   void* workspace, size_t workspace_bytes, void* stream) {
+  if (n_p < 0 || n_w < 0 || n_r < 0) return KR_ERR_INVALID_ARGUMENT;
+  if (n_w == 0 || n_r == 0) return KR_OK;
+  if (!U || !omega || !offsets) return KR_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (n_p == 0) {
+    cudaError_t e = cudaMemsetAsync(U, 0, (size_t)n_r * n_w * sizeof(double2), st);
+    if (e != cudaSuccess) set_last_error("kr_bessel_sum: memset", e);
+    return cuda_status(e);
+  }
+  if (!R || !p || !pw) return KR_ERR_INVALID_ARGUMENT;
+  if ((n_r + kBsR - 1) / kBsR > 65535) return KR_ERR_TOO_LARGE;
+  BesselPlan b = bessel_plan(n_p, n_w, n_r);
+  if (!workspace || workspace_bytes < b.partial_bytes) return KR_ERR_WORKSPACE;
+  double2* partial = reinterpret_cast<double2*>(workspace);
+  dim3 grid((n_w + kBsW - 1) / kBsW, (n_r + kBsR - 1) / kBsR, b.n_slices);
+  bessel_partial_kernel<<<grid, dim3(kBsW, kBsR), 0, st>>>(
+      reinterpret_cast<const double2*>(R), p, pw, n_p, dp, omega, n_w, offsets, n_r,
+      b.p_per_slice, partial);
+  kr_status s = check_launch("kr_bessel_sum: partial");
+  if (s != KR_OK) return s;
+  const size_t n_elem = (size_t)n_r * n_w;
+  int blocks = (int)((n_elem + 255) / 256);
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  reduce_slices_kernel<<<blocks, 256, 0, st>>>(partial, b.n_slices, n_elem,
+                                               reinterpret_cast<double2*>(U));
+  return check_launch("kr_bessel_sum: reduce");
+}
+
+extern "C" size_t kr_traces_workspace_bytes(int32_t n_r, int32_t nw) {
+  if (n_r <= 0 || nw <= 1) return 0;
+  std::lock_guard<std::mutex> lk(g_fft_mu);
+  FftEntry* e = nullptr;
+  if (get_fft_plan(2 * nw, n_r, &e) != KR_OK) return 0;
+  return align256((size_t)n_r * (nw + 1) * sizeof(double2)) + e->work;
+}
+
+extern "C" kr_status kr_traces(const double* U, const double* S, int32_t n_r, int32_t nw,
+                               const double* decay, double* traces, void* workspace,
+                               size_t workspace_bytes, void* stream) {
+  if (n_r < 0 || nw < 0) return KR_ERR_INVALID_ARGUMENT;
+  if (n_r == 0) return KR_OK;
+  if (nw < 2) return KR_ERR_INVALID_ARGUMENT;
+  if (!U || !traces) return KR_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  std::lock_guard<std::mutex> lk(g_fft_mu);
+  FftEntry* e = nullptr;
+  kr_status s = get_fft_plan(2 * nw, n_r, &e);
+  if (s != KR_OK) return s;
+  const size_t xbytes = align256((size_t)n_r * (nw + 1) * sizeof(double2));
+  if (!workspace || workspace_bytes < xbytes + e->work) return KR_ERR_WORKSPACE;
+  double2* X = reinterpret_cast<double2*>(workspace);
+  void* work = static_cast<unsigned char*>(workspace) + xbytes;
+  const size_t nx = (size_t)n_r * (nw + 1);
+  int blocks = (int)((nx + 255) / 256);
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  half_spectrum_kernel<<<blocks, 256, 0, st>>>(reinterpret_cast<const double2*>(U),
+                                               reinterpret_cast<const double2*>(S), n_r, nw, X);
+  s = check_launch("kr_traces: half spectrum");
+  if (s != KR_OK) return s;
+  if (cufftSetStream(e->plan, st) != CUFFT_SUCCESS) return KR_ERR_CUFFT;
+  if (e->work && cufftSetWorkArea(e->plan, work) != CUFFT_SUCCESS) return KR_ERR_CUFFT;
+  if (cufftExecZ2D(e->plan, reinterpret_cast<cufftDoubleComplex*>(X), traces) != CUFFT_SUCCESS) {
+    set_last_error_msg("kr_traces: cufftExecZ2D failed");
+    return KR_ERR_CUFFT;
+  }
+  if (decay) {
+    const size_t nt_all = (size_t)n_r * 2 * nw;
+    int b2 = (int)((nt_all + 255) / 256);
+    if (b2 > 148 * 16) b2 = 148 * 16;
+    decay_kernel<<<b2, 256, 0, st>>>(traces, decay, n_r, 2 * nw);
+    return check_launch("kr_traces: decay");
+  }
+  return KR_OK;
+}

@@ -1,0 +1,66 @@
+// Internal declarations shared by the library's translation units (not part of the C-ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../../include/kennett_b200.h"
+#include "kr_math.cuh"
+
+namespace kr {
+
+constexpr int kMaxLayers = KR_MAX_LAYERS;
+
+// Dynamic shared memory of the per-slowness prologue: layer terms + interface coefficients.
+inline size_t prologue_smem_bytes(int n_layers) {
+  return sizeof(LayerP) * (size_t)n_layers + sizeof(Iface) * (size_t)(n_layers - 1);
+}
+
+inline kr_status cuda_status(cudaError_t e) { return e == cudaSuccess ? KR_OK : KR_ERR_CUDA; }
+
+// Remembers the last CUDA error string for kr_last_error().
+void set_last_error(const char* where, cudaError_t e);
+void set_last_error_msg(const char* msg);
+
+inline kr_status check_launch(const char* where) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_last_error(where, e);
+    return KR_ERR_CUDA;
+  }
+  return KR_OK;
+}
+
+// Computes the layer terms and interface coefficients of one slowness into shared memory
+// (threads of the block cooperate: one layer / one interface per thread).  Ends with a
+// block barrier.
+__device__ __forceinline__ void block_prologue(const double* __restrict__ tab, int n_layers,
+                                               double p, LayerP* s_layer, Iface* s_iface) {
+  for (int l = threadIdx.x; l < n_layers; l += blockDim.x) s_layer[l] = layer_terms(tab, n_layers, l, p);
+  __syncthreads();
+  for (int i = threadIdx.x; i < n_layers - 1; i += blockDim.x)
+    s_iface[i] = interface_coeffs(p, i, s_layer[i], s_layer[i + 1]);
+  __syncthreads();
+}
+
+// The full upward sweep for one (omega, p) with coefficients in shared memory.
+// Returns RRd_PP below the ocean.
+__device__ __forceinline__ cd sweep(cd w, int n_layers, const LayerP* s_layer,
+                                    const Iface* s_iface) {
+  const int I = n_layers - 1;
+  // Bottom interface: RRd below it is 0, so RRd = Rd.
+  Sym r;
+  r.a = s_iface[I - 1].rd11;
+  r.b = s_iface[I - 1].rd12;
+  r.c = s_iface[I - 1].rd22;
+  for (int i = I - 2; i >= 0; --i) {
+    const LayerP& lb = s_layer[i + 1];
+    cd ea = cexp_(w * lb.ca);
+    cd eb = cexp_(w * lb.cb);
+    r = kennett_step(r, ea, eb, s_iface[i]);
+  }
+  return r.a;
+}
+
+}  // namespace kr

@@ -1,0 +1,287 @@
+// Complex FP64 arithmetic, layer slownesses, interface scattering coefficients and the
+// Kennett 2x2 addition step, shared by every kernel of the library.
+//
+// Physics follows tmnestor/SeismicInversion, Kennett_Reflectivity/:
+//   complex slowness      layer_model.py:15-45
+//   vertical slowness     layer_model.py:48-74   (Im(eta) > 0 branch, flip when Im <= 0)
+//   solid-solid coeffs    scattering_matrices.py:42-161
+//   ocean-bottom coeffs   scattering_matrices.py:164-296
+//   Kennett step          kennett_reflectivity.py:227-256
+//   PP + free surface     kennett_reflectivity.py:264-326
+//
+// Storage choices (ours): Rd and Ru are symmetric and Tu = Td^T (reciprocity,
+// scattering_matrices.py:150), so an interface is 10 complex numbers; the cumulative
+// reflection matrix RRd stays symmetric through the recursion (MT (I - Ru MT)^-1 is symmetric
+// when MT and Ru are), so the sweep carries 3 complex numbers instead of 4.  The 2x2 inverse
+// is one reciprocal of the determinant times the adjugate.
+#pragma once
+
+#include <math.h>
+
+#ifdef __CUDACC__
+#define KR_HD __host__ __device__ __forceinline__
+#else
+#define KR_HD inline
+#endif
+
+namespace kr {
+
+struct cd {
+  double x, y;
+};
+
+KR_HD cd mk(double x, double y) { cd r; r.x = x; r.y = y; return r; }
+KR_HD cd operator+(cd a, cd b) { return mk(a.x + b.x, a.y + b.y); }
+KR_HD cd operator-(cd a, cd b) { return mk(a.x - b.x, a.y - b.y); }
+KR_HD cd operator-(cd a) { return mk(-a.x, -a.y); }
+KR_HD cd operator*(cd a, cd b) {
+  return mk(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+KR_HD cd operator*(double s, cd a) { return mk(s * a.x, s * a.y); }
+KR_HD cd operator*(cd a, double s) { return mk(s * a.x, s * a.y); }
+KR_HD cd operator+(cd a, double s) { return mk(a.x + s, a.y); }
+KR_HD cd operator+(double s, cd a) { return mk(a.x + s, a.y); }
+KR_HD cd operator-(double s, cd a) { return mk(s - a.x, -a.y); }
+KR_HD cd operator-(cd a, double s) { return mk(a.x - s, a.y); }
+KR_HD cd conj(cd a) { return mk(a.x, -a.y); }
+KR_HD double abs2(cd a) { return fma(a.x, a.x, a.y * a.y); }
+
+// 1/z via the conjugate over |z|^2, with a power-of-two prescale so that |z|^2 neither
+// overflows nor underflows for the magnitudes met here (down to ~1e-150).
+KR_HD cd recip(cd z) {
+  double m = fmax(fabs(z.x), fabs(z.y));
+  double s = 1.0;
+  if (m > 1e150) s = 1e-150; else if (m < 1e-150 && m > 0.0) s = 1e150;
+  double zx = z.x * s, zy = z.y * s;
+  double inv = 1.0 / fma(zx, zx, zy * zy);
+  return mk(zx * inv * s, -zy * inv * s);
+}
+KR_HD cd operator/(cd a, cd b) { return a * recip(b); }
+KR_HD cd operator/(cd a, double s) { return mk(a.x / s, a.y / s); }
+
+// Principal square root, branch cut on the negative real axis, sqrt(conj z) = conj sqrt z
+// (C99 csqrt semantics, the convention NumPy and torch use).
+KR_HD cd csqrt(cd z) {
+  if (z.x == 0.0 && z.y == 0.0) return mk(0.0, z.y);
+  double t = sqrt(0.5 * (fabs(z.x) + hypot(z.x, z.y)));
+  if (z.x >= 0.0) return mk(t, z.y / (2.0 * t));
+  return mk(fabs(z.y) / (2.0 * t), copysign(t, z.y));
+}
+
+KR_HD cd cexp_(cd z) {
+  double e = exp(z.x);
+  double s, c;
+#ifdef __CUDA_ARCH__
+  sincos(z.y, &s, &c);
+#else
+  s = sin(z.y);
+  c = cos(z.y);
+#endif
+  return mk(e * c, e * s);
+}
+
+// Complex slowness of a layer with velocity v and quality factor Q.
+KR_HD cd complex_slowness(double v, double Q) {
+  double q2 = 2.0 * Q;
+  double q2sq = q2 * q2;
+  double den = (1.0 + q2sq) * v;
+  return mk(q2sq / den, q2 / den);
+}
+
+// eta = sqrt((s + p)(s - p)) with Im(eta) > 0.
+KR_HD cd vertical_slowness(cd s, double p) {
+  cd t = (s + p) * (s - p);
+  cd e = csqrt(t);
+  if (e.y <= 0.0) e = -e;
+  return e;
+}
+
+KR_HD bool is_half_space(double h) { return !(h < 1e30); }  // +inf, >= 1e30 (and NaN)
+
+// ---------------------------------------------------------------------------------------
+// Per-layer quantities for one slowness.
+// ---------------------------------------------------------------------------------------
+struct LayerP {
+  cd eta;    // vertical P slowness
+  cd neta;   // vertical S slowness (0 in the ocean)
+  cd betac;  // complex S velocity 1/s_s (0 where beta = 0)
+  cd ca;     // i * eta * h   (0 for the half-space: phase factor exactly 1)
+  cd cb;     // i * neta * h
+  double rho;
+};
+
+// Layer table layout (device or host): 6 rows of n_layers doubles:
+// alpha, beta, rho, thickness, Q_alpha, Q_beta.
+KR_HD LayerP layer_terms(const double* tab, int n_layers, int l, double p) {
+  const double alpha = tab[l];
+  const double beta = tab[n_layers + l];
+  const double rho = tab[2 * n_layers + l];
+  const double h = tab[3 * n_layers + l];
+  const double qa = tab[4 * n_layers + l];
+  const double qb = tab[5 * n_layers + l];
+  LayerP o;
+  cd sp = complex_slowness(alpha, qa);
+  cd ss = beta > 0.0 ? complex_slowness(beta, qb) : mk(0.0, 0.0);
+  o.betac = (ss.x != 0.0 || ss.y != 0.0) ? recip(ss) : mk(0.0, 0.0);
+  o.eta = vertical_slowness(sp, p);
+  o.neta = (l == 0) ? mk(0.0, 0.0) : vertical_slowness(ss, p);
+  if (is_half_space(h)) {
+    o.ca = mk(0.0, 0.0);
+    o.cb = mk(0.0, 0.0);
+  } else {
+    o.ca = mk(-o.eta.y * h, o.eta.x * h);
+    o.cb = mk(-o.neta.y * h, o.neta.x * h);
+  }
+  o.rho = rho;
+  return o;
+}
+
+// ---------------------------------------------------------------------------------------
+// Interface coefficients: Rd, Ru symmetric (3 entries each), Td full (Tu = Td^T).
+// ---------------------------------------------------------------------------------------
+template <class T>
+struct IfaceT {
+  T rd11, rd12, rd22;
+  T ru11, ru12, ru22;
+  T td11, td12, td21, td22;
+};
+typedef IfaceT<cd> Iface;
+
+// Scalar-generic so that the same code yields values (T = cd) and forward-mode tangents
+// (T = a dual number).  rho enters as T so its tangent can be seeded.
+template <class T>
+KR_HD void solid_solid(double p, T eta1, T neta1, T rho1, T beta1, T eta2, T neta2, T rho2,
+                       T beta2, IfaceT<T>& o) {
+  T rteta1 = csqrt(eta1), rteta2 = csqrt(eta2);
+  T rtneta1 = csqrt(neta1), rtneta2 = csqrt(neta2);
+  T rtrho1 = csqrt(rho1), rtrho2 = csqrt(rho2);
+  T rtza1 = rteta1 * rtrho1, rtza2 = rteta2 * rtrho2;
+  T rtzb1 = rtneta1 * rtrho1, rtzb2 = rtneta2 * rtrho2;
+  const double psq = p * p;
+  T dmu = rho2 * beta2 * beta2 - rho1 * beta1 * beta1;
+  T d = 2.0 * dmu;
+  T psqd = psq * d;
+  T a = (rho2 - rho1) - psqd;
+  T b = rho2 - psqd;
+  T c = rho1 + psqd;
+  T E = b * eta1 + c * eta2;
+  T F = b * neta1 + c * neta2;
+  T G = a - d * eta1 * neta2;
+  T H = a - d * eta2 * neta1;
+  T det = E * F + G * H * psq;
+  T idet = recip(det);
+  E = E * idet;
+  F = F * idet;
+  G = G * idet;
+  H = H * idet;
+  T Qv = (b * eta1 - c * eta2) * F;
+  T Rv = (a + d * eta1 * neta2) * H * psq;
+  T Sv = (a * b + c * d * eta2 * neta2) * p * idet;
+  T Tv = (b * neta1 - c * neta2) * E;
+  T Uv = (a + d * eta2 * neta1) * G * psq;
+  T Vv = (a * c + b * d * eta1 * neta1) * p * idet;
+  const cd m2i = mk(0.0, -2.0);
+  o.rd11 = Qv - Rv;
+  o.rd12 = m2i * (rteta1 * rtneta1 * Sv);
+  o.rd22 = Tv - Uv;
+  o.ru11 = -(Qv + Uv);
+  o.ru12 = m2i * (rteta2 * rtneta2 * Vv);
+  o.ru22 = -(Tv + Rv);
+  o.td11 = 2.0 * (rtza1 * rtza2 * F);
+  o.td12 = m2i * (rtzb1 * rtza2 * G * p);
+  o.td21 = m2i * (rtza1 * rtzb2 * H * p);
+  o.td22 = 2.0 * (rtzb1 * rtzb2 * E);
+}
+
+template <class T>
+KR_HD void ocean_bottom(double p, T eta1, T rho1, T eta2, T neta2, T rho2, T beta2,
+                        IfaceT<T>& o) {
+  T rteta1 = csqrt(eta1), rteta2 = csqrt(eta2), rtneta2 = csqrt(neta2);
+  T rtrho1 = csqrt(rho1), rtrho2 = csqrt(rho2);
+  T rtza1 = rtrho1 * rteta1, rtza2 = rtrho2 * rteta2, rtzb2 = rtrho2 * rtneta2;
+  const double psq = p * p;
+  T d = 2.0 * (rho2 * beta2 * beta2);
+  T psqd = psq * d;
+  T a = (rho2 - rho1) - psqd;
+  T b = rho2 - psqd;
+  T c = rho1 + psqd;
+  T E = b * eta1 + c * eta2;
+  T F = b;
+  T G = a - d * eta1 * neta2;
+  T H = -(d * eta2);
+  T det = E * F + G * H * psq;
+  T idet = recip(det);
+  E = E * idet;
+  F = F * idet;
+  G = G * idet;
+  H = H * idet;
+  T T1 = (b * eta1 - c * eta2) * F;
+  T T2 = (a + d * eta1 * neta2) * H * psq;
+  T T4 = b * E;
+  T T5 = d * eta2 * G * psq;
+  T T6 = b * d * eta1 * p * idet;
+  const cd mi = mk(0.0, -1.0);
+  T zero = 0.0 * rho1;
+  o.rd11 = T1 - T2;
+  o.rd12 = zero;
+  o.rd22 = zero;
+  o.ru11 = -(T1 + T5);
+  o.ru12 = mi * (2.0 * (rteta2 * rtneta2 * T6));
+  o.ru22 = -(T2 + T4);
+  o.td11 = 2.0 * (rtza1 * rtza2 * F);
+  o.td12 = zero;
+  o.td21 = mi * (2.0 * (rtza1 * rtzb2 * H * p));
+  o.td22 = zero;
+}
+
+KR_HD cd to_c(double r) { return mk(r, 0.0); }
+
+// Coefficients of interface `iface` (between layers iface and iface+1) from layer terms.
+KR_HD Iface interface_coeffs(double p, int iface, const LayerP& up, const LayerP& lo) {
+  Iface o;
+  if (iface == 0)
+    ocean_bottom<cd>(p, up.eta, to_c(up.rho), lo.eta, lo.neta, to_c(lo.rho), lo.betac, o);
+  else
+    solid_solid<cd>(p, up.eta, up.neta, to_c(up.rho), up.betac, lo.eta, lo.neta, to_c(lo.rho),
+                    lo.betac, o);
+  return o;
+}
+
+// ---------------------------------------------------------------------------------------
+// One Kennett addition step: RRd <- Rd + Tu MT (I - Ru MT)^-1 Td with MT = E RRd E,
+// E = diag(ea, eb) of the layer below the interface.  RRd = [[a, b], [b, c]].
+// ---------------------------------------------------------------------------------------
+struct Sym {
+  cd a, b, c;
+};
+
+KR_HD Sym kennett_step(const Sym& r, cd ea, cd eb, const Iface& f) {
+  cd eaea = ea * ea, ebeb = eb * eb, eaeb = ea * eb;
+  cd m11 = eaea * r.a, m12 = eaeb * r.b, m22 = ebeb * r.c;
+  cd n11 = 1.0 - (f.ru11 * m11 + f.ru12 * m12);
+  cd n12 = -(f.ru11 * m12 + f.ru12 * m22);
+  cd n21 = -(f.ru12 * m11 + f.ru22 * m12);
+  cd n22 = 1.0 - (f.ru12 * m12 + f.ru22 * m22);
+  cd idet = recip(n11 * n22 - n12 * n21);
+  cd x11 = (m11 * n22 - m12 * n21) * idet;
+  cd x12 = (m12 * n11 - m11 * n12) * idet;
+  cd x22 = (m22 * n11 - m12 * n12) * idet;
+  cd y11 = x11 * f.td11 + x12 * f.td21;
+  cd y12 = x11 * f.td12 + x12 * f.td22;
+  cd y21 = x12 * f.td11 + x22 * f.td21;
+  cd y22 = x12 * f.td12 + x22 * f.td22;
+  Sym o;
+  o.a = f.rd11 + (f.td11 * y11 + f.td21 * y21);
+  o.b = f.rd12 + (f.td11 * y12 + f.td21 * y22);
+  o.c = f.rd22 + (f.td12 * y12 + f.td22 * y22);
+  return o;
+}
+
+// PP reflectivity at the surface from RRd_PP below the ocean and the ocean phase e0.
+KR_HD cd pp_surface(cd rpp, cd e0, bool free_surface) {
+  cd y = (e0 * e0) * rpp;
+  if (!free_surface) return y;
+  return y * recip(1.0 + y);
+}
+
+}  // namespace kr

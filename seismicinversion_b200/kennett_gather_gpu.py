@@ -1,0 +1,93 @@
+"""Drop-in for ``Kennett_Reflectivity.kennett_gather_gpu`` (``kennett_gather_gpu.py:56-284``).
+
+All three stages run on the GPU in float64 with device-resident intermediates:
+(1) the reflectivity grid at damped frequencies (fused Kennett kernel), (2) the
+Bessel-weighted slowness sum with J0 evaluated in the kernel, (3) the Hermitian
+omega -> t transform (cuFFT) with the exp(-gamma t) compensation.  The reference does (1) in
+NumPy on the CPU, J0 in SciPy on the CPU and the sum in float32 on the device.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import device as _dev
+from .earth_models import default_ocean_crust_model
+from .layer_model import LayerModel
+from .source import ricker_spectrum
+
+__all__ = ["compute_gather_gpu", "default_ocean_crust_model", "gather_device"]
+
+
+def _gpu_bessel_summation(R, p_samples, omega_real, offsets, dp, device=None):
+    """U[r, w] = dp sum_j R[j, w] taper_j p_j w J0(w p_j r) (``kennett_gather_gpu.py:56-166``).
+
+    The Hann taper uses p_max = p_samples[-1] as in the reference.  float64 throughout.
+    """
+    on_device = isinstance(R, torch.Tensor) and R.is_cuda
+    dev = _dev.require_cuda(R.device if on_device else device)
+    p = np.asarray(p_samples.cpu() if isinstance(p_samples, torch.Tensor) else p_samples,
+                   dtype=np.float64)
+    taper = 0.5 * (1.0 + np.cos(np.pi * p / p[-1]))
+    Rt = R if on_device else torch.as_tensor(np.ascontiguousarray(R, dtype=np.complex128), device=dev)
+    U = _dev.bessel_sum(Rt, p, taper * p, dp, omega_real, offsets)
+    return U if on_device else U.cpu().numpy()
+
+
+def gather_device(model: LayerModel, offsets, T=64.0, nw=2048, np_slow=4096, p_max=1.2,
+                  gamma=None, source_func=None, free_surface=False, device=None):
+    """Device-resident gather: returns ``(time, R, U, gather)`` with R, U, gather CUDA tensors."""
+    dev = _dev.require_cuda(device)
+    if gamma is None:
+        gamma = np.pi / T
+    dw = 2.0 * np.pi / T
+    omega = np.arange(1, nw, dtype=np.float64) * dw
+    wmax = nw * dw
+    S = ricker_spectrum(omega, wmax) if source_func is None else source_func(omega, wmax)
+    nt = 2 * nw
+    time = np.arange(nt, dtype=np.float64) * (T / float(nt))
+    dp = p_max / np_slow
+    p = np.arange(1, np_slow + 1, dtype=np.float64) * dp
+    taper = 0.5 * (1.0 + np.cos(np.pi * p / p_max))
+    tab = _dev.layer_table(model, dev)
+    R = _dev.reflectivity(tab, p, omega + 1j * gamma, free_surface)
+    U = _dev.bessel_sum(R, p, taper * p, dp, omega, offsets)
+    g = _dev.traces(U, nw, S=np.asarray(S, dtype=np.complex128), decay=np.exp(-gamma * time))
+    return time, R, U, g
+
+
+_PINNED: dict = {}
+
+
+def _pinned(shape, dtype) -> torch.Tensor:
+    """A reusable page-locked host buffer (fast, async-capable device-to-host copies)."""
+    key = (tuple(shape), dtype)
+    buf = _PINNED.get(key)
+    if buf is None:
+        buf = torch.empty(shape, dtype=dtype, pin_memory=True)
+        _PINNED[key] = buf
+    return buf
+
+
+def compute_gather_gpu(model: LayerModel, offsets, T: float = 64.0, nw: int = 2048,
+                       np_slow: int = 4096, p_max: float = 1.2, gamma=None, source_func=None,
+                       free_surface: bool = False, device=None,
+                       return_reflectivity: bool = False):
+    """``(time, offsets, gather)`` exactly as ``compute_gather_gpu`` (``kennett_gather_gpu.py:169-284``).
+
+    With ``return_reflectivity=True`` the full R(p, omega + i gamma) grid is returned as a
+    fourth element (copied once through a pinned host buffer).  Returned arrays may share
+    that pinned buffer with the next call; copy them to keep them.
+    """
+    time, R, _, g = gather_device(model, offsets, T, nw, np_slow, p_max, gamma, source_func,
+                                  free_surface, device)
+    gh = _pinned(tuple(g.shape), g.dtype)
+    gh.copy_(g, non_blocking=True)
+    if return_reflectivity:
+        Rh = _pinned(tuple(R.shape), R.dtype)
+        Rh.copy_(R, non_blocking=True)
+    torch.cuda.current_stream(g.device).synchronize()
+    if return_reflectivity:
+        return time, np.asarray(offsets), gh.numpy(), Rh.numpy()
+    return time, np.asarray(offsets), gh.numpy().copy()

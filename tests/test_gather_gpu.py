@@ -1,0 +1,121 @@
+"""Parity of the gather path (kr_bessel_sum + kr_traces) and of compute_seismogram.
+
+Reference golden vectors: ``compute_gather`` (float64 CPU gather) on two small cases and
+``compute_seismogram`` on the 6-layer model.  At the full gather size (8192 slownesses,
+2047 frequencies, 100 offsets) each stage is checked against a float64 NumPy/SciPy
+evaluation of that stage on the GPU's own inputs: sampled U(r, w) entries (full sum over
+all 8192 slownesses with scipy's J0) and the trace FFT of the whole U.  Tolerance 1e-10.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_err
+from oracle import kennett_oracle as O
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+
+def _m(g, prefix=""):
+    from seismicinversion_b200.layer_model import LayerModel
+
+    return LayerModel(*[g[prefix + k] for k in ("alpha", "beta", "rho", "thickness", "Q_alpha", "Q_beta")])
+
+
+def test_gather_small_golden(golden):
+    from seismicinversion_b200 import compute_gather, compute_gather_gpu
+    from seismicinversion_b200.earth_models import default_ocean_crust_model
+    from seismicinversion_b200.source import ricker_10hz
+
+    g = golden("gather_small.npz")
+    t, offs, gm1 = compute_gather_gpu(_m(g, "m1_"), g["offsets"], T=64.0, nw=256, np_slow=128,
+                                      p_max=1.2, source_func=ricker_10hz, free_surface=True)
+    assert gm1.shape == (8, 512) and np.array_equal(t, g["time_m1"])
+    assert rel_err(gm1, g["gather_m1"]) < TOL
+    _, _, gd = compute_gather(default_ocean_crust_model(), g["offsets"], T=32.0, nw=128,
+                              np_slow=96, p_max=1.0)
+    assert rel_err(gd, g["gather_md"]) < TOL
+
+
+def test_seismogram_c0(golden):
+    from seismicinversion_b200 import compute_seismogram
+    from seismicinversion_b200.source import ricker_10hz
+
+    g = golden("c0_trace.npz")
+    t, tr = compute_seismogram(_m(g), float(g["p"]), T=64.0, nw=2048, source_func=ricker_10hz,
+                               free_surface=True)
+    assert np.array_equal(t, g["time"])
+    assert rel_err(tr, g["trace"]) < TOL
+
+
+def test_seismogram_default_eps():
+    from seismicinversion_b200 import compute_seismogram
+    from seismicinversion_b200.earth_models import default_ocean_crust_model
+
+    m = default_ocean_crust_model()
+    t, tr = compute_seismogram(m, 0.3, T=32.0, nw=256, eps=0.05)
+    _, tro, _ = O.seismogram(m.alpha, m.beta, m.rho, m.thickness, m.Q_alpha, m.Q_beta, 0.3,
+                             T=32.0, nw=256, eps=0.05)
+    assert rel_err(tr, tro) < TOL
+
+
+def test_bessel_sum_random_and_ragged():
+    from seismicinversion_b200 import device as D
+
+    rng = np.random.default_rng(3)
+    for n_p, n_w, n_r in [(300, 100, 7), (1, 1, 1), (65, 33, 9), (1000, 31, 3)]:
+        R = rng.standard_normal((n_p, n_w)) + 1j * rng.standard_normal((n_p, n_w))
+        p = np.sort(rng.uniform(0.001, 1.2, n_p))
+        pw = rng.uniform(0, 1, n_p) * p
+        om = np.sort(rng.uniform(0.05, 200.0, n_w))
+        r = rng.uniform(0.0, 50.0, n_r)
+        U = D.bessel_sum(torch.as_tensor(R, device="cuda"), p, pw, 1.3e-3, om, r).cpu().numpy()
+        Uo = O.bessel_sum(R, p, om, r, 1.3e-3, taper=pw / p)
+        assert rel_err(U, Uo) < 1e-12, (n_p, n_w, n_r)
+    # no slownesses: U = 0
+    U = D.bessel_sum(torch.zeros((0, 5), dtype=torch.complex128, device="cuda"), [], [], 0.1,
+                     np.arange(1, 6.0), [1.0, 2.0])
+    assert torch.count_nonzero(U) == 0
+
+
+def test_traces_vs_numpy():
+    from seismicinversion_b200 import device as D
+
+    rng = np.random.default_rng(4)
+    for n_r, nw in [(3, 8), (5, 256), (1, 2048)]:
+        U = rng.standard_normal((n_r, nw - 1)) + 1j * rng.standard_normal((n_r, nw - 1))
+        S = rng.standard_normal(nw - 1) + 1j * rng.standard_normal(nw - 1)
+        decay = np.exp(-0.05 * np.arange(2 * nw))
+        tr = D.traces(torch.as_tensor(U, device="cuda"), nw, S=S, decay=decay).cpu().numpy()
+        assert rel_err(tr, O.hermitian_traces(U * S, nw, decay)) < 1e-13
+
+
+def test_full_size_gather_stagewise():
+    from seismicinversion_b200.earth_models import random_layered_model
+    from seismicinversion_b200.kennett_gather_gpu import gather_device
+    from seismicinversion_b200.source import ricker_10hz
+    from scipy.special import j0
+
+    m = random_layered_model(20, seed=1)
+    offsets = np.arange(1, 101) * 0.5
+    T, nw, npp, pmax = 64.0, 2048, 8192, 1.2
+    time, R, U, g = gather_device(m, offsets, T, nw, npp, pmax, source_func=ricker_10hz,
+                                  free_surface=True)
+    assert g.shape == (100, 4096)
+    Rh, Uh, gh = R.cpu().numpy(), U.cpu().numpy(), g.cpu().numpy()
+    dw = 2 * np.pi / T
+    om = np.arange(1, nw) * dw
+    dp = pmax / npp
+    p = np.arange(1, npp + 1) * dp
+    taper = 0.5 * (1 + np.cos(np.pi * p / pmax))
+    rng = np.random.default_rng(9)
+    for _ in range(24):
+        ir, iw = int(rng.integers(100)), int(rng.integers(nw - 1))
+        ref = np.sum(j0((om[iw] * p) * offsets[ir]) * (Rh[:, iw] * (((taper * p) * om[iw]) * dp)))
+        scale = np.max(np.abs(Uh[:, iw])) + 1e-300
+        assert abs(Uh[ir, iw] - ref) / scale < TOL, (ir, iw)
+    gamma = np.pi / T
+    S = ricker_10hz(om, nw * dw)
+    assert rel_err(gh, O.hermitian_traces(Uh * S, nw, np.exp(-gamma * time))) < 1e-12
