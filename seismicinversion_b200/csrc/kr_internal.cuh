@@ -50,10 +50,11 @@ __device__ __forceinline__ cd sweep(cd w, int n_layers, const LayerP* s_layer,
                                     const Iface* s_iface) {
   const int I = n_layers - 1;
   // Bottom interface: RRd below it is 0, so RRd = Rd.
-  Sym r;
+  M2 r;
   r.a = s_iface[I - 1].rd11;
   r.b = s_iface[I - 1].rd12;
-  r.c = s_iface[I - 1].rd22;
+  r.c = s_iface[I - 1].rd12;
+  r.d = s_iface[I - 1].rd22;
   for (int i = I - 2; i >= 0; --i) {
     const LayerP& lb = s_layer[i + 1];
     cd ea = cexp_(w * lb.ca);

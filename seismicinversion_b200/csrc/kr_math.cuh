@@ -10,10 +10,8 @@
 //   PP + free surface     kennett_reflectivity.py:264-326
 //
 // Storage choices (ours): Rd and Ru are symmetric and Tu = Td^T (reciprocity,
-// scattering_matrices.py:150), so an interface is 10 complex numbers; the cumulative
-// reflection matrix RRd stays symmetric through the recursion (MT (I - Ru MT)^-1 is symmetric
-// when MT and Ru are), so the sweep carries 3 complex numbers instead of 4.  The 2x2 inverse
-// is one reciprocal of the determinant times the adjugate.
+// scattering_matrices.py:150), so an interface is 10 complex numbers.  The 2x2 inverse is
+// one reciprocal of the determinant times the adjugate.
 #pragma once
 
 #include <math.h>
@@ -249,31 +247,38 @@ KR_HD Iface interface_coeffs(double p, int iface, const LayerP& up, const LayerP
 
 // ---------------------------------------------------------------------------------------
 // One Kennett addition step: RRd <- Rd + Tu MT (I - Ru MT)^-1 Td with MT = E RRd E,
-// E = diag(ea, eb) of the layer below the interface.  RRd = [[a, b], [b, c]].
+// E = diag(ea, eb) of the layer below the interface.  RRd = [[a, b], [c, d]].
+//
+// RRd is symmetric in exact arithmetic, but the two off-diagonal entries carry different
+// rounding, and at large slowness (evanescent layers, near-cancelling interface
+// determinants) the recursion amplifies rounding by ~1e6-1e8: carrying one off-diagonal
+// for both positions loses 1e-8 relative accuracy against an extended-precision
+// evaluation, the full matrix keeps the reference's ~1e-10.  So the step carries all four
+// entries, in the reference's product order (kennett_reflectivity.py:235-256).
 // ---------------------------------------------------------------------------------------
-struct Sym {
-  cd a, b, c;
+struct M2 {
+  cd a, b, c, d;
 };
 
-KR_HD Sym kennett_step(const Sym& r, cd ea, cd eb, const Iface& f) {
+KR_HD M2 kennett_step(const M2& r, cd ea, cd eb, const Iface& f) {
   cd eaea = ea * ea, ebeb = eb * eb, eaeb = ea * eb;
-  cd m11 = eaea * r.a, m12 = eaeb * r.b, m22 = ebeb * r.c;
-  cd n11 = 1.0 - (f.ru11 * m11 + f.ru12 * m12);
+  cd m11 = eaea * r.a, m12 = eaeb * r.b, m21 = eaeb * r.c, m22 = ebeb * r.d;
+  cd n11 = 1.0 - (f.ru11 * m11 + f.ru12 * m21);
   cd n12 = -(f.ru11 * m12 + f.ru12 * m22);
-  cd n21 = -(f.ru12 * m11 + f.ru22 * m12);
+  cd n21 = -(f.ru12 * m11 + f.ru22 * m21);
   cd n22 = 1.0 - (f.ru12 * m12 + f.ru22 * m22);
   cd idet = recip(n11 * n22 - n12 * n21);
-  cd x11 = (m11 * n22 - m12 * n21) * idet;
-  cd x12 = (m12 * n11 - m11 * n12) * idet;
-  cd x22 = (m22 * n11 - m12 * n12) * idet;
-  cd y11 = x11 * f.td11 + x12 * f.td21;
-  cd y12 = x11 * f.td12 + x12 * f.td22;
-  cd y21 = x12 * f.td11 + x22 * f.td21;
-  cd y22 = x12 * f.td12 + x22 * f.td22;
-  Sym o;
-  o.a = f.rd11 + (f.td11 * y11 + f.td21 * y21);
-  o.b = f.rd12 + (f.td11 * y12 + f.td21 * y22);
-  o.c = f.rd22 + (f.td12 * y12 + f.td22 * y22);
+  cd u11 = n22 * idet, u12 = -(n12 * idet), u21 = -(n21 * idet), u22 = n11 * idet;
+  cd x11 = m11 * u11 + m12 * u21, x12 = m11 * u12 + m12 * u22;
+  cd x21 = m21 * u11 + m22 * u21, x22 = m21 * u12 + m22 * u22;
+  // Tu X with Tu = Td^T
+  cd z11 = f.td11 * x11 + f.td21 * x21, z12 = f.td11 * x12 + f.td21 * x22;
+  cd z21 = f.td12 * x11 + f.td22 * x21, z22 = f.td12 * x12 + f.td22 * x22;
+  M2 o;
+  o.a = f.rd11 + (z11 * f.td11 + z12 * f.td21);
+  o.b = f.rd12 + (z11 * f.td12 + z12 * f.td22);
+  o.c = f.rd12 + (z21 * f.td11 + z22 * f.td21);
+  o.d = f.rd22 + (z21 * f.td12 + z22 * f.td22);
   return o;
 }
 
