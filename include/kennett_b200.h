@@ -94,6 +94,27 @@ kr_status kr_bessel_sum(const double* R, const double* p, const double* pw, int3
                         int32_t n_r, double* U, void* workspace, size_t workspace_bytes,
                         void* stream);
 
+/*
+ * Allocation-free variant of kr_bessel_sum.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory -- an application that reserved the GPU in
+ * its own pool and hands out only pointers, a C/Fortran system whose device buffers are owned
+ * by another component, or a loop that must avoid cudaMalloc's implicit synchronisation.  The
+ * caller passes inputs and U only (same meaning as kr_bessel_sum); the slice partials live in
+ * a 16 MiB file-scope device array that every GPU loading the library holds until exit.
+ * Limit: n_r * n_w <= 1048576 (one slice must fit), else KR_ERR_TOO_LARGE.  No cudaMalloc,
+ * cudaFree or allocating library call is made.  The first call on each device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (other streams, other
+ * host threads) race and must be serialised by the caller.
+ */
+kr_status kr_bessel_sum_noalloc(const double* R, const double* p, const double* pw,
+                                int32_t n_p, double dp, const double* omega, int32_t n_w,
+                                const double* offsets, int32_t n_r, double* U, void* stream);
+
+/* Size in bytes of the static scratch array used by kr_bessel_sum_noalloc (16 MiB). */
+size_t kr_bessel_sum_noalloc_scratch_bytes(void);
+
 /* Bytes of device workspace kr_traces needs. */
 size_t kr_traces_workspace_bytes(int32_t n_r, int32_t nw);
 

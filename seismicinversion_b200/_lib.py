@@ -40,6 +40,9 @@ _SIGNATURES = {
     "kr_bessel_sum_workspace_bytes": (_size_t, [_i32, _i32, _i32]),
     "kr_bessel_sum": (_i32, [_vp, _vp, _vp, _i32, ctypes.c_double, _vp, _i32, _vp, _i32, _vp,
                              _vp, _size_t, _vp]),
+    "kr_bessel_sum_noalloc": (_i32, [_vp, _vp, _vp, _i32, ctypes.c_double, _vp, _i32, _vp,
+                                     _i32, _vp, _vp]),
+    "kr_bessel_sum_noalloc_scratch_bytes": (_size_t, []),
     "kr_traces_workspace_bytes": (_size_t, [_i32, _i32]),
     "kr_traces": (_i32, [_vp, _vp, _i32, _i32, _vp, _vp, _vp, _size_t, _vp]),
     # include/kennett_b200_bench.h

@@ -12,6 +12,7 @@
 // (np.fft.fft) equals the inverse real transform of conj(H).  The decay exp(-gamma t) is
 // applied by a last elementwise kernel.
 #include <cufft.h>
+#include <stdio.h>
 
 #include <mutex>
 #include <vector>
@@ -252,4 +253,107 @@ extern "C" kr_status kr_traces(const double* U, const double* S, int32_t n_r, in
     return check_launch("kr_traces: decay");
   }
   return KR_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Allocation-free variant of kr_bessel_sum.
+//
+// Some callers cannot allocate device memory at all: a host application that reserved the
+// whole GPU in its own pool at start-up and hands out only pointers, a processing system
+// that reaches this library through a C/Fortran FFI with device buffers owned by another
+// component, or a loop that must not hit cudaMalloc's implicit device synchronisation.
+// They pass inputs and the output only; the slice partials live in this file-scope device
+// array instead of a caller workspace.  Every GPU that loads the library holds the array
+// (16 MiB) until the process exits.
+// ---------------------------------------------------------------------------------------
+namespace kr {
+
+constexpr size_t kNoAllocScratchBytes = (size_t)16 << 20;
+static __device__ __align__(256) unsigned char g_bessel_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+static std::mutex g_scratch_mu;
+static void* g_scratch_addr[kMaxDevices];
+
+// Device address of g_bessel_scratch on the current device.  The host-side symbol is only a
+// stand-in, so the address is looked up once per device (with that device current) and
+// cached.
+static kr_status scratch_address(void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    set_last_error("kr_bessel_sum_noalloc: cudaGetDevice", e);
+    return KR_ERR_CUDA;
+  }
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_last_error_msg("kr_bessel_sum_noalloc: device index beyond 63");
+    return KR_ERR_TOO_LARGE;
+  }
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  if (!g_scratch_addr[dev]) {
+    void* ptr = nullptr;
+    e = cudaGetSymbolAddress(&ptr, g_bessel_scratch);
+    if (e != cudaSuccess || !ptr) {
+      set_last_error("kr_bessel_sum_noalloc: cudaGetSymbolAddress", e);
+      return KR_ERR_CUDA;
+    }
+    g_scratch_addr[dev] = ptr;
+  }
+  *out = g_scratch_addr[dev];
+  return KR_OK;
+}
+
+}  // namespace kr
+
+extern "C" size_t kr_bessel_sum_noalloc_scratch_bytes(void) { return kNoAllocScratchBytes; }
+
+extern "C" kr_status kr_bessel_sum_noalloc(const double* R, const double* p, const double* pw,
+                                           int32_t n_p, double dp, const double* omega,
+                                           int32_t n_w, const double* offsets, int32_t n_r,
+                                           double* U, void* stream) {
+  if (n_p < 0 || n_w < 0 || n_r < 0) return KR_ERR_INVALID_ARGUMENT;
+  if (n_w == 0 || n_r == 0) return KR_OK;
+  if (!U || !omega || !offsets) return KR_ERR_INVALID_ARGUMENT;
+  const size_t slice_bytes = (size_t)n_r * n_w * sizeof(double2);
+  if (slice_bytes > kNoAllocScratchBytes) {
+    char buf[200];
+    snprintf(buf, sizeof buf,
+             "kr_bessel_sum_noalloc: n_r * n_w = %lld exceeds the static scratch "
+             "(16 MiB holds n_r * n_w <= %lld)",
+             (long long)n_r * n_w, (long long)(kNoAllocScratchBytes / sizeof(double2)));
+    set_last_error_msg(buf);
+    return KR_ERR_TOO_LARGE;
+  }
+  if ((n_r + kBsR - 1) / kBsR > 65535) return KR_ERR_TOO_LARGE;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (n_p == 0) {
+    cudaError_t e = cudaMemsetAsync(U, 0, (size_t)n_r * n_w * sizeof(double2), st);
+    if (e != cudaSuccess) set_last_error("kr_bessel_sum_noalloc: memset", e);
+    return cuda_status(e);
+  }
+  if (!R || !p || !pw) return KR_ERR_INVALID_ARGUMENT;
+  void* scratch = nullptr;
+  kr_status s = scratch_address(&scratch);
+  if (s != KR_OK) return s;
+  // As many slowness slices as the occupancy target asks for and the scratch holds.  Each
+  // slice element is written by exactly one thread before the reduction reads it, so the
+  // array needs no clearing between calls.
+  BesselPlan b = bessel_plan(n_p, n_w, n_r);
+  const int cap = (int)(kNoAllocScratchBytes / slice_bytes);
+  int n_slices = b.n_slices < cap ? b.n_slices : cap;
+  const int p_per_slice = (n_p + n_slices - 1) / n_slices;
+  n_slices = (n_p + p_per_slice - 1) / p_per_slice;
+  double2* partial = reinterpret_cast<double2*>(scratch);
+  dim3 grid((n_w + kBsW - 1) / kBsW, (n_r + kBsR - 1) / kBsR, n_slices);
+  bessel_partial_kernel<<<grid, dim3(kBsW, kBsR), 0, st>>>(
+      reinterpret_cast<const double2*>(R), p, pw, n_p, dp, omega, n_w, offsets, n_r,
+      p_per_slice, partial);
+  s = check_launch("kr_bessel_sum_noalloc: partial");
+  if (s != KR_OK) return s;
+  const size_t n_elem = (size_t)n_r * n_w;
+  int blocks = (int)((n_elem + 255) / 256);
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  reduce_slices_kernel<<<blocks, 256, 0, st>>>(partial, n_slices, n_elem,
+                                               reinterpret_cast<double2*>(U));
+  return check_launch("kr_bessel_sum_noalloc: reduce");
 }
