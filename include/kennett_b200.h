@@ -72,6 +72,45 @@ kr_status kr_reflectivity(const double* layers, int32_t n_layers, const double* 
                           const double* omega, int32_t n_w, uint32_t flags, double* R,
                           void* stream);
 
+/* Bytes of device workspace kr_jacobian needs. */
+size_t kr_jacobian_workspace_bytes(int32_t n_layers, int32_t n_p, int32_t n_w);
+
+/*
+ * Reflectivity and its Jacobian with respect to every layer's alpha, beta, rho, h.
+ * Replaces the autograd graph of kennett_reflectivity_torch
+ * (Kennett_Reflectivity/kennett_torch.py:312-480) and jacobian (kennett_torch.py:611-641,
+ * jacrev of Re and Im).  Hand-written adjoint: one reverse sweep per (omega, p), states
+ * recomputed from sqrt(I) checkpoints; interface-coefficient tangents by forward-mode dual
+ * numbers once per (p, interface).
+ *   layers, p, omega, flags : as kr_reflectivity
+ *   R : device complex [n_p][n_w] output, or NULL
+ *   J : device complex [n_p][4*n_layers][n_w] output, J[j][k*L + l][w] = dR(p_j, w)/d theta,
+ *       theta = alpha_l (k=0), beta_l (1), rho_l (2), h_l (3).  Derivatives through the
+ *       ocean's S quantities, layers with beta = 0 and the half-space phase are zero.
+ *   workspace : >= kr_jacobian_workspace_bytes(n_layers, n_p, n_w) bytes
+ */
+kr_status kr_jacobian(const double* layers, int32_t n_layers, const double* p, int32_t n_p,
+                      const double* omega, int32_t n_w, uint32_t flags, double* R, double* J,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
+/* Bytes of device workspace kr_misfit_gradient needs. */
+size_t kr_misfit_gradient_workspace_bytes(int32_t n_layers, int32_t n_p, int32_t n_w);
+
+/*
+ * Misfit chi = sum_{p, w} |R - R_obs|^2 and its gradient with respect to every layer's
+ * alpha, beta, rho, h, without forming the Jacobian (block-reduced in a fixed order).
+ * Replaces the per-slowness misfit + torch.autograd.grad of taup_misfit_grad_hessian
+ * (Kennett_Reflectivity/taup_inversion.py:112-187) for the gradient part.
+ *   R_obs    : device complex [n_p][n_w]
+ *   R        : device complex [n_p][n_w] output (the forward result), or NULL
+ *   chi_grad : device float64 [4*n_layers + 1] output: gradient (index k*L + l as in
+ *              kr_jacobian) followed by chi.
+ */
+kr_status kr_misfit_gradient(const double* layers, int32_t n_layers, const double* p,
+                             int32_t n_p, const double* omega, int32_t n_w, uint32_t flags,
+                             const double* R_obs, double* R, double* chi_grad, void* workspace,
+                             size_t workspace_bytes, void* stream);
+
 /* Bytes of device workspace kr_bessel_sum needs for these sizes. */
 size_t kr_bessel_sum_workspace_bytes(int32_t n_p, int32_t n_w, int32_t n_r);
 

@@ -1,0 +1,265 @@
+// Derivatives of the Kennett path.
+//
+// R is a holomorphic function of every complex intermediate (coefficients, phase factors,
+// the 2x2 matrices), so one reverse sweep per (omega, p) carries "adjoints"
+// Zbar = dR/dZ (complex partial derivatives, no conjugation) from R down to
+//   * the 10 independent coefficients of each interface (Rd, Ru symmetric, Td; Tu = Td^T),
+//   * the two phase factors ea, eb of each layer.
+// dR/dtheta for a real layer parameter theta is then sum_z zbar * dz/dtheta, with
+// dz/dtheta from (i) forward-mode tangents of the coefficients (ScatTan, omega independent,
+// once per slowness and interface) and (ii) closed-form phase derivatives:
+//   ea = exp(omega * i eta h):  dea/dalpha = ea * omega * (i h deta/dalpha),
+//                               dea/dh     = ea * omega * (i eta),        likewise eb.
+// Primitive chains: ds/dv = -s/v (complex slowness), deta/dv = -s^2 / (eta v),
+// d(beta_c)/dbeta = beta_c / beta (beta_c = 1/s_s); zero where beta = 0 and for the ocean
+// S quantities; phase derivatives are zero in the half-space (phase fixed to 1), as in the
+// reference's torch forward (kennett_torch.py:369-390, torch.where masks).
+#pragma once
+
+#include "kr_dual.cuh"
+#include "kr_math.cuh"
+
+namespace kr {
+
+// ---------------- 2x2 complex matrix helpers ([[a, b], [c, d]]) ----------------
+KR_HD M2 m2(cd a, cd b, cd c, cd d) { M2 r; r.a = a; r.b = b; r.c = c; r.d = d; return r; }
+KR_HD M2 mmul(const M2& x, const M2& y) {
+  return m2(x.a * y.a + x.b * y.c, x.a * y.b + x.b * y.d, x.c * y.a + x.d * y.c,
+            x.c * y.b + x.d * y.d);
+}
+KR_HD M2 mT(const M2& x) { return m2(x.a, x.c, x.b, x.d); }
+KR_HD M2 madd(const M2& x, const M2& y) { return m2(x.a + y.a, x.b + y.b, x.c + y.c, x.d + y.d); }
+KR_HD M2 mneg(const M2& x) { return m2(-x.a, -x.b, -x.c, -x.d); }
+
+// Per-layer derivative factors for one slowness.
+struct LayerD {
+  cd ca_alpha;  // d(ca)/d alpha = i h deta/dalpha      (0 in the half-space)
+  cd cb_beta;   // d(cb)/d beta  = i h dneta/dbeta      (0 in the half-space / beta = 0)
+  cd ca_h;      // d(ca)/d h     = i eta                (0 in the half-space)
+  cd cb_h;      // d(cb)/d h     = i neta
+  cd eta_alpha; // deta/dalpha
+  cd neta_beta; // dneta/dbeta
+  cd betac_beta;// dbeta_c/dbeta
+};
+
+KR_HD LayerD layer_derivs(const double* tab, int n_layers, int l, double p, const LayerP& lp) {
+  const double alpha = tab[l];
+  const double beta = tab[n_layers + l];
+  const double h = tab[3 * n_layers + l];
+  const double qa = tab[4 * n_layers + l];
+  const double qb = tab[5 * n_layers + l];
+  LayerD o;
+  cd sp = complex_slowness(alpha, qa);
+  o.eta_alpha = -((sp * sp) * recip(lp.eta * alpha));
+  if (beta > 0.0 && l > 0) {
+    cd ss = complex_slowness(beta, qb);
+    o.neta_beta = -((ss * ss) * recip(lp.neta * beta));
+    o.betac_beta = lp.betac * (1.0 / beta);
+  } else {
+    o.neta_beta = mk(0.0, 0.0);
+    o.betac_beta = (beta > 0.0) ? lp.betac * (1.0 / beta) : mk(0.0, 0.0);
+  }
+  if (is_half_space(h)) {
+    o.ca_alpha = o.cb_beta = o.ca_h = o.cb_h = mk(0.0, 0.0);
+  } else {
+    const cd ih = mk(0.0, h);
+    o.ca_alpha = ih * o.eta_alpha;
+    o.cb_beta = ih * o.neta_beta;
+    o.ca_h = mk(-lp.eta.y, lp.eta.x);
+    o.cb_h = mk(-lp.neta.y, lp.neta.x);
+  }
+  return o;
+}
+
+// Tangents of the 10 independent coefficients of interface `iface` with respect to
+// (alpha_u, beta_u, rho_u, alpha_l, beta_l, rho_l) of the upper (u = iface) and lower
+// (l = iface + 1) layer: t[k][j], k in coefficient order rd11 rd12 rd22 ru11 ru12 ru22
+// td11 td12 td21 td22.
+struct ScatTan {
+  cd t[10][6];
+};
+
+KR_HD void interface_tangents(double p, int iface, const LayerP& up, const LayerD& dup,
+                              const LayerP& lo, const LayerD& dlo, ScatTan& out) {
+  typedef Dual<6> D;
+  D eta1 = dconst<6>(up.eta), neta1 = dconst<6>(up.neta), rho1 = dconst<6>(to_c(up.rho));
+  D betac1 = dconst<6>(up.betac);
+  D eta2 = dconst<6>(lo.eta), neta2 = dconst<6>(lo.neta), rho2 = dconst<6>(to_c(lo.rho));
+  D betac2 = dconst<6>(lo.betac);
+  eta1.d[0] = dup.eta_alpha;
+  neta1.d[1] = dup.neta_beta;
+  betac1.d[1] = dup.betac_beta;
+  rho1.d[2] = mk(1.0, 0.0);
+  eta2.d[3] = dlo.eta_alpha;
+  neta2.d[4] = dlo.neta_beta;
+  betac2.d[4] = dlo.betac_beta;
+  rho2.d[5] = mk(1.0, 0.0);
+  IfaceT<D> f;
+  if (iface == 0)
+    ocean_bottom<D>(p, eta1, rho1, eta2, neta2, rho2, betac2, f);
+  else
+    solid_solid<D>(p, eta1, neta1, rho1, betac1, eta2, neta2, rho2, betac2, f);
+  const D* c[10] = {&f.rd11, &f.rd12, &f.rd22, &f.ru11, &f.ru12,
+                    &f.ru22, &f.td11, &f.td12, &f.td21, &f.td22};
+  for (int k = 0; k < 10; ++k)
+    for (int j = 0; j < 6; ++j) out.t[k][j] = c[k]->d[j];
+}
+
+// Reverse of kennett_step.  Inputs: the step's input state r, the phase factors, the
+// interface, and ob = dR/d(step output).  Outputs: rbar = dR/d(step input), dR/dea, dR/deb
+// and the 10 coefficient adjoints cbar (same order as ScatTan).
+KR_HD void kennett_step_reverse(const M2& r, cd ea, cd eb, const Iface& f, const M2& ob,
+                                M2& rbar, cd& eabar, cd& ebbar, cd cbar[10]) {
+  cd eaea = ea * ea, ebeb = eb * eb, eaeb = ea * eb;
+  M2 m = m2(eaea * r.a, eaeb * r.b, eaeb * r.c, ebeb * r.d);
+  M2 Ru = m2(f.ru11, f.ru12, f.ru12, f.ru22);
+  M2 Td = m2(f.td11, f.td12, f.td21, f.td22);
+  M2 Rm = mmul(Ru, m);
+  M2 N = m2(1.0 - Rm.a, -Rm.b, -Rm.c, 1.0 - Rm.d);
+  cd idet = recip(N.a * N.d - N.b * N.c);
+  M2 U = m2(N.d * idet, -(N.b * idet), -(N.c * idet), N.a * idet);
+  M2 X = mmul(m, U);
+  M2 Z = mmul(mT(Td), X);
+  // out = Rd + Z Td
+  M2 Zb = mmul(ob, mT(Td));
+  M2 Tdb = mmul(mT(Z), ob);
+  // Z = Td^T X
+  M2 Xb = mmul(Td, Zb);
+  Tdb = madd(Tdb, mmul(X, mT(Zb)));
+  // X = m U
+  M2 mb = mmul(Xb, mT(U));
+  M2 Ub = mmul(mT(m), Xb);
+  // U = N^-1
+  M2 UT = mT(U);
+  M2 Nb = mneg(mmul(mmul(UT, Ub), UT));
+  // N = I - Ru m
+  M2 Rub = mneg(mmul(Nb, mT(m)));
+  mb = madd(mb, mneg(mmul(Ru, Nb)));
+  // m = E r E
+  rbar = m2(mb.a * eaea, mb.b * eaeb, mb.c * eaeb, mb.d * ebeb);
+  cd cross = r.b * mb.b + r.c * mb.c;
+  eabar = 2.0 * (ea * (r.a * mb.a)) + eb * cross;
+  ebbar = 2.0 * (eb * (r.d * mb.d)) + ea * cross;
+  cbar[0] = ob.a;
+  cbar[1] = ob.b + ob.c;
+  cbar[2] = ob.d;
+  cbar[3] = Rub.a;
+  cbar[4] = Rub.b + Rub.c;
+  cbar[5] = Rub.d;
+  cbar[6] = Tdb.a;
+  cbar[7] = Tdb.b;
+  cbar[8] = Tdb.c;
+  cbar[9] = Tdb.d;
+}
+
+// dR/d(alpha, beta, rho, h) of one layer.
+struct Acc {
+  cd a, b, r, h;
+};
+
+KR_HD Acc acc_zero() {
+  Acc z;
+  z.a = z.b = z.r = z.h = mk(0.0, 0.0);
+  return z;
+}
+
+// Adds the coefficient-tangent contractions of one interface to its upper / lower layer.
+KR_HD void contract(const ScatTan& t, const cd cbar[10], Acc& up, Acc& lo) {
+  cd s[6];
+  for (int j = 0; j < 6; ++j) s[j] = mk(0.0, 0.0);
+  for (int k = 0; k < 10; ++k) {
+    if (cbar[k].x == 0.0 && cbar[k].y == 0.0) continue;
+    for (int j = 0; j < 6; ++j) s[j] = s[j] + cbar[k] * t.t[k][j];
+  }
+  up.a = up.a + s[0];
+  up.b = up.b + s[1];
+  up.r = up.r + s[2];
+  lo.a = lo.a + s[3];
+  lo.b = lo.b + s[4];
+  lo.r = lo.r + s[5];
+}
+
+constexpr int kSegMax = 16;  // checkpoint spacing cap: (I - 1) <= 16 * 16 covers 256 layers
+constexpr int kCpMax = 16;
+
+KR_HD int checkpoint_spacing(int nsteps) {
+  int s = 1;
+  while (s * s < nsteps) ++s;
+  return s;
+}
+
+// R and dR/dtheta for one (omega, p) pair.  Forward sweep storing the state every `seg`
+// steps, then the reverse sweep top-down, each segment recomputed from its checkpoint
+// (memory O(sqrt(I)) states instead of I).  sink.reflectivity(R) is called once before
+// the reverse pass, sink.layer(l, acc) once per layer l (in order 0, 1, ..., L-1) with
+// the finished dR/d(alpha_l, beta_l, rho_l, h_l).
+#ifdef __CUDACC__
+#pragma nv_exec_check_disable
+#endif
+template <class Sink>
+KR_HD void jacobian_pair(int L, cd w, bool free_surface, int seg, const LayerP* lay,
+                         const LayerD* dlay, const Iface* coef, const ScatTan* tan, Sink& sink) {
+  const int I = L - 1;
+  const int nsteps = I - 1;  // step s applies interface i = I - 2 - s
+  M2 cp[kCpMax];
+  M2 r = m2(coef[I - 1].rd11, coef[I - 1].rd12, coef[I - 1].rd12, coef[I - 1].rd22);
+  for (int s = 0; s < nsteps; ++s) {
+    if (s % seg == 0) cp[s / seg] = r;
+    const int i = I - 2 - s;
+    r = kennett_step(r, cexp_(w * lay[i + 1].ca), cexp_(w * lay[i + 1].cb), coef[i]);
+  }
+  const cd e0 = cexp_(w * lay[0].ca);
+  sink.reflectivity(pp_surface(r.a, e0, free_surface));
+  // top: R = E0^2 RRd_00, or y / (1 + y) with y = E0^2 RRd_00
+  cd g = mk(1.0, 0.0);
+  if (free_surface) {
+    cd q = recip(1.0 + (e0 * e0) * r.a);
+    g = q * q;
+  }
+  M2 ob = m2((e0 * e0) * g, mk(0.0, 0.0), mk(0.0, 0.0), mk(0.0, 0.0));
+  const cd f0 = 2.0 * (e0 * r.a) * g * e0 * w;
+  Acc cur = acc_zero(), nxt = acc_zero();
+  cur.a = f0 * dlay[0].ca_alpha;
+  cur.h = f0 * dlay[0].ca_h;
+  M2 sg[kSegMax];
+  const int ncp = nsteps > 0 ? (nsteps + seg - 1) / seg : 0;
+  for (int q = ncp - 1; q >= 0; --q) {
+    const int s0 = q * seg;
+    const int s1 = s0 + seg < nsteps ? s0 + seg : nsteps;
+    M2 x = cp[q];
+    for (int s = s0; s < s1; ++s) {
+      sg[s - s0] = x;
+      const int i = I - 2 - s;
+      if (s + 1 < s1)
+        x = kennett_step(x, cexp_(w * lay[i + 1].ca), cexp_(w * lay[i + 1].cb), coef[i]);
+    }
+    for (int s = s1 - 1; s >= s0; --s) {
+      const int i = I - 2 - s;  // interface i, lower layer i + 1
+      const cd ea = cexp_(w * lay[i + 1].ca), eb = cexp_(w * lay[i + 1].cb);
+      M2 rb;
+      cd eab, ebb, cbar[10];
+      kennett_step_reverse(sg[s - s0], ea, eb, coef[i], ob, rb, eab, ebb, cbar);
+      contract(tan[i], cbar, cur, nxt);
+      const LayerD& d = dlay[i + 1];
+      const cd fa = eab * ea * w, fb = ebb * eb * w;
+      nxt.a = nxt.a + fa * d.ca_alpha;
+      nxt.b = nxt.b + fb * d.cb_beta;
+      nxt.h = nxt.h + fa * d.ca_h + fb * d.cb_h;
+      sink.layer(i, cur);
+      cur = nxt;
+      nxt = acc_zero();
+      ob = rb;
+    }
+  }
+  // bottom interface I-1 initialises RRd = Rd
+  cd cbar[10];
+  cbar[0] = ob.a;
+  cbar[1] = ob.b + ob.c;
+  cbar[2] = ob.d;
+  for (int k = 3; k < 10; ++k) cbar[k] = mk(0.0, 0.0);
+  contract(tan[I - 1], cbar, cur, nxt);
+  sink.layer(I - 1, cur);
+  sink.layer(L - 1, nxt);
+}
+
+}  // namespace kr

@@ -1,0 +1,291 @@
+// Jacobian and misfit gradient of the reflectivity with respect to every layer's
+// (alpha, beta, rho, h): the hand-written adjoint of the Kennett recursion.
+//
+// Three kernels:
+//   deriv_layer_kernel : per (p, layer)      layer terms + derivative factors  -> workspace
+//   deriv_iface_kernel : per (p, interface)  coefficients + 10x6 tangents      -> workspace
+//   deriv_sweep_kernel : per (omega, p)      forward sweep with sqrt(I) checkpoints, then the
+//                        reverse sweep segment by segment (each segment recomputed from its
+//                        checkpoint: per-layer recomputation instead of a full tape), giving
+//                        dR/d(theta) for all 4L parameters.  JAC mode writes them
+//                        (J[p][k*L + l][omega], k = alpha, beta, rho, h); GRAD mode contracts
+//                        them with the residual, 2 Re(conj(R - R_obs) dR/dtheta), and reduces
+//                        over the block in a fixed order; a last kernel adds the block
+//                        partials in order (deterministic).
+// Replaces the torch autograd graph of kennett_reflectivity_torch (kennett_torch.py:312-480),
+// jacobian (:611-641) and the per-slowness gradient of taup_misfit_grad_hessian
+// (taup_inversion.py:112-187).
+#include "kr_adjoint.cuh"
+#include "kr_internal.cuh"
+
+namespace kr {
+
+constexpr int kDerThreads = 128;
+
+static size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct DerivWs {
+  LayerP* lay;
+  LayerD* dlay;
+  Iface* coef;
+  ScatTan* tan;
+  double* partial;  // [blocks][4L + 1] (gradient mode)
+  size_t bytes;
+};
+
+static DerivWs deriv_ws(void* base, int L, int n_p, size_t n_blocks) {
+  DerivWs w;
+  const int I = L - 1;
+  size_t off = 0;
+  unsigned char* b = static_cast<unsigned char*>(base);
+  w.lay = reinterpret_cast<LayerP*>(b + off);
+  off = a256(off + sizeof(LayerP) * (size_t)n_p * L);
+  w.dlay = reinterpret_cast<LayerD*>(b + off);
+  off = a256(off + sizeof(LayerD) * (size_t)n_p * L);
+  w.coef = reinterpret_cast<Iface*>(b + off);
+  off = a256(off + sizeof(Iface) * (size_t)n_p * I);
+  w.tan = reinterpret_cast<ScatTan*>(b + off);
+  off = a256(off + sizeof(ScatTan) * (size_t)n_p * I);
+  w.partial = reinterpret_cast<double*>(b + off);
+  off = a256(off + sizeof(double) * n_blocks * (size_t)(4 * L + 1));
+  w.bytes = off;
+  return w;
+}
+
+__global__ void deriv_layer_kernel(const double* __restrict__ tab, int L,
+                                   const double* __restrict__ p, int n_p, LayerP* lay,
+                                   LayerD* dlay) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n_p * L) return;
+  const int j = idx / L, l = idx % L;
+  LayerP lp = layer_terms(tab, L, l, p[j]);
+  lay[idx] = lp;
+  dlay[idx] = layer_derivs(tab, L, l, p[j], lp);
+}
+
+__global__ void deriv_iface_kernel(const double* __restrict__ p, int n_p, int L,
+                                   const LayerP* __restrict__ lay,
+                                   const LayerD* __restrict__ dlay, Iface* coef, ScatTan* tan) {
+  const int I = L - 1;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n_p * I) return;
+  const int j = idx / I, i = idx % I;
+  const LayerP up = lay[j * L + i], lo = lay[j * L + i + 1];
+  coef[idx] = interface_coeffs(p[j], i, up, lo);
+  interface_tangents(p[j], i, up, dlay[j * L + i], lo, dlay[j * L + i + 1], tan[idx]);
+}
+
+template <bool GRAD>
+__device__ __forceinline__ void finalize_layer(int l, int L, const Acc& acc, bool valid, cd res,
+                                               int ip, int iw, int n_w, double2* __restrict__ J,
+                                               double* s_grad, double* s_warp) {
+  if (!GRAD) {
+    if (valid) {
+      const size_t base = ((size_t)ip * 4 * L) * n_w + iw;
+      J[base + (size_t)(0 * L + l) * n_w] = make_double2(acc.a.x, acc.a.y);
+      J[base + (size_t)(1 * L + l) * n_w] = make_double2(acc.b.x, acc.b.y);
+      J[base + (size_t)(2 * L + l) * n_w] = make_double2(acc.r.x, acc.r.y);
+      J[base + (size_t)(3 * L + l) * n_w] = make_double2(acc.h.x, acc.h.y);
+    }
+  } else {
+    // d chi / d theta = 2 Re(conj(res) dR/dtheta) = 2 (res.x dR.x + res.y dR.y)
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    if (valid) {
+      v[0] = 2.0 * (res.x * acc.a.x + res.y * acc.a.y);
+      v[1] = 2.0 * (res.x * acc.b.x + res.y * acc.b.y);
+      v[2] = 2.0 * (res.x * acc.r.x + res.y * acc.r.y);
+      v[3] = 2.0 * (res.x * acc.h.x + res.y * acc.h.y);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+      for (int k = 0; k < 4; ++k) s_warp[warp * 4 + k] = v[k];
+    __syncthreads();
+    if (threadIdx.x < 4) {
+      double t = 0.0;
+      for (int w = 0; w < kDerThreads / 32; ++w) t += s_warp[w * 4 + threadIdx.x];
+      s_grad[threadIdx.x * L + l] += t;
+    }
+    __syncthreads();
+  }
+}
+
+// Receives R and the per-layer derivatives of one thread's (omega, p) pair.
+template <bool GRAD>
+struct PairSink {
+  int L, ip, iw, n_w;
+  bool valid;
+  const double2* R_obs;
+  double2* R_out;
+  double2* J;
+  double* s_grad;
+  double* s_warp;
+  cd res;
+  __device__ void reflectivity(cd R) {
+    res = mk(0.0, 0.0);
+    if (!valid) return;
+    if (R_out) R_out[(size_t)ip * n_w + iw] = make_double2(R.x, R.y);
+    if (GRAD) {
+      const double2 o = R_obs[(size_t)ip * n_w + iw];
+      res = mk(R.x - o.x, R.y - o.y);
+    }
+  }
+  __device__ void layer(int l, const Acc& acc) {
+    finalize_layer<GRAD>(l, L, acc, valid, res, ip, iw, n_w, J, s_grad, s_warp);
+  }
+};
+
+template <bool GRAD>
+__global__ void __launch_bounds__(kDerThreads)
+deriv_sweep_kernel(int L, const double* __restrict__ p, int n_p,
+                   const double2* __restrict__ omega, int n_w, int n_wtiles, int free_surface,
+                   int seg, const LayerP* __restrict__ lay_all, const LayerD* __restrict__ dlay_all,
+                   const Iface* __restrict__ coef_all, const ScatTan* __restrict__ tan_all,
+                   const double2* __restrict__ R_obs, double2* __restrict__ R_out,
+                   double2* __restrict__ J, double* __restrict__ partial) {
+  extern __shared__ double s_dyn[];
+  double* s_grad = s_dyn;                 // [4L + 1]
+  double* s_warp = s_dyn + 4 * L + 1;     // [warps * 4]
+  const int ip = blockIdx.x / n_wtiles;
+  const int iw = (blockIdx.x % n_wtiles) * kDerThreads + threadIdx.x;
+  const bool valid = iw < n_w;
+  const int I = L - 1;
+  if (GRAD) {
+    for (int k = threadIdx.x; k < 4 * L + 1; k += blockDim.x) s_grad[k] = 0.0;
+    __syncthreads();
+  }
+  cd w = mk(0.0, 0.0);
+  if (valid) {
+    const double2 wv = omega[iw];
+    w = mk(wv.x, wv.y);
+  }
+  PairSink<GRAD> sink;
+  sink.L = L;
+  sink.ip = ip;
+  sink.iw = iw;
+  sink.n_w = n_w;
+  sink.valid = valid;
+  sink.R_obs = R_obs;
+  sink.R_out = R_out;
+  sink.J = J;
+  sink.s_grad = s_grad;
+  sink.s_warp = s_warp;
+  jacobian_pair(L, w, free_surface != 0, seg, lay_all + (size_t)ip * L,
+                dlay_all + (size_t)ip * L, coef_all + (size_t)ip * I, tan_all + (size_t)ip * I,
+                sink);
+  if (GRAD) {
+    const cd res = sink.res;
+    double c2 = valid ? (res.x * res.x + res.y * res.y) : 0.0;
+    for (int o = 16; o > 0; o >>= 1) c2 += __shfl_down_sync(0xffffffffu, c2, o);
+    if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = c2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int wi = 0; wi < kDerThreads / 32; ++wi) t += s_warp[wi];
+      s_grad[4 * L] = t;
+    }
+    __syncthreads();
+    double* dst = partial + (size_t)blockIdx.x * (4 * L + 1);
+    for (int k = threadIdx.x; k < 4 * L + 1; k += blockDim.x) dst[k] = s_grad[k];
+  }
+}
+
+__global__ void reduce_partials_kernel(const double* __restrict__ partial, int n_blocks, int n,
+                                       double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  double t = 0.0;
+  for (int b = 0; b < n_blocks; ++b) t += partial[(size_t)b * n + k];
+  out[k] = t;
+}
+
+template <bool GRAD>
+static kr_status launch_deriv(const double* layers, int L, const double* p, int n_p,
+                              const double* omega, int n_w, uint32_t flags, const double* R_obs,
+                              double* R, double* J, double* chi_grad, void* ws, size_t ws_bytes,
+                              cudaStream_t st) {
+  const int n_wtiles = (n_w + kDerThreads - 1) / kDerThreads;
+  const size_t n_blocks = (size_t)n_p * n_wtiles;
+  if (n_blocks > 0x7fffffffULL) return KR_ERR_TOO_LARGE;
+  DerivWs w = deriv_ws(ws, L, n_p, GRAD ? n_blocks : 0);
+  if (!ws || ws_bytes < w.bytes) return KR_ERR_WORKSPACE;
+  const int I = L - 1;
+  int nb = (n_p * L + 127) / 128;
+  deriv_layer_kernel<<<nb, 128, 0, st>>>(layers, L, p, n_p, w.lay, w.dlay);
+  kr_status s = check_launch("kr_deriv: layers");
+  if (s != KR_OK) return s;
+  nb = (n_p * I + 63) / 64;
+  deriv_iface_kernel<<<nb, 64, 0, st>>>(p, n_p, L, w.lay, w.dlay, w.coef, w.tan);
+  s = check_launch("kr_deriv: interfaces");
+  if (s != KR_OK) return s;
+  const int seg = checkpoint_spacing(I - 1 > 0 ? I - 1 : 1);
+  const size_t smem = sizeof(double) * ((size_t)4 * L + 1 + (kDerThreads / 32) * 4);
+  deriv_sweep_kernel<GRAD><<<(unsigned)n_blocks, kDerThreads, smem, st>>>(
+      L, p, n_p, reinterpret_cast<const double2*>(omega), n_w, n_wtiles,
+      (flags & KR_FREE_SURFACE) ? 1 : 0, seg, w.lay, w.dlay, w.coef, w.tan,
+      reinterpret_cast<const double2*>(R_obs), reinterpret_cast<double2*>(R),
+      reinterpret_cast<double2*>(J), w.partial);
+  s = check_launch("kr_deriv: sweep");
+  if (s != KR_OK || !GRAD) return s;
+  const int n = 4 * L + 1;
+  reduce_partials_kernel<<<(n + 127) / 128, 128, 0, st>>>(w.partial, (int)n_blocks, n, chi_grad);
+  return check_launch("kr_deriv: reduce");
+}
+
+static kr_status deriv_args(const double* layers, int L, const double* p, int n_p,
+                            const double* omega, int n_w, uint32_t flags) {
+  if (n_p < 0 || n_w < 0 || (flags & ~KR_FREE_SURFACE)) return KR_ERR_INVALID_ARGUMENT;
+  if (L < 2) return KR_ERR_INVALID_MODEL;
+  if (L > kMaxLayers) return KR_ERR_TOO_LARGE;
+  if (n_p > 0 && n_w > 0 && (!layers || !p || !omega)) return KR_ERR_INVALID_ARGUMENT;
+  return KR_OK;
+}
+
+}  // namespace kr
+
+using namespace kr;
+
+extern "C" size_t kr_jacobian_workspace_bytes(int32_t n_layers, int32_t n_p, int32_t n_w) {
+  if (n_layers < 2 || n_p <= 0 || n_w <= 0) return 0;
+  (void)n_w;
+  return deriv_ws(nullptr, n_layers, n_p, 0).bytes;
+}
+
+extern "C" kr_status kr_jacobian(const double* layers, int32_t n_layers, const double* p,
+                                 int32_t n_p, const double* omega, int32_t n_w, uint32_t flags,
+                                 double* R, double* J, void* workspace, size_t workspace_bytes,
+                                 void* stream) {
+  kr_status s = deriv_args(layers, n_layers, p, n_p, omega, n_w, flags);
+  if (s != KR_OK) return s;
+  if (n_p == 0 || n_w == 0) return KR_OK;
+  if (!J) return KR_ERR_INVALID_ARGUMENT;
+  return launch_deriv<false>(layers, n_layers, p, n_p, omega, n_w, flags, nullptr, R, J, nullptr,
+                             workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+extern "C" size_t kr_misfit_gradient_workspace_bytes(int32_t n_layers, int32_t n_p, int32_t n_w) {
+  if (n_layers < 2 || n_p <= 0 || n_w <= 0) return 0;
+  const size_t n_blocks = (size_t)n_p * ((n_w + kDerThreads - 1) / kDerThreads);
+  return deriv_ws(nullptr, n_layers, n_p, n_blocks).bytes;
+}
+
+extern "C" kr_status kr_misfit_gradient(const double* layers, int32_t n_layers, const double* p,
+                                        int32_t n_p, const double* omega, int32_t n_w,
+                                        uint32_t flags, const double* R_obs, double* R,
+                                        double* chi_grad, void* workspace,
+                                        size_t workspace_bytes, void* stream) {
+  kr_status s = deriv_args(layers, n_layers, p, n_p, omega, n_w, flags);
+  if (s != KR_OK) return s;
+  if (!chi_grad) return KR_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (n_p == 0 || n_w == 0) {
+    cudaError_t e = cudaMemsetAsync(chi_grad, 0, sizeof(double) * (4 * (size_t)n_layers + 1), st);
+    if (e != cudaSuccess) set_last_error("kr_misfit_gradient: memset", e);
+    return cuda_status(e);
+  }
+  if (!R_obs) return KR_ERR_INVALID_ARGUMENT;
+  return launch_deriv<true>(layers, n_layers, p, n_p, omega, n_w, flags, R_obs, R, nullptr,
+                            chi_grad, workspace, workspace_bytes, st);
+}

@@ -20,6 +20,9 @@ __all__ = [
     "reflectivity",
     "bessel_sum",
     "traces",
+    "jacobian",
+    "misfit_gradient",
+    "table_from_tensors",
     "stream_handle",
 ]
 
@@ -138,3 +141,65 @@ def traces(U: torch.Tensor, nw: int, S=None, decay=None,
                      ws.data_ptr(), ws_bytes, stream_handle(dev))
     _lib.check(st, "kr_traces")
     return out
+
+
+def jacobian(layers: torch.Tensor, p, omega, free_surface: bool = False,
+             want_R: bool = True):
+    """(R [n_p, n_w], J [n_p, 4L, n_w]) complex128 on the device: ``kr_jacobian``.
+
+    J[j, k*L + l, w] = dR(p_j, w) / d theta with theta = alpha_l, beta_l, rho_l, h_l (k = 0..3).
+    """
+    dev = layers.device
+    L = layers.shape[1]
+    p_t = _dev_f64(p, dev).reshape(-1)
+    w_t = _dev_c128(omega, dev).reshape(-1)
+    n_p, n_w = p_t.numel(), w_t.numel()
+    h = _lib.lib()
+    ws_bytes = h.kr_jacobian_workspace_bytes(L, n_p, n_w)
+    ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
+    R = torch.empty((n_p, n_w), dtype=torch.complex128, device=dev) if want_R else None
+    J = torch.empty((n_p, 4 * L, n_w), dtype=torch.complex128, device=dev)
+    flags = _lib.KR_FREE_SURFACE if free_surface else 0
+    st = h.kr_jacobian(layers.data_ptr(), L, p_t.data_ptr(), n_p, w_t.data_ptr(), n_w, flags,
+                       _ptr(R), J.data_ptr(), ws.data_ptr(), ws_bytes, stream_handle(dev))
+    _lib.check(st, "kr_jacobian")
+    return R, J
+
+
+def misfit_gradient(layers: torch.Tensor, p, omega, R_obs, free_surface: bool = False,
+                    want_R: bool = False):
+    """chi = sum |R - R_obs|^2 and d chi / d theta [4L] on the device: ``kr_misfit_gradient``.
+
+    Returns ``(chi_grad [4L + 1] float64 tensor (gradient then chi), R or None)``.
+    """
+    dev = layers.device
+    L = layers.shape[1]
+    p_t = _dev_f64(p, dev).reshape(-1)
+    w_t = _dev_c128(omega, dev).reshape(-1)
+    n_p, n_w = p_t.numel(), w_t.numel()
+    Ro = _dev_c128(R_obs, dev)
+    if Ro.shape != (n_p, n_w):
+        raise ValueError(f"R_obs must have shape ({n_p}, {n_w}), got {tuple(Ro.shape)}")
+    h = _lib.lib()
+    ws_bytes = h.kr_misfit_gradient_workspace_bytes(L, n_p, n_w)
+    ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
+    R = torch.empty((n_p, n_w), dtype=torch.complex128, device=dev) if want_R else None
+    out = torch.empty(4 * L + 1, dtype=torch.float64, device=dev)
+    flags = _lib.KR_FREE_SURFACE if free_surface else 0
+    st = h.kr_misfit_gradient(layers.data_ptr(), L, p_t.data_ptr(), n_p, w_t.data_ptr(), n_w,
+                              flags, Ro.data_ptr(), _ptr(R), out.data_ptr(), ws.data_ptr(),
+                              ws_bytes, stream_handle(dev))
+    _lib.check(st, "kr_misfit_gradient")
+    return out, R
+
+
+def table_from_tensors(alpha, beta, rho, thickness, Q_alpha, Q_beta, device) -> torch.Tensor:
+    """Layer table [6, L] on the device from six 1-D tensors (values only, no autograd)."""
+    rows = [torch.as_tensor(x).detach().to(device=device, dtype=torch.float64).reshape(-1)
+            for x in (alpha, beta, rho, thickness, Q_alpha, Q_beta)]
+    L = rows[0].numel()
+    if any(r.numel() != L for r in rows):
+        raise ValueError("alpha, beta, rho, thickness, Q_alpha, Q_beta must have equal length")
+    tab = torch.stack(rows).contiguous()
+    validate_table(tab.cpu().numpy())
+    return tab

@@ -1,0 +1,280 @@
+"""Drop-in for ``Kennett_Reflectivity.kennett_torch`` (``kennett_torch.py:312-725``).
+
+``kennett_reflectivity_torch`` keeps the reference signature and returns the same complex128
+R(omega), differentiable with respect to ``alpha, beta, rho, thickness``: the forward and its
+Jacobian come from the hand-written adjoint kernel (``kr_jacobian``), wrapped in a
+``torch.autograd.Function`` whose backward / jvp are plain tensor contractions with that
+Jacobian, so ``backward()``, ``torch.autograd.grad``, ``torch.func.jacrev`` / ``jacfwd`` /
+``vjp`` / ``jvp`` all work.  Second derivatives through the Function treat the Jacobian as
+constant, so ``torch.func.hessian`` of a misfit built on it gives the Gauss-Newton matrix
+2 Re(J^H J); ``hessian()`` below gives the full Hessian (central differences of the exact
+adjoint gradient).  ``Q_alpha``, ``Q_beta``, ``p`` and ``omega`` are constants (no gradient).
+
+Inputs may live on the CPU (as in the reference) or on a CUDA device; the result is returned
+on ``omega``'s device.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import device as D
+from .layer_model import LayerModel
+
+__all__ = [
+    "kennett_reflectivity_torch",
+    "forward_model_torch",
+    "jacobian",
+    "hessian",
+    "model_to_tensors",
+    "misfit_gradient_packed",
+]
+
+_CDTYPE = torch.complex128
+_FDTYPE = torch.float64
+
+
+def _device_for(*tensors) -> torch.device:
+    for t in tensors:
+        if isinstance(t, torch.Tensor) and t.is_cuda:
+            return D.require_cuda(t.device)
+    return D.require_cuda()
+
+
+def _compute(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface, need_jac):
+    """R (and J if ``need_jac``) for the given layer arrays, on the compute device.
+
+    Returns ``(R [n_p, n_w], J [n_p, 4L, n_w] or None)``.
+    """
+    dev = _device_for(alpha, omega)
+    tab = D.table_from_tensors(alpha, beta, rho, thickness, Q_alpha, Q_beta, dev)
+    p_t = torch.as_tensor(p, dtype=_FDTYPE).detach().reshape(-1)
+    w = torch.as_tensor(omega).detach()
+    if need_jac:
+        return D.jacobian(tab, p_t, w, free_surface)
+    return D.reflectivity(tab, p_t, w, free_surface), None
+
+
+class _KennettFunction(torch.autograd.Function):
+    """R(alpha, beta, rho, thickness) with the adjoint-kernel Jacobian as its derivative."""
+
+    @staticmethod
+    def forward(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface, need_jac):
+        R, J = _compute(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface,
+                        need_jac)
+        out_dev = omega.device
+        L = alpha.shape[0]
+        if J is None:
+            J = torch.zeros((R.shape[0], 4 * L, R.shape[1]), dtype=_CDTYPE, device=R.device)
+        R, J = R.to(out_dev), J.to(out_dev)
+        if torch.as_tensor(p).dim() == 0:
+            R, J = R[0], J[0]
+        return R, J
+
+    @staticmethod
+    def setup_context(ctx, inputs, output):
+        _, J = output
+        ctx.mark_non_differentiable(J)
+        ctx.save_for_backward(J)
+        ctx.save_for_forward(J)
+        ctx.L = inputs[0].shape[0]
+        ctx.dtypes = [x.dtype for x in inputs[:4]]
+
+    @staticmethod
+    def backward(ctx, gR, gJ):
+        (J,) = ctx.saved_tensors
+        L = ctx.L
+        # d loss / d theta = Re(sum_w conj(gR[w]) J[theta, w])  (PyTorch complex convention)
+        g = (gR.conj().unsqueeze(-2) * J).real.sum(-1)
+        if g.dim() > 1:
+            g = g.sum(-2)
+        ga, gb, gr, gh = (g[..., k * L:(k + 1) * L].to(ctx.dtypes[k]) for k in range(4))
+        return ga, gb, gr, gh, None, None, None, None, None, None
+
+    @staticmethod
+    def vmap(info, in_dims, alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega,
+             free_surface, need_jac):
+        # One evaluation per batch element (each is one kernel launch over all p and omega).
+        args = (alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega)
+        Rs, Js = [], []
+        for b in range(info.batch_size):
+            sl = [x if d is None else x.select(d, b) for x, d in zip(args, in_dims[:8])]
+            R, J = _KennettFunction.apply(*sl, free_surface, need_jac)
+            Rs.append(R)
+            Js.append(J)
+        return (torch.stack(Rs), torch.stack(Js)), (0, 0)
+
+    @staticmethod
+    def jvp(ctx, ta, tb, tr, th, tqa, tqb, tp, tw, tfs, tneed):
+        (J,) = ctx.saved_tensors
+        L = ctx.L
+        parts = []
+        for t in (ta, tb, tr, th):
+            parts.append(torch.zeros(L, dtype=_FDTYPE, device=J.device) if t is None
+                         else t.to(device=J.device, dtype=_FDTYPE))
+        t = torch.cat(parts).to(_CDTYPE)
+        dR = (J * t.unsqueeze(-1)).sum(-2)
+        return dR, None
+
+
+def _needs_grad(*tensors) -> bool:
+    """Whether any layer input carries reverse- or forward-mode derivative information."""
+    for t in tensors:
+        if not isinstance(t, torch.Tensor):
+            continue
+        if t.requires_grad and torch.is_grad_enabled():
+            return True
+        if torch._C._functorch.is_functorch_wrapped_tensor(t):
+            return True
+        try:
+            if torch.autograd.forward_ad.unpack_dual(t).tangent is not None:
+                return True
+        except RuntimeError:
+            pass
+    return False
+
+
+def kennett_reflectivity_torch(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega,
+                               free_surface: bool = False):
+    """Complex PP reflectivity (nfreq,) -- ``kennett_torch.py:312-480`` signature.
+
+    ``p`` may also be a 1-D tensor of slownesses, giving R of shape (n_p, nfreq) in one
+    launch.  The half-space may be marked by a thickness >= 1e30 (the reference's sentinel) or
+    +inf.
+    """
+    if not isinstance(omega, torch.Tensor):
+        omega = torch.as_tensor(omega)
+    need = _needs_grad(alpha, beta, rho, thickness)
+    R, _ = _KennettFunction.apply(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega,
+                                  bool(free_surface), need)
+    return R
+
+
+def forward_model_torch(alpha, beta, rho, thickness, Q_alpha, Q_beta, p: float, T: float = 64.0,
+                        nw: int = 2048, free_surface: bool = False):
+    """``(time, seismogram)`` (``kennett_torch.py:488-544``): R x Ricker, Hermitian FFT.
+
+    R is differentiable (adjoint kernel); the spectrum assembly and FFT are torch ops on the
+    result's device.
+    """
+    dw = 2.0 * np.pi / T
+    nwm = nw - 1
+    wmax = nw * dw
+    dev = alpha.device if isinstance(alpha, torch.Tensor) else torch.device("cpu")
+    omega = torch.arange(1, nwm + 1, dtype=_FDTYPE, device=dev) * dw
+    a = 0.1 * wmax
+    t0 = 5.0 / (a * (2.0**0.5))
+    Z = (omega**2) / (4.0 * a**2)
+    S = Z * torch.exp(-Z + 1j * omega * t0)
+    R = kennett_reflectivity_torch(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega,
+                                   free_surface=free_surface)
+    Y = R * S
+    nt = 2 * nw
+    Uwk = torch.cat([torch.zeros(1, dtype=_CDTYPE, device=dev), Y,
+                     torch.zeros(1, dtype=_CDTYPE, device=dev), torch.conj(torch.flip(Y, [0]))])
+    time = torch.arange(nt, dtype=_FDTYPE, device=dev) * (T / float(nt))
+    return time, torch.fft.fft(Uwk).real
+
+
+# ---------------------------------------------------------------------------------------
+# Packed sub-ocean parameters (kennett_torch.py:552-608)
+# ---------------------------------------------------------------------------------------
+
+def _pack_params(alpha, beta, rho, thickness):
+    """m = [Vp_1..N, Vs_1..N, rho_1..N, h_1..N-1] (ocean and half-space thickness excluded)."""
+    return torch.cat([alpha[1:], beta[1:], rho[1:], thickness[1:-1]])
+
+
+def _unpack_params(params, alpha_full, beta_full, rho_full, thickness_full):
+    n_sub = alpha_full.shape[0] - 1
+    n_thick = n_sub - 1
+    a = params[:n_sub]
+    b = params[n_sub:2 * n_sub]
+    r = params[2 * n_sub:3 * n_sub]
+    h = params[3 * n_sub:3 * n_sub + n_thick]
+    return (torch.cat([alpha_full[:1].detach(), a]), torch.cat([beta_full[:1].detach(), b]),
+            torch.cat([rho_full[:1].detach(), r]),
+            torch.cat([thickness_full[:1].detach(), h, thickness_full[-1:].detach()]))
+
+
+def packed_index(L: int) -> list[int]:
+    """Rows of the full [4L] layer-parameter vector that form the packed vector."""
+    return ([0 * L + l for l in range(1, L)] + [1 * L + l for l in range(1, L)]
+            + [2 * L + l for l in range(1, L)] + [3 * L + l for l in range(1, L - 1)])
+
+
+def jacobian(alpha, beta, rho, thickness, Q_alpha, Q_beta, p: float, omega,
+             free_surface: bool = False) -> torch.Tensor:
+    """dR(omega_i)/dm_j, shape (nfreq, 4N-1) complex (``kennett_torch.py:611-641``).
+
+    One launch of the adjoint kernel (the reference runs jacrev twice, for Re and Im).
+    Returned on ``omega``'s device.
+    """
+    omega = torch.as_tensor(omega)
+    _, J = _compute(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface, True)
+    L = torch.as_tensor(alpha).shape[0]
+    Jp = J[0][packed_index(L)].transpose(0, 1).contiguous()
+    return Jp.to(omega.device)
+
+
+def misfit_gradient_packed(params, alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega,
+                           R_obs, free_surface: bool = False):
+    """(chi, d chi / d m) for packed parameters m, all slownesses ``p`` in one launch.
+
+    chi = sum_{p, w} |R - R_obs|^2; ``R_obs`` has shape (n_p, n_w) (or (n_w,) for one p).
+    Returns ``(chi float, grad float64 tensor on the compute device)``.
+    """
+    a, b, r, h = _unpack_params(torch.as_tensor(params, dtype=_FDTYPE).detach().cpu(),
+                                *(torch.as_tensor(x, dtype=_FDTYPE).cpu() for x in
+                                  (alpha, beta, rho, thickness)))
+    dev = _device_for(omega, R_obs)
+    tab = D.table_from_tensors(a, b, r, h, Q_alpha, Q_beta, dev)
+    p_t = torch.as_tensor(p, dtype=_FDTYPE).reshape(-1)
+    Ro = torch.as_tensor(R_obs).reshape(p_t.numel(), -1)
+    out, _ = D.misfit_gradient(tab, p_t, torch.as_tensor(omega), Ro, free_surface)
+    L = a.shape[0]
+    return float(out[4 * L]), out[packed_index(L)]
+
+
+def hessian(alpha, beta, rho, thickness, Q_alpha, Q_beta, p: float, omega, R_obs=None,
+            free_surface: bool = False, step: float = 1e-5) -> torch.Tensor:
+    """Hessian of chi = ||R - R_obs||^2 over the packed parameters (``kennett_torch.py:644-684``).
+
+    Column j is the central difference of the exact adjoint gradient with a relative step
+    ``step`` in m_j; the result is symmetrised.  Accuracy ~1e-8 relative (the reference
+    uses torch.func.hessian).  Returned on ``omega``'s device as float64 (n_params, n_params).
+    """
+    omega = torch.as_tensor(omega)
+    if R_obs is None:
+        R_obs = torch.zeros(omega.shape[0], dtype=_CDTYPE)
+    m0 = _pack_params(*(torch.as_tensor(x, dtype=_FDTYPE).detach().cpu()
+                        for x in (alpha, beta, rho, thickness)))
+    P = m0.numel()
+    H = torch.empty((P, P), dtype=_FDTYPE)
+    for j in range(P):
+        d = step * max(abs(float(m0[j])), 1e-3)
+        mp, mm = m0.clone(), m0.clone()
+        mp[j] += d
+        mm[j] -= d
+        _, gp = misfit_gradient_packed(mp, alpha, beta, rho, thickness, Q_alpha, Q_beta, p,
+                                       omega, R_obs, free_surface)
+        _, gm = misfit_gradient_packed(mm, alpha, beta, rho, thickness, Q_alpha, Q_beta, p,
+                                       omega, R_obs, free_surface)
+        H[:, j] = ((gp - gm) / (2.0 * d)).cpu()
+    H = 0.5 * (H + H.T)
+    return H.to(omega.device)
+
+
+def model_to_tensors(model: LayerModel, requires_grad: bool = False) -> dict:
+    """Dict of float64 tensors; half-space thickness -> 1e30 (``kennett_torch.py:692-725``)."""
+    thick = model.thickness.copy()
+    thick[np.isinf(thick)] = 1e30
+    out = {}
+    for name, arr in [("alpha", model.alpha), ("beta", model.beta), ("rho", model.rho),
+                      ("thickness", thick), ("Q_alpha", model.Q_alpha), ("Q_beta", model.Q_beta)]:
+        t = torch.tensor(arr, dtype=_FDTYPE)
+        if requires_grad and name in ("alpha", "beta", "rho", "thickness"):
+            t.requires_grad_(True)
+        out[name] = t
+    return out

@@ -1,0 +1,207 @@
+"""Parity of the derivative path: kr_jacobian / kr_misfit_gradient and the torch drop-ins.
+
+References: the reference's torch.func.jacrev ``jacobian`` and ``hessian`` and its
+``invert_taup`` run (golden vectors), plus central finite differences of the oracle.
+Tolerances: Jacobian vs jacrev 1e-10 relative (both exact derivatives); gradient vs the
+Jacobian contraction 1e-12; vs finite differences 1e-6; Hessian (central differences of the
+exact gradient) vs torch.func.hessian 1e-6.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_err
+from oracle import kennett_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _m(g):
+    from seismicinversion_b200.layer_model import LayerModel
+
+    return LayerModel(*[g[k] for k in ("alpha", "beta", "rho", "thickness", "Q_alpha", "Q_beta")])
+
+
+def _tensors(m):
+    from seismicinversion_b200.kennett_torch import model_to_tensors
+
+    return model_to_tensors(m)
+
+
+@pytest.mark.parametrize("p", [0.2, 0.4])
+@pytest.mark.parametrize("fs", [False, True])
+def test_jacobian_vs_reference_jacrev(golden, p, fs):
+    from seismicinversion_b200.earth_models import default_ocean_crust_model
+    from seismicinversion_b200.kennett_torch import jacobian
+
+    g = golden("derivs_default.npz")
+    t = _tensors(default_ocean_crust_model())
+    J = jacobian(t["alpha"], t["beta"], t["rho"], t["thickness"], t["Q_alpha"], t["Q_beta"], p,
+                 torch.as_tensor(g["omega"]), free_surface=fs)
+    assert J.shape == (32, 14) and J.device.type == "cpu"
+    assert rel_err(J.numpy(), g[f"J_p{p}_fs{int(fs)}"]) < 1e-10
+    if not fs:
+        assert rel_err(J.numpy(), g[f"F_p{p}"]) < 1e-10  # analytical Frechet as well
+
+
+def test_jacobian_21_layers_and_torch_forward(golden):
+    from seismicinversion_b200.kennett_torch import jacobian, kennett_reflectivity_torch
+
+    g = golden("derivs_c2.npz")
+    t = _tensors(_m(g))
+    for p in (0.05, 0.3):
+        R = kennett_reflectivity_torch(**t, p=p, omega=torch.as_tensor(g["omega"]))
+        assert rel_err(R.numpy(), g[f"R_p{p}"]) < 1e-10
+        J = jacobian(t["alpha"], t["beta"], t["rho"], t["thickness"], t["Q_alpha"], t["Q_beta"],
+                     p, torch.as_tensor(g["omega"]))
+        assert J.shape == (64, 79)
+        assert rel_err(J.numpy(), g[f"J_p{p}"]) < 1e-10
+    w1024 = torch.arange(1, 1025, dtype=torch.float64) * (2 * np.pi / 64)
+    R = kennett_reflectivity_torch(**t, p=0.3, omega=w1024)
+    assert rel_err(R.numpy(), g["R1024_p0.3"]) < 1e-10
+
+
+def test_autograd_and_func_jacrev_through_function(golden):
+    from seismicinversion_b200.earth_models import default_ocean_crust_model
+    from seismicinversion_b200.kennett_torch import (
+        _pack_params,
+        _unpack_params,
+        kennett_reflectivity_torch,
+        model_to_tensors,
+    )
+
+    g = golden("derivs_default.npz")
+    t = model_to_tensors(default_ocean_crust_model(), requires_grad=True)
+    w = torch.as_tensor(g["omega"])
+    R = kennett_reflectivity_torch(**t, p=0.2, omega=w)
+    loss = (R.real**2 + R.imag**2).sum()
+    loss.backward()
+    Jg = g["J_p0.2_fs0"]  # packed: alpha_1..4, beta_1..4, rho_1..4, h_1..3
+    grad_ref = 2 * (R.detach().numpy().conj()[:, None] * Jg).real.sum(0)
+    got = np.concatenate([t["alpha"].grad[1:], t["beta"].grad[1:], t["rho"].grad[1:],
+                          t["thickness"].grad[1:-1]])
+    assert rel_err(got, grad_ref) < 1e-10
+    # torch.func.jacrev through the Function, as the reference's jacobian() does it
+    t2 = model_to_tensors(default_ocean_crust_model())
+    m0 = _pack_params(t2["alpha"], t2["beta"], t2["rho"], t2["thickness"])
+
+    def f(m):
+        a, b, r, h = _unpack_params(m, t2["alpha"], t2["beta"], t2["rho"], t2["thickness"])
+        return kennett_reflectivity_torch(a, b, r, h, t2["Q_alpha"], t2["Q_beta"], 0.2, w)
+
+    Jr = torch.func.jacrev(lambda m: f(m).real)(m0) + 1j * torch.func.jacrev(lambda m: f(m).imag)(m0)
+    assert rel_err(Jr.numpy(), Jg) < 1e-10
+
+
+def test_misfit_gradient_vs_jacobian_and_fd():
+    from seismicinversion_b200 import device as D
+    from seismicinversion_b200.earth_models import random_layered_model
+
+    m = random_layered_model(6, seed=21)
+    L = m.n_layers
+    tab = D.layer_table(m)
+    p = np.array([0.05, 0.22, 0.41, 0.7])
+    w = np.arange(1, 300) * (2 * np.pi / 64) + 1j * (np.pi / 64)
+    for fs in (False, True):
+        R_true = O.reflectivity(m.alpha, m.beta, m.rho, m.thickness, m.Q_alpha, m.Q_beta, p, w, fs)
+        R_obs = R_true * (1 + 0.03 * np.cos(np.arange(w.size)))[None, :]
+        out, R = D.misfit_gradient(tab, p, w, R_obs, fs, want_R=True)
+        out = out.cpu().numpy()
+        Rg, J = D.jacobian(tab, p, w, fs)
+        r = Rg.cpu().numpy() - R_obs
+        g_ref = 2 * (r.conj()[:, None, :] * J.cpu().numpy()).real.sum(axis=(0, 2))
+        assert rel_err(out[:4 * L], g_ref) < 1e-12
+        assert abs(out[4 * L] - O.misfit(R_true, R_obs)) / O.misfit(R_true, R_obs) < 1e-10
+        assert rel_err(R.cpu().numpy(), R_true) < 1e-10
+        # central differences of the oracle misfit on a few parameters
+        base = [m.alpha, m.beta, m.rho, m.thickness]
+        for k, l in [(0, 1), (1, 3), (2, 5), (3, 2), (0, 0), (2, 0), (3, 0)]:
+            arrs = [b.copy() for b in base]
+            d = 1e-6 * arrs[k][l]
+            arrs[k][l] += d
+            cp = O.misfit(O.reflectivity(*arrs, m.Q_alpha, m.Q_beta, p, w, fs), R_obs)
+            arrs[k][l] -= 2 * d
+            cm = O.misfit(O.reflectivity(*arrs, m.Q_alpha, m.Q_beta, p, w, fs), R_obs)
+            fd = (cp - cm) / (2 * d)
+            assert abs(out[k * L + l] - fd) / (np.max(np.abs(out[:4 * L])) + 1e-300) < 1e-6, (k, l)
+
+
+def test_gradient_inversion_size_64p_1024w():
+    """21-layer inversion model, 64 slownesses x 1024 frequencies in one launch: gradient
+    entries vs central differences of the oracle misfit (subset of 8 slownesses for the
+    FD cost), and the full-size gradient vs the Jacobian contraction."""
+    from seismicinversion_b200 import device as D
+    from seismicinversion_b200.earth_models import random_layered_model
+
+    true = random_layered_model(20, seed=2)
+    rng = np.random.default_rng(2)
+    start = random_layered_model(20, seed=2)
+    for name in ("alpha", "beta", "rho"):
+        getattr(start, name)[1:] *= np.exp(0.1 * rng.standard_normal(20))
+    start.thickness[1:-1] *= np.exp(0.1 * rng.standard_normal(19))
+    L = true.n_layers
+    p = np.linspace(0.05, 0.6, 64)
+    w = np.arange(1, 1025) * (2 * np.pi / 64)
+    tab_true, tab = D.layer_table(true), D.layer_table(start)
+    R_obs = D.reflectivity(tab_true, p, w)
+    out, _ = D.misfit_gradient(tab, p, w, R_obs)
+    Rg, J = D.jacobian(tab, p, w)
+    r = Rg - R_obs
+    g_ref = (2 * (r.conj()[:, None, :] * J).real.sum(dim=(0, 2))).cpu().numpy()
+    out = out.cpu().numpy()
+    assert rel_err(out[:4 * L], g_ref) < 1e-12
+    sub = np.arange(0, 64, 8)
+    out_s, _ = D.misfit_gradient(tab, p[sub], w, R_obs[sub])
+    out_s = out_s.cpu().numpy()
+    Ro = R_obs[sub].cpu().numpy()
+    base = [start.alpha, start.beta, start.rho, start.thickness]
+    for k, l in [(0, 3), (1, 10), (2, 17), (3, 8)]:
+        arrs = [b.copy() for b in base]
+        d = 1e-6 * arrs[k][l]
+        arrs[k][l] += d
+        cp = O.misfit(O.reflectivity(*arrs, start.Q_alpha, start.Q_beta, p[sub], w), Ro)
+        arrs[k][l] -= 2 * d
+        cm = O.misfit(O.reflectivity(*arrs, start.Q_alpha, start.Q_beta, p[sub], w), Ro)
+        fd = (cp - cm) / (2 * d)
+        assert abs(out_s[k * L + l] - fd) / np.max(np.abs(out_s[:4 * L])) < 1e-6, (k, l)
+
+
+def test_hessian_vs_reference(golden):
+    from seismicinversion_b200.earth_models import default_ocean_crust_model
+    from seismicinversion_b200.kennett_torch import hessian, model_to_tensors
+
+    g = golden("derivs_default.npz")
+    t = model_to_tensors(default_ocean_crust_model())
+    a = t["alpha"].clone()
+    a[1] *= 1.02
+    H = hessian(a, t["beta"], t["rho"], t["thickness"], t["Q_alpha"], t["Q_beta"], 0.2,
+                torch.as_tensor(g["omega"]), R_obs=torch.as_tensor(g["R_obs_p0.2"]))
+    assert rel_err(H.numpy(), g["H_p0.2_alpha1x1.02"]) < 1e-6
+
+
+def test_invert_taup_matches_reference_run(golden):
+    from seismicinversion_b200.earth_models import default_ocean_crust_model
+    from seismicinversion_b200.taup_inversion import invert_taup
+
+    g = golden("invert_small.npz")
+    res = invert_taup(default_ocean_crust_model(), [0.1, 0.2, 0.3, 0.4], nfreq=32,
+                      perturbation=0.05, max_iter=30)
+    assert res.converged and res.param_error_history[-1] < 1e-3
+    assert np.allclose(res.initial_model.alpha, g["init_alpha"], rtol=1e-14)
+    n = min(5, len(res.misfit_history), len(g["misfit"]))
+    # identical start; the first LM iterates agree closely (exact vs finite-difference Hessian)
+    assert abs(res.misfit_history[0] - g["misfit"][0]) / g["misfit"][0] < 1e-10
+    for k in range(1, n):
+        assert abs(res.param_error_history[k] - g["param_err"][k]) <= 1e-3 * g["param_err"][0]
+    assert np.allclose(res.recovered_model.alpha, g["rec_alpha"], rtol=1e-5)
+    assert np.allclose(res.recovered_model.thickness[:-1], g["rec_thickness"][:-1], rtol=1e-5)
+
+
+def test_invert_taup_gauss_newton_converges():
+    from seismicinversion_b200.earth_models import default_ocean_crust_model
+    from seismicinversion_b200.taup_inversion import invert_taup
+
+    res = invert_taup(default_ocean_crust_model(), [0.1, 0.2, 0.3, 0.4], nfreq=32,
+                      perturbation=0.02, max_iter=20, hessian="gauss-newton")
+    assert res.converged and res.param_error_history[-1] < 1e-6

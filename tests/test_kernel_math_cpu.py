@@ -73,3 +73,84 @@ def test_random_depths(emu):
         R = emu(m, p, w, True)
         Ro = O.reflectivity(m.alpha, m.beta, m.rho, m.thickness, m.Q_alpha, m.Q_beta, p, w, True)
         assert rel_err(R, Ro) < 1e-10
+
+
+@pytest.fixture(scope="module")
+def emu_jac(emu, tmp_path_factory):
+    import glob
+
+    so = sorted(glob.glob(str(tmp_path_factory.getbasetemp() / "emu*" / "libkr_emulate.so")))[-1]
+    lib = ctypes.CDLL(so)
+
+    def run(model, p, omega, fs=False):
+        from seismicinversion_b200.layer_model import pack_layers
+
+        tab = np.ascontiguousarray(pack_layers(model))
+        L = model.n_layers
+        p = np.ascontiguousarray(np.atleast_1d(p), dtype=np.float64)
+        w = np.ascontiguousarray(np.asarray(omega, dtype=np.complex128))
+        R = np.zeros((len(p), len(w)), dtype=np.complex128)
+        J = np.zeros((len(p), 4 * L, len(w)), dtype=np.complex128)
+        lib.emu_jacobian(ctypes.c_void_p(tab.ctypes.data), L, ctypes.c_void_p(p.ctypes.data),
+                         len(p), ctypes.c_void_p(w.ctypes.data), len(w), int(fs),
+                         ctypes.c_void_p(R.ctypes.data), ctypes.c_void_p(J.ctypes.data))
+        return R, J
+
+    return run
+
+
+def packed(J, L):
+    """Full [4L] layer-parameter Jacobian -> the reference's packed sub-ocean order
+    [alpha_1..N, beta_1..N, rho_1..N, h_1..N-1] (kennett_torch.py:552-571)."""
+    idx = [0 * L + l for l in range(1, L)] + [1 * L + l for l in range(1, L)] + \
+          [2 * L + l for l in range(1, L)] + [3 * L + l for l in range(1, L - 1)]
+    return np.moveaxis(J[..., idx, :], -1, -2)
+
+
+@pytest.mark.parametrize("p", [0.2, 0.4])
+@pytest.mark.parametrize("fs", [0, 1])
+def test_adjoint_vs_reference_jacrev(emu_jac, golden, p, fs):
+    from seismicinversion_b200.earth_models import default_ocean_crust_model
+
+    g = golden("derivs_default.npz")
+    m = default_ocean_crust_model()
+    R, J = emu_jac(m, p, g["omega"], fs)
+    Jp = packed(J, m.n_layers)[0]
+    assert rel_err(Jp, g[f"J_p{p}_fs{fs}"]) < 1e-10
+
+
+def test_adjoint_vs_reference_jacrev_21_layers(emu_jac, golden):
+    g = golden("derivs_c2.npz")
+    from seismicinversion_b200.layer_model import LayerModel
+
+    m = LayerModel(*[g[k] for k in ("alpha", "beta", "rho", "thickness", "Q_alpha", "Q_beta")])
+    for p in (0.05, 0.3):
+        R, J = emu_jac(m, p, g["omega"])
+        assert rel_err(R[0], g[f"R_p{p}"]) < 1e-12
+        assert rel_err(packed(J, m.n_layers)[0], g[f"J_p{p}"]) < 1e-10
+
+
+def test_adjoint_vs_fd_all_parameters(emu_jac):
+    """Every layer parameter incl. the ocean's alpha, rho, h, damped frequencies, free surface."""
+    from seismicinversion_b200.earth_models import random_layered_model
+
+    m = random_layered_model(4, seed=11)
+    L = m.n_layers
+    w = np.arange(1, 40) * 0.2 + 0.03j
+    p = np.array([0.15, 0.5])
+    for fs in (0, 1):
+        R, J = emu_jac(m, p, w, fs)
+        base = [m.alpha, m.beta, m.rho, m.thickness]
+        for k in range(4):
+            for l in range(L):
+                if (k == 1 and l == 0) or (k == 3 and l == L - 1):
+                    assert np.all(J[:, k * L + l] == 0)
+                    continue
+                arrs = [b.copy() for b in base]
+                d = 1e-6 * arrs[k][l]
+                arrs[k][l] += d
+                Rp = O.reflectivity(*arrs, m.Q_alpha, m.Q_beta, p, w, bool(fs))
+                arrs[k][l] -= 2 * d
+                Rm = O.reflectivity(*arrs, m.Q_alpha, m.Q_beta, p, w, bool(fs))
+                fd = (Rp - Rm) / (2 * d)
+                assert rel_err(J[:, k * L + l], fd) < 1e-6, (fs, k, l, rel_err(J[:, k * L + l], fd))

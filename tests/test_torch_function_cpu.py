@@ -1,0 +1,87 @@
+"""Autograd / torch.func plumbing of the kennett_reflectivity_torch Function, on the CPU.
+
+The device computation is replaced by an analytic stand-in with a known Jacobian (test-only
+monkeypatch of ``_compute``), so the routing of gradients, jacrev / jacfwd, vjp / jvp and the
+Gauss-Newton behaviour of torch.func.hessian are checked without a GPU.  The GPU tests check
+the real kernel through the same Function.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import seismicinversion_b200.kennett_torch as KT
+
+
+def _fake_compute(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface, need_jac):
+    # R(w) = sum_k sum_l c[k, l](w) * x_k[l]^2  (nonlinear, known derivative)
+    xs = [torch.as_tensor(t, dtype=torch.float64).detach() for t in (alpha, beta, rho, thickness)]
+    L = xs[0].shape[0]
+    w = torch.as_tensor(omega).detach().to(torch.complex128)
+    p_t = torch.as_tensor(p, dtype=torch.float64).reshape(-1)
+    R = torch.zeros((p_t.numel(), w.numel()), dtype=torch.complex128)
+    J = torch.zeros((p_t.numel(), 4 * L, w.numel()), dtype=torch.complex128)
+    for j, pj in enumerate(p_t):
+        for k, x in enumerate(xs):
+            for l in range(L):
+                c = torch.exp(1j * w * (0.1 * (l + 1) + 0.01 * k)) * (1 + pj)
+                R[j] += c * x[l] ** 2
+                J[j, k * L + l] = c * 2 * x[l]
+    return R, (J if need_jac else None)
+
+
+@pytest.fixture
+def fake(monkeypatch):
+    monkeypatch.setattr(KT, "_compute", _fake_compute)
+
+
+def _model():
+    t = KT.model_to_tensors(
+        __import__("seismicinversion_b200.earth_models", fromlist=["x"]).random_layered_model(3, 1))
+    return t
+
+
+def test_backward_matches_jacobian(fake):
+    t = _model()
+    for k in ("alpha", "beta", "rho", "thickness"):
+        t[k] = t[k].clone().requires_grad_(True)
+    t["thickness"] = t["thickness"].detach().clone()
+    t["thickness"][-1] = 5.0
+    t["thickness"].requires_grad_(True)
+    w = torch.arange(1, 9, dtype=torch.float64) * 0.5
+    R = KT.kennett_reflectivity_torch(**t, p=0.2, omega=w)
+    loss = (R.real**2 + R.imag**2).sum()
+    loss.backward()
+    Rf, J = _fake_compute(t["alpha"], t["beta"], t["rho"], t["thickness"], 0, 0, 0.2, w, False, True)
+    L = t["alpha"].shape[0]
+    g = (2 * Rf[0].conj().unsqueeze(0) * J[0]).real.sum(-1)
+    for k, name in enumerate(("alpha", "beta", "rho", "thickness")):
+        assert torch.allclose(t[name].grad, g[k * L:(k + 1) * L], rtol=1e-12, atol=1e-12)
+
+
+def test_jacrev_jacfwd_and_gauss_newton_hessian(fake):
+    t = _model()
+    w = torch.arange(1, 6, dtype=torch.float64) * 0.3
+    m0 = KT._pack_params(t["alpha"], t["beta"], t["rho"], t["thickness"])
+
+    def f(m):
+        a, b, r, h = KT._unpack_params(m, t["alpha"], t["beta"], t["rho"], t["thickness"])
+        return KT.kennett_reflectivity_torch(a, b, r, h, t["Q_alpha"], t["Q_beta"], 0.3, w)
+
+    _, J = _fake_compute(*KT._unpack_params(m0, t["alpha"], t["beta"], t["rho"], t["thickness"]),
+                         0, 0, 0.3, w, False, True)
+    L = t["alpha"].shape[0]
+    Jp = J[0][KT.packed_index(L)].T  # (nw, P)
+    Jr = torch.func.jacrev(lambda m: f(m).real)(m0) + 1j * torch.func.jacrev(lambda m: f(m).imag)(m0)
+    assert torch.allclose(Jr, Jp, rtol=1e-12, atol=1e-12)
+    Jf = torch.func.jacfwd(lambda m: torch.view_as_real(f(m)))(m0)
+    assert torch.allclose(Jf[..., 0, :] + 1j * Jf[..., 1, :], Jp, rtol=1e-12, atol=1e-12)
+    R_obs = f(m0).detach() * 0.9
+
+    def chi(m):
+        r = f(m) - R_obs
+        return (r.real**2 + r.imag**2).sum()
+
+    H = torch.func.hessian(chi)(m0)
+    H_gn = 2 * (Jp.conj().T @ Jp).real
+    assert torch.allclose(H, H_gn, rtol=1e-10, atol=1e-10)
