@@ -39,7 +39,7 @@ def test_jacobian_vs_reference_jacrev(golden, p, fs):
     t = _tensors(default_ocean_crust_model())
     J = jacobian(t["alpha"], t["beta"], t["rho"], t["thickness"], t["Q_alpha"], t["Q_beta"], p,
                  torch.as_tensor(g["omega"]), free_surface=fs)
-    assert J.shape == (32, 14) and J.device.type == "cpu"
+    assert J.shape == (32, 15) and J.device.type == "cpu"
     assert rel_err(J.numpy(), g[f"J_p{p}_fs{int(fs)}"]) < 1e-10
     if not fs:
         assert rel_err(J.numpy(), g[f"F_p{p}"]) < 1e-10  # analytical Frechet as well
