@@ -175,6 +175,90 @@ kr_status kr_traces(const double* U, const double* S, int32_t n_r, int32_t nw,
                     const double* decay, double* traces, void* workspace,
                     size_t workspace_bytes, void* stream);
 
+/* ------------------------------------------------------------------------------------- *
+ * Batched evaluation of many models of uneven size (no single reference counterpart: the
+ * reference evaluates one model per call -- kennett_reflectivity / kennett_reflectivity_torch
+ * -- and the batch replaces loops of those calls, e.g. the per-slowness loops of
+ * taup_misfit_grad_hessian, Kennett_Reflectivity/taup_inversion.py:153-178).
+ * ------------------------------------------------------------------------------------- */
+
+#define KR_BATCH_GRADIENT 0x2u  /* model asks for chi and d chi / d(alpha, beta, rho, h)     */
+#define KR_BATCH_STORE_R 0x4u   /* gradient model also writes its R grid                      */
+
+/* One model of a batch.  Offsets index caller-owned packed device buffers:
+ *   layers_off : doubles into `layers` (the model's [6][n_layers] table)
+ *   p_off      : doubles into `p`;  omega_off : complex elements into `omega`
+ *   R_off      : complex elements into `R` ([n_p][n_w], forward models and KR_BATCH_STORE_R)
+ *   obs_off    : complex elements into `R_obs` ([n_p][n_w], gradient models)
+ *   grad_off   : doubles into `chi_grad` ([4*n_layers + 1]: gradient as in
+ *                kr_misfit_gradient, then chi; gradient models)
+ * flags: KR_FREE_SURFACE | KR_BATCH_GRADIENT | KR_BATCH_STORE_R. */
+typedef struct {
+  int32_t n_layers;
+  int32_t n_p;
+  int32_t n_w;
+  uint32_t flags;
+  int64_t layers_off;
+  int64_t p_off;
+  int64_t omega_off;
+  int64_t R_off;
+  int64_t obs_off;
+  int64_t grad_off;
+} kr_model_desc;
+
+/* Schedule of a batch: threads per block (64 or 128) and frequencies per work item. */
+typedef struct {
+  int32_t threads;
+  int32_t tile_w;
+  int32_t reserved0;
+  int32_t reserved1;
+} kr_batch_config;
+
+/* Device bytes of the plan buffer for this batch shape and schedule (0 if invalid). */
+size_t kr_batch_plan_bytes(const kr_model_desc* descs_host, int32_t n_models,
+                           const kr_batch_config* cfg);
+
+/*
+ * Builds the plan of a batch on the host (pair table, work lists sorted by descending cost)
+ * and uploads it into `plan` (device, >= kr_batch_plan_bytes).  Synchronises `stream` once.
+ * The plan depends only on the batch SHAPE (layer counts, grid sizes, flags, offsets), not on
+ * parameter values: relaunching after updating `layers` / `p` / `omega` / `R_obs` in place is
+ * valid.
+ */
+kr_status kr_batch_plan(const kr_model_desc* descs_host, int32_t n_models,
+                        const kr_batch_config* cfg, void* plan, size_t plan_bytes, void* stream);
+
+/* Size of the plan's metadata image (the first bytes of the plan buffer). */
+size_t kr_batch_plan_meta_bytes(const kr_model_desc* descs_host, int32_t n_models,
+                                const kr_batch_config* cfg);
+
+/*
+ * Host-only variant of kr_batch_plan: writes the metadata image into HOST memory `image`
+ * (>= kr_batch_plan_meta_bytes); the caller copies it to the start of a plan buffer of
+ * kr_batch_plan_bytes (e.g. asynchronously from pinned memory) -- no CUDA call, no stream
+ * synchronisation.
+ */
+kr_status kr_batch_plan_host(const kr_model_desc* descs_host, int32_t n_models,
+                             const kr_batch_config* cfg, void* image, size_t image_bytes);
+
+/*
+ * Runs a planned batch: reset -> per-(model, slowness) coefficient prep -> persistent
+ * forward kernel -> persistent gradient kernel, all enqueued on `stream` with no host
+ * synchronisation or allocation (capturable in a CUDA graph).  `cfg` must be the plan's
+ * schedule and `max_layers` the largest n_layers of the batch.
+ */
+kr_status kr_batch_launch(void* plan, const kr_batch_config* cfg, int32_t max_layers,
+                          const double* layers, const double* p, const double* omega,
+                          const double* R_obs, double* R, double* chi_grad, void* stream);
+
+/*
+ * Tuning knob (no counterpart in the reference): register budget of the kr_reflectivity
+ * kernel as the number of 128-thread blocks each SM must fit (4 -> 128 registers per thread,
+ * 5 -> 96, 6 -> 80; other values select 4).  Process-wide; results are identical for every
+ * setting, only speed changes.
+ */
+void kr_set_forward_variant(int32_t min_blocks_per_sm);
+
 #ifdef __cplusplus
 }
 #endif

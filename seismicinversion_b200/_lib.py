@@ -23,6 +23,21 @@ KR_ERR_WORKSPACE = 5
 KR_ERR_TOO_LARGE = 6
 
 KR_FREE_SURFACE = 0x1
+KR_BATCH_GRADIENT = 0x2
+KR_BATCH_STORE_R = 0x4
+
+
+class BatchConfig(ctypes.Structure):
+    """kr_batch_config."""
+
+    _fields_ = [("threads", ctypes.c_int32), ("tile_w", ctypes.c_int32),
+                ("reserved0", ctypes.c_int32), ("reserved1", ctypes.c_int32)]
+
+
+# numpy dtype with the layout of kr_model_desc (64 bytes)
+MODEL_DESC_FIELDS = [("n_layers", "<i4"), ("n_p", "<i4"), ("n_w", "<i4"), ("flags", "<u4"),
+                     ("layers_off", "<i8"), ("p_off", "<i8"), ("omega_off", "<i8"),
+                     ("R_off", "<i8"), ("obs_off", "<i8"), ("grad_off", "<i8")]
 
 _c_double_p = ctypes.c_void_p  # device pointers travel as integers
 _size_t = ctypes.c_size_t
@@ -50,6 +65,12 @@ _SIGNATURES = {
     "kr_bessel_sum_noalloc_scratch_bytes": (_size_t, []),
     "kr_traces_workspace_bytes": (_size_t, [_i32, _i32]),
     "kr_traces": (_i32, [_vp, _vp, _i32, _i32, _vp, _vp, _vp, _size_t, _vp]),
+    "kr_set_forward_variant": (None, [_i32]),
+    "kr_batch_plan_bytes": (_size_t, [_vp, _i32, _vp]),
+    "kr_batch_plan": (_i32, [_vp, _i32, _vp, _vp, _size_t, _vp]),
+    "kr_batch_plan_meta_bytes": (_size_t, [_vp, _i32, _vp]),
+    "kr_batch_plan_host": (_i32, [_vp, _i32, _vp, _vp, _size_t]),
+    "kr_batch_launch": (_i32, [_vp, _vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     # include/kennett_b200_bench.h
     "kr_bench_fp64_fma": (_i32, [_i32, _i32, _vp, _vp]),
     "kr_bench_fp64_fma_flops": (ctypes.c_double, [_i32, _i32]),

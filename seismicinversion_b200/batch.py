@@ -1,0 +1,275 @@
+"""Batched evaluation of many earth models of uneven size (``kr_batch_*``).
+
+A ``ModelBatch`` packs models with different layer counts, slowness and frequency grids
+into device buffers, plans the batch once (work lists sorted by cost), and runs it as a
+persistent launch: forward R grids for some models, forward + misfit gradient for others.
+The launch needs no host synchronisation or allocation, so it can be captured in a CUDA
+graph and replayed; ``update_layers`` changes parameter values in place between replays
+(inversion iterates of the same shapes).
+
+The schedule (threads per block, frequencies per work item) is chosen by ``autotune``, which
+times the candidate schedules on the batch itself and caches the winner per batch signature.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+import time
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from . import _lib
+from . import device as D
+from .layer_model import LayerModel, pack_layers
+
+__all__ = ["BatchItem", "ModelBatch", "autotune", "SCHEDULES"]
+
+#: Candidate schedules: (threads per block, frequencies per work item).
+SCHEDULES = [(64, 64), (64, 128), (128, 128), (128, 256), (128, 512), (64, 256)]
+
+
+@dataclass
+class BatchItem:
+    """One model of a batch.
+
+    ``gradient=True`` asks for chi = sum |R - R_obs|^2 and its gradient with respect to every
+    layer's (alpha, beta, rho, h) (``R_obs`` required, shape (n_p, n_w)); otherwise the R grid
+    is computed.  ``store_R`` also stores R for gradient models.
+    """
+
+    model: LayerModel
+    p: np.ndarray
+    omega: np.ndarray
+    gradient: bool = False
+    R_obs: np.ndarray | None = None
+    free_surface: bool = False
+    store_R: bool = False
+
+
+class ModelBatch:
+    """Device-resident packed batch with its plan; see the module docstring."""
+
+    def __init__(self, items: list[BatchItem], schedule: tuple[int, int] | None = None,
+                 device=None):
+        self.dev = D.require_cuda(device)
+        self.items = items
+        n = len(items)
+        desc = np.zeros(n, dtype=_lib.MODEL_DESC_FIELDS)
+        tabs, ps, ws, obs = [], [], [], []
+        lo = po = wo = ro = oo = go = 0
+        self.max_layers = 2
+        for b, it in enumerate(items):
+            tab = pack_layers(it.model)
+            D.validate_table(tab)
+            L = tab.shape[1]
+            p = np.ascontiguousarray(it.p, dtype=np.float64).reshape(-1)
+            w = np.ascontiguousarray(it.omega, dtype=np.complex128).reshape(-1)
+            flags = _lib.KR_FREE_SURFACE if it.free_surface else 0
+            if it.gradient:
+                if it.R_obs is None:
+                    raise ValueError(f"batch item {b}: gradient requested without R_obs")
+                o = np.ascontiguousarray(it.R_obs, dtype=np.complex128).reshape(len(p), len(w))
+                flags |= _lib.KR_BATCH_GRADIENT | (_lib.KR_BATCH_STORE_R if it.store_R else 0)
+            d = desc[b]
+            d["n_layers"], d["n_p"], d["n_w"], d["flags"] = L, len(p), len(w), flags
+            d["layers_off"], d["p_off"], d["omega_off"] = lo, po, wo
+            tabs.append(tab.ravel())
+            ps.append(p)
+            ws.append(w)
+            lo += tab.size
+            po += len(p)
+            wo += len(w)
+            if (not it.gradient) or it.store_R:
+                d["R_off"] = ro
+                ro += len(p) * len(w)
+            if it.gradient:
+                d["obs_off"], d["grad_off"] = oo, go
+                obs.append(o.ravel())
+                oo += o.size
+                go += 4 * L + 1
+            self.max_layers = max(self.max_layers, L)
+        self.desc = desc
+        dev = self.dev
+        self.layers = torch.as_tensor(np.concatenate(tabs) if tabs else np.zeros(1), device=dev)
+        self.p = torch.as_tensor(np.concatenate(ps) if ps else np.zeros(1), device=dev)
+        self.omega = torch.as_tensor(np.concatenate(ws) if ws else np.zeros(1, np.complex128),
+                                     device=dev)
+        self.R_obs = torch.as_tensor(np.concatenate(obs), device=dev) if obs else None
+        self.R = torch.empty(max(ro, 1), dtype=torch.complex128, device=dev)
+        self.chi_grad = torch.zeros(max(go, 1), dtype=torch.float64, device=dev)
+        self.graph = None
+        self.schedule = None
+        self.plan = None
+        self.set_schedule(schedule or (128, 256))
+
+    # -- planning ------------------------------------------------------------------------
+    def _cfg(self, schedule):
+        return _lib.BatchConfig(int(schedule[0]), int(schedule[1]), 0, 0)
+
+    def set_schedule(self, schedule: tuple[int, int]) -> None:
+        """(Re)plan the batch for a schedule (threads, frequencies per item)."""
+        h = _lib.lib()
+        cfg = self._cfg(schedule)
+        n = len(self.desc)
+        nbytes = h.kr_batch_plan_bytes(self.desc.ctypes.data, n, ctypes.byref(cfg))
+        if nbytes == 0:
+            raise ValueError(f"invalid batch or schedule {schedule}")
+        meta = h.kr_batch_plan_meta_bytes(self.desc.ctypes.data, n, ctypes.byref(cfg))
+        image = torch.empty(meta, dtype=torch.uint8, pin_memory=True)
+        st = h.kr_batch_plan_host(self.desc.ctypes.data, n, ctypes.byref(cfg), image.data_ptr(),
+                                  meta)
+        _lib.check(st, "kr_batch_plan_host")
+        plan = torch.empty(nbytes, dtype=torch.uint8, device=self.dev)
+        plan[:meta].copy_(image, non_blocking=True)  # stream-ordered before any launch
+        self._plan_image = image  # keep the pinned source alive until the copy has run
+        self.plan, self.schedule, self._cfg_obj, self.graph = plan, tuple(schedule), cfg, None
+
+    # -- running -------------------------------------------------------------------------
+    def launch(self) -> None:
+        """Enqueue the batch on the current stream (no synchronisation)."""
+        h = _lib.lib()
+        obs = self.R_obs.data_ptr() if self.R_obs is not None else None
+        st = h.kr_batch_launch(self.plan.data_ptr(), ctypes.byref(self._cfg_obj), self.max_layers,
+                               self.layers.data_ptr(), self.p.data_ptr(), self.omega.data_ptr(),
+                               obs, self.R.data_ptr(), self.chi_grad.data_ptr(),
+                               D.stream_handle(self.dev))
+        _lib.check(st, "kr_batch_launch")
+
+    def capture(self) -> torch.cuda.CUDAGraph:
+        """Capture one launch in a CUDA graph (replay with ``run``)."""
+        s = torch.cuda.Stream(self.dev)
+        s.wait_stream(torch.cuda.current_stream(self.dev))
+        with torch.cuda.stream(s):
+            self.launch()  # warm: loads modules outside capture
+        torch.cuda.current_stream(self.dev).wait_stream(s)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            self.launch()
+        self.graph = g
+        return g
+
+    def run(self) -> None:
+        """Replay the captured graph if any, else launch directly."""
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            self.launch()
+
+    def update_layers(self, models: list[LayerModel]) -> None:
+        """Copy new layer values (same layer counts) into the device buffer in place."""
+        tabs = []
+        for b, m in enumerate(models):
+            tab = pack_layers(m)
+            if tab.shape[1] != self.desc[b]["n_layers"]:
+                raise ValueError(f"model {b}: layer count changed")
+            D.validate_table(tab)
+            tabs.append(tab.ravel())
+        self.layers.copy_(torch.from_numpy(np.concatenate(tabs)), non_blocking=False)
+
+    # -- results -------------------------------------------------------------------------
+    def reflectivity(self, b: int) -> torch.Tensor:
+        """R grid (n_p, n_w) of model b (device view)."""
+        d = self.desc[b]
+        if (d["flags"] & _lib.KR_BATCH_GRADIENT) and not (d["flags"] & _lib.KR_BATCH_STORE_R):
+            raise ValueError(f"model {b} is a gradient model without store_R")
+        n = int(d["n_p"]) * int(d["n_w"])
+        return self.R[int(d["R_off"]):int(d["R_off"]) + n].view(int(d["n_p"]), int(d["n_w"]))
+
+    def misfit_gradient(self, b: int) -> tuple[torch.Tensor, torch.Tensor]:
+        """(chi, gradient [4L]) of gradient model b (device views)."""
+        d = self.desc[b]
+        if not d["flags"] & _lib.KR_BATCH_GRADIENT:
+            raise ValueError(f"model {b} is not a gradient model")
+        L = int(d["n_layers"])
+        v = self.chi_grad[int(d["grad_off"]):int(d["grad_off"]) + 4 * L + 1]
+        return v[4 * L], v[:4 * L]
+
+    def work(self) -> dict:
+        """Algorithmic work of one launch: forward and gradient (omega, p, interface) updates."""
+        fwd = grad = 0
+        for d in self.desc:
+            u = int(d["n_p"]) * int(d["n_w"]) * (int(d["n_layers"]) - 1)
+            if d["flags"] & _lib.KR_BATCH_GRADIENT:
+                grad += u
+            else:
+                fwd += u
+        return {"forward_updates": fwd, "gradient_updates": grad,
+                "gradient_models": int(np.sum(self.desc["flags"] & _lib.KR_BATCH_GRADIENT > 0)),
+                "models": len(self.desc)}
+
+    def signature(self) -> str:
+        w = self.work()
+        Ls = self.desc["n_layers"]
+        return (f"m{len(self.desc)}-f{w['forward_updates']:.2e}-g{w['gradient_updates']:.2e}"
+                f"-L{int(Ls.min())}-{int(Ls.max())}")
+
+
+def _time_launch(batch: ModelBatch, reps: int) -> float:
+    st = torch.cuda.current_stream(batch.dev)
+    batch.launch()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for _ in range(reps):
+        batch.launch()
+    b.record(st)
+    b.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+_TUNE_CACHE: dict = {}
+
+
+def autotune(batch: ModelBatch, candidates=None, reps: int = 2, cache_file: str | None = None):
+    """Time each candidate schedule on ``batch`` and keep the fastest.
+
+    Returns ``(best_schedule, {schedule: ms})``.  Winners are cached per batch signature in
+    memory and, if ``cache_file`` (or ``KR_TUNE_CACHE``) names a JSON file, on disk.
+    """
+    sig = batch.signature()
+    path = cache_file or os.environ.get("KR_TUNE_CACHE")
+    disk = {}
+    if path and Path(path).exists():
+        try:
+            disk = json.loads(Path(path).read_text())
+        except (OSError, ValueError):
+            disk = {}
+    hit = _TUNE_CACHE.get(sig) or disk.get(sig)
+    if hit:
+        batch.set_schedule(tuple(hit))
+        return tuple(hit), {}
+    times = {}
+    for sch in candidates or SCHEDULES:
+        batch.set_schedule(sch)
+        times[sch] = _time_launch(batch, reps)
+    best = min(times, key=times.get)
+    batch.set_schedule(best)
+    _TUNE_CACHE[sig] = list(best)
+    if path:
+        disk[sig] = list(best)
+        try:
+            Path(path).write_text(json.dumps(disk, indent=1))
+        except OSError:
+            pass
+    return best, times
+
+
+def per_call_reference(items: list[BatchItem], device=None) -> float:
+    """Wall time (s) of the plain per-call path: one fused-kernel call per model with a
+    synchronisation after each (kr_reflectivity or kr_misfit_gradient), for comparison."""
+    dev = D.require_cuda(device)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for it in items:
+        tab = D.layer_table(it.model, dev)
+        if it.gradient:
+            D.misfit_gradient(tab, it.p, it.omega, it.R_obs, it.free_surface)
+        else:
+            D.reflectivity(tab, it.p, it.omega, it.free_surface)
+        torch.cuda.synchronize(dev)
+    return time.perf_counter() - t0

@@ -1,0 +1,480 @@
+// Batched evaluation of many earth models of uneven size in persistent launches.
+//
+// A batch is a list of models, each with its own layer count, slowness grid and frequency
+// grid, asking for the forward reflectivity or forward + misfit gradient.  kr_batch_plan
+// (host) builds, once per batch shape:
+//   * a pair table: one entry per (model, slowness) with the offset of its coefficient block
+//     in the plan buffer;
+//   * two work lists (forward items, gradient items), item = (pair, first frequency, count),
+//     sorted by descending cost (layers x frequencies, x4 for gradients) so the dynamic
+//     scheduler hands out the longest items first (LPT);
+// and uploads them into the caller's plan buffer.  kr_batch_launch (device only, capturable
+// in a CUDA graph) then runs:
+//   1. batch_prep_kernel: one block per pair -> layer terms and interface coefficients (and,
+//      for gradient models, layer derivative factors and coefficient tangents) into the plan;
+//   2. batch_forward_kernel and batch_gradient_kernel: persistent grids (resident blocks
+//      only) that pull items with an atomic counter until the list is exhausted.
+// Gradient items reduce their contributions per block in a fixed order and add them to the
+// model's chi_grad with FP64 atomics (the order of those additions across blocks is not
+// fixed: results agree to rounding, ~1e-16 relative, run to run).
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "kr_adjoint.cuh"
+#include "kr_internal.cuh"
+
+namespace kr {
+
+struct PairRec {
+  int32_t model;
+  int32_t j;
+  int64_t coef_off;  // bytes into the plan buffer
+};
+
+struct ItemRec {
+  int32_t pair;
+  int32_t w0;
+  int32_t nw;
+  int32_t pad;
+};
+
+struct PlanHeader {
+  int32_t n_models, n_pairs, n_fwd, n_grad;
+  int32_t threads, tile_w, grid_fwd, grid_grad;
+  int64_t off_models, off_pairs, off_fwd, off_grad, total_bytes;
+  int32_t counters[4];  // [0] forward item counter, [1] gradient item counter
+};
+
+__host__ __device__ inline size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static size_t pair_bytes(const kr_model_desc& d) {
+  const int L = d.n_layers, I = d.n_layers - 1;
+  size_t b = a256(sizeof(LayerP) * L) + a256(sizeof(Iface) * I);
+  if (d.flags & KR_BATCH_GRADIENT) b += a256(sizeof(LayerD) * L) + a256(sizeof(ScatTan) * I);
+  return b;
+}
+
+struct PairView {
+  const LayerP* lay;
+  const Iface* coef;
+  const LayerD* dlay;
+  const ScatTan* tan;
+};
+
+__device__ __forceinline__ PairView pair_view(const unsigned char* plan, const PairRec& pr,
+                                              const kr_model_desc& d) {
+  const int L = d.n_layers, I = d.n_layers - 1;
+  const unsigned char* b = plan + pr.coef_off;
+  PairView v;
+  v.lay = reinterpret_cast<const LayerP*>(b);
+  b += a256(sizeof(LayerP) * L);
+  v.coef = reinterpret_cast<const Iface*>(b);
+  b += a256(sizeof(Iface) * I);
+  v.dlay = reinterpret_cast<const LayerD*>(b);
+  b += a256(sizeof(LayerD) * L);
+  v.tan = reinterpret_cast<const ScatTan*>(b);
+  return v;
+}
+
+__global__ void batch_prep_kernel(unsigned char* plan, const double* __restrict__ layers,
+                                  const double* __restrict__ p_all) {
+  const PlanHeader* h = reinterpret_cast<const PlanHeader*>(plan);
+  const kr_model_desc* models = reinterpret_cast<const kr_model_desc*>(plan + h->off_models);
+  const PairRec* pairs = reinterpret_cast<const PairRec*>(plan + h->off_pairs);
+  for (int q = blockIdx.x; q < h->n_pairs; q += gridDim.x) {
+    const PairRec pr = pairs[q];
+    const kr_model_desc d = models[pr.model];
+    const int L = d.n_layers, I = L - 1;
+    const double* tab = layers + d.layers_off;
+    const double pj = p_all[d.p_off + pr.j];
+    unsigned char* b = plan + pr.coef_off;
+    LayerP* lay = reinterpret_cast<LayerP*>(b);
+    b += a256(sizeof(LayerP) * L);
+    Iface* coef = reinterpret_cast<Iface*>(b);
+    b += a256(sizeof(Iface) * I);
+    LayerD* dlay = reinterpret_cast<LayerD*>(b);
+    b += a256(sizeof(LayerD) * L);
+    ScatTan* tan = reinterpret_cast<ScatTan*>(b);
+    const bool grad = (d.flags & KR_BATCH_GRADIENT) != 0;
+    for (int l = threadIdx.x; l < L; l += blockDim.x) {
+      lay[l] = layer_terms(tab, L, l, pj);
+      if (grad) dlay[l] = layer_derivs(tab, L, l, pj, lay[l]);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < I; i += blockDim.x) {
+      coef[i] = interface_coeffs(pj, i, lay[i], lay[i + 1]);
+      if (grad) interface_tangents(pj, i, lay[i], dlay[i], lay[i + 1], dlay[i + 1], tan[i]);
+    }
+    __syncthreads();
+  }
+}
+
+// Zeroes chi_grad of gradient models and the item counters (first node of a launch).
+__global__ void batch_reset_kernel(unsigned char* plan, double* chi_grad) {
+  PlanHeader* h = reinterpret_cast<PlanHeader*>(plan);
+  const kr_model_desc* models = reinterpret_cast<const kr_model_desc*>(plan + h->off_models);
+  if (blockIdx.x == 0 && threadIdx.x < 4) h->counters[threadIdx.x] = 0;
+  for (int b = blockIdx.x; b < h->n_models; b += gridDim.x) {
+    const kr_model_desc d = models[b];
+    if (!(d.flags & KR_BATCH_GRADIENT)) continue;
+    for (int k = threadIdx.x; k < 4 * d.n_layers + 1; k += blockDim.x) chi_grad[d.grad_off + k] = 0.0;
+  }
+}
+
+__device__ __forceinline__ int next_item(int* counter) {
+  __shared__ int s_item;
+  __syncthreads();
+  if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+  __syncthreads();
+  return s_item;
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS)
+batch_forward_kernel(unsigned char* plan, const double2* __restrict__ omega_all,
+                     double2* __restrict__ R_all) {
+  PlanHeader* h = reinterpret_cast<PlanHeader*>(plan);
+  const kr_model_desc* models = reinterpret_cast<const kr_model_desc*>(plan + h->off_models);
+  const PairRec* pairs = reinterpret_cast<const PairRec*>(plan + h->off_pairs);
+  const ItemRec* items = reinterpret_cast<const ItemRec*>(plan + h->off_fwd);
+  const int n_items = h->n_fwd;
+  for (;;) {
+    const int it = next_item(&h->counters[0]);
+    if (it >= n_items) break;
+    const ItemRec item = items[it];
+    const PairRec pr = pairs[item.pair];
+    const kr_model_desc d = models[pr.model];
+    const PairView v = pair_view(plan, pr, d);
+    const bool fs = (d.flags & KR_FREE_SURFACE) != 0;
+    for (int k = threadIdx.x; k < item.nw; k += THREADS) {
+      const int iw = item.w0 + k;
+      const double2 wv = omega_all[d.omega_off + iw];
+      const cd w = mk(wv.x, wv.y);
+      const cd rpp = sweep(w, d.n_layers, v.lay, v.coef);
+      const cd out = pp_surface(rpp, cexp_(w * v.lay[0].ca), fs);
+      R_all[d.R_off + (size_t)pr.j * d.n_w + iw] = make_double2(out.x, out.y);
+    }
+  }
+}
+
+// Per-thread sink for gradient items: accumulates 2 Re(conj(res) dR/dtheta) per layer into
+// block shared memory (warp shuffles, then warps in order).
+template <int THREADS>
+struct BatchGradSink {
+  bool valid;
+  cd res;
+  const double2* obs;
+  double2* R_out;
+  double* s_acc;   // [4L + 1]
+  double* s_warp;  // [THREADS / 32 * 4]
+  int L;
+  __device__ void reflectivity(cd R) {
+    res = mk(0.0, 0.0);
+    if (!valid) return;
+    if (R_out) *R_out = make_double2(R.x, R.y);
+    const double2 o = *obs;
+    res = mk(R.x - o.x, R.y - o.y);
+  }
+  __device__ void layer(int l, const Acc& a) {
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    if (valid) {
+      v[0] = 2.0 * (res.x * a.a.x + res.y * a.a.y);
+      v[1] = 2.0 * (res.x * a.b.x + res.y * a.b.y);
+      v[2] = 2.0 * (res.x * a.r.x + res.y * a.r.y);
+      v[3] = 2.0 * (res.x * a.h.x + res.y * a.h.y);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    const int warp = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0)
+      for (int k = 0; k < 4; ++k) s_warp[warp * 4 + k] = v[k];
+    __syncthreads();
+    if (threadIdx.x < 4) {
+      double t = 0.0;
+      for (int w = 0; w < THREADS / 32; ++w) t += s_warp[w * 4 + threadIdx.x];
+      s_acc[threadIdx.x * L + l] += t;
+    }
+    __syncthreads();
+  }
+};
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS)
+batch_gradient_kernel(unsigned char* plan, const double2* __restrict__ omega_all,
+                      const double2* __restrict__ obs_all, double2* __restrict__ R_all,
+                      double* __restrict__ chi_grad) {
+  extern __shared__ double s_dyn[];
+  double* s_warp = s_dyn;                    // [THREADS / 32 * 4]
+  double* s_acc = s_dyn + THREADS / 32 * 4;  // [4L + 1]
+  PlanHeader* h = reinterpret_cast<PlanHeader*>(plan);
+  const kr_model_desc* models = reinterpret_cast<const kr_model_desc*>(plan + h->off_models);
+  const PairRec* pairs = reinterpret_cast<const PairRec*>(plan + h->off_pairs);
+  const ItemRec* items = reinterpret_cast<const ItemRec*>(plan + h->off_grad);
+  const int n_items = h->n_grad;
+  for (;;) {
+    const int it = next_item(&h->counters[1]);
+    if (it >= n_items) break;
+    const ItemRec item = items[it];
+    const PairRec pr = pairs[item.pair];
+    const kr_model_desc d = models[pr.model];
+    const PairView v = pair_view(plan, pr, d);
+    const int L = d.n_layers;
+    for (int k = threadIdx.x; k < 4 * L + 1; k += THREADS) s_acc[k] = 0.0;
+    __syncthreads();
+    const int seg = checkpoint_spacing(L - 2 > 0 ? L - 2 : 1);
+    const bool fs = (d.flags & KR_FREE_SURFACE) != 0;
+    for (int k0 = 0; k0 < item.nw; k0 += THREADS) {
+      const int iw = item.w0 + k0 + threadIdx.x;
+      const bool valid = k0 + threadIdx.x < item.nw;
+      cd w = mk(0.0, 0.0);
+      if (valid) {
+        const double2 wv = omega_all[d.omega_off + iw];
+        w = mk(wv.x, wv.y);
+      }
+      BatchGradSink<THREADS> sink;
+      sink.valid = valid;
+      sink.L = L;
+      sink.s_acc = s_acc;
+      sink.s_warp = s_warp;
+      const size_t e = (size_t)pr.j * d.n_w + (valid ? iw : 0);
+      sink.obs = obs_all + d.obs_off + e;
+      sink.R_out = (d.flags & KR_BATCH_STORE_R) ? R_all + d.R_off + e : nullptr;
+      jacobian_pair(L, w, fs, seg, v.lay, v.dlay, v.coef, v.tan, sink);
+      double c2 = valid ? (sink.res.x * sink.res.x + sink.res.y * sink.res.y) : 0.0;
+      for (int o = 16; o > 0; o >>= 1) c2 += __shfl_down_sync(0xffffffffu, c2, o);
+      if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = c2;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int wi = 0; wi < THREADS / 32; ++wi) t += s_warp[wi];
+        s_acc[4 * L] += t;
+      }
+      __syncthreads();
+    }
+    for (int k = threadIdx.x; k < 4 * L + 1; k += THREADS)
+      atomicAdd(chi_grad + d.grad_off + k, s_acc[k]);
+  }
+}
+
+static int occupancy_grid(const void* fn, int threads, size_t smem) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return per_sm * sms;
+}
+
+static bool valid_config(const kr_batch_config* c) {
+  return c && (c->threads == 64 || c->threads == 128) && c->tile_w >= 32 && c->tile_w <= 8192;
+}
+
+struct PlanLayout {
+  PlanHeader h;
+  size_t bytes;
+};
+
+static kr_status layout(const kr_model_desc* descs, int n_models, const kr_batch_config* cfg,
+                        PlanLayout* out, std::vector<PairRec>* pairs,
+                        std::vector<ItemRec>* fwd, std::vector<ItemRec>* grad) {
+  PlanHeader h{};
+  h.n_models = n_models;
+  h.threads = cfg->threads;
+  h.tile_w = cfg->tile_w;
+  size_t off = a256(sizeof(PlanHeader));
+  h.off_models = (int64_t)off;
+  off = a256(off + sizeof(kr_model_desc) * (size_t)n_models);
+  long long n_pairs = 0;
+  for (int b = 0; b < n_models; ++b) {
+    const kr_model_desc& d = descs[b];
+    if (d.n_layers < 2) return KR_ERR_INVALID_MODEL;
+    if (d.n_layers > kMaxLayers) return KR_ERR_TOO_LARGE;
+    if (d.n_p < 0 || d.n_w < 0 || (d.flags & ~(KR_FREE_SURFACE | KR_BATCH_GRADIENT |
+                                               KR_BATCH_STORE_R)))
+      return KR_ERR_INVALID_ARGUMENT;
+    n_pairs += d.n_p;
+  }
+  if (n_pairs > 0x7fffffffLL) return KR_ERR_TOO_LARGE;
+  h.n_pairs = (int)n_pairs;
+  h.off_pairs = (int64_t)off;
+  off = a256(off + sizeof(PairRec) * (size_t)n_pairs);
+  // item lists (count first)
+  struct Costed {
+    double cost;
+    ItemRec it;
+  };
+  std::vector<Costed> cf, cg;
+  int q = 0;
+  for (int b = 0; b < n_models; ++b) {
+    const kr_model_desc& d = descs[b];
+    const bool gr = (d.flags & KR_BATCH_GRADIENT) != 0;
+    for (int j = 0; j < d.n_p; ++j, ++q) {
+      for (int w0 = 0; w0 < d.n_w; w0 += cfg->tile_w) {
+        ItemRec it{q, w0, std::min(cfg->tile_w, d.n_w - w0), 0};
+        const double cost = (double)(d.n_layers - 1) * it.nw * (gr ? 4.0 : 1.0);
+        (gr ? cg : cf).push_back({cost, it});
+      }
+    }
+  }
+  auto by_cost = [](const Costed& a, const Costed& b) { return a.cost > b.cost; };
+  std::stable_sort(cf.begin(), cf.end(), by_cost);
+  std::stable_sort(cg.begin(), cg.end(), by_cost);
+  h.n_fwd = (int)cf.size();
+  h.n_grad = (int)cg.size();
+  h.off_fwd = (int64_t)off;
+  off = a256(off + sizeof(ItemRec) * cf.size());
+  h.off_grad = (int64_t)off;
+  off = a256(off + sizeof(ItemRec) * cg.size());
+  if (pairs) {
+    pairs->clear();
+    pairs->reserve((size_t)n_pairs);
+  }
+  for (int b = 0; b < n_models; ++b) {
+    const size_t pb = pair_bytes(descs[b]);
+    for (int j = 0; j < descs[b].n_p; ++j) {
+      if (pairs) pairs->push_back(PairRec{b, j, (int64_t)off});
+      off += pb;
+    }
+  }
+  h.total_bytes = (int64_t)off;
+  if (fwd) {
+    fwd->clear();
+    for (auto& c : cf) fwd->push_back(c.it);
+  }
+  if (grad) {
+    grad->clear();
+    for (auto& c : cg) grad->push_back(c.it);
+  }
+  out->h = h;
+  out->bytes = off;
+  return KR_OK;
+}
+
+template <int THREADS>
+static void grids(PlanHeader& h, int max_layers) {
+  h.grid_fwd = occupancy_grid((const void*)batch_forward_kernel<THREADS>, THREADS, 0);
+  const size_t smem = sizeof(double) * (THREADS / 32 * 4 + 4 * (size_t)max_layers + 1);
+  h.grid_grad = occupancy_grid((const void*)batch_gradient_kernel<THREADS>, THREADS, smem);
+}
+
+}  // namespace kr
+
+using namespace kr;
+
+extern "C" size_t kr_batch_plan_bytes(const kr_model_desc* descs, int32_t n_models,
+                                      const kr_batch_config* cfg) {
+  if (!descs || n_models < 0 || !valid_config(cfg)) return 0;
+  PlanLayout lay;
+  if (layout(descs, n_models, cfg, &lay, nullptr, nullptr, nullptr) != KR_OK) return 0;
+  return lay.bytes;
+}
+
+// Fills the plan's metadata image (header, model table, pair table, work lists) in host
+// memory; returns its size in *meta_bytes.  Host only: no CUDA call.
+static kr_status plan_image(const kr_model_desc* descs, int n_models, const kr_batch_config* cfg,
+                            std::vector<unsigned char>* img, size_t* total_bytes) {
+  PlanLayout lay;
+  std::vector<PairRec> pairs;
+  std::vector<ItemRec> fwd, grad;
+  kr_status s = layout(descs, n_models, cfg, &lay, &pairs, &fwd, &grad);
+  if (s != KR_OK) return s;
+  const size_t meta = (size_t)(lay.h.off_grad + sizeof(ItemRec) * grad.size());
+  img->assign(meta, 0);
+  memcpy(img->data(), &lay.h, sizeof(PlanHeader));
+  memcpy(img->data() + lay.h.off_models, descs, sizeof(kr_model_desc) * (size_t)n_models);
+  if (!pairs.empty())
+    memcpy(img->data() + lay.h.off_pairs, pairs.data(), sizeof(PairRec) * pairs.size());
+  if (!fwd.empty()) memcpy(img->data() + lay.h.off_fwd, fwd.data(), sizeof(ItemRec) * fwd.size());
+  if (!grad.empty())
+    memcpy(img->data() + lay.h.off_grad, grad.data(), sizeof(ItemRec) * grad.size());
+  *total_bytes = lay.bytes;
+  return KR_OK;
+}
+
+extern "C" size_t kr_batch_plan_meta_bytes(const kr_model_desc* descs, int32_t n_models,
+                                           const kr_batch_config* cfg) {
+  if (!descs || n_models < 0 || !valid_config(cfg)) return 0;
+  std::vector<unsigned char> img;
+  size_t total = 0;
+  if (plan_image(descs, n_models, cfg, &img, &total) != KR_OK) return 0;
+  return img.size();
+}
+
+extern "C" kr_status kr_batch_plan_host(const kr_model_desc* descs, int32_t n_models,
+                                        const kr_batch_config* cfg, void* image,
+                                        size_t image_bytes) {
+  if (!descs || n_models < 0 || !image) return KR_ERR_INVALID_ARGUMENT;
+  if (!valid_config(cfg)) return KR_ERR_INVALID_ARGUMENT;
+  std::vector<unsigned char> img;
+  size_t total = 0;
+  kr_status s = plan_image(descs, n_models, cfg, &img, &total);
+  if (s != KR_OK) return s;
+  if (image_bytes < img.size()) return KR_ERR_WORKSPACE;
+  memcpy(image, img.data(), img.size());
+  return KR_OK;
+}
+
+extern "C" kr_status kr_batch_plan(const kr_model_desc* descs, int32_t n_models,
+                                   const kr_batch_config* cfg, void* plan, size_t plan_bytes,
+                                   void* stream) {
+  if (!descs || n_models < 0 || !plan) return KR_ERR_INVALID_ARGUMENT;
+  if (!valid_config(cfg)) return KR_ERR_INVALID_ARGUMENT;
+  std::vector<unsigned char> img;
+  size_t total = 0;
+  kr_status s = plan_image(descs, n_models, cfg, &img, &total);
+  if (s != KR_OK) return s;
+  if (plan_bytes < total) return KR_ERR_WORKSPACE;
+  // Pageable source: synchronise before the vector goes out of scope.
+  cudaError_t e = cudaMemcpyAsync(plan, img.data(), img.size(), cudaMemcpyHostToDevice,
+                                  (cudaStream_t)stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
+  if (e != cudaSuccess) {
+    set_last_error("kr_batch_plan: upload", e);
+    return KR_ERR_CUDA;
+  }
+  return KR_OK;
+}
+
+extern "C" kr_status kr_batch_launch(void* plan, const kr_batch_config* cfg, int32_t max_layers,
+                                     const double* layers, const double* p, const double* omega,
+                                     const double* R_obs, double* R, double* chi_grad,
+                                     void* stream) {
+  if (!plan || !valid_config(cfg) || !layers || !p || !omega) return KR_ERR_INVALID_ARGUMENT;
+  if (max_layers < 2 || max_layers > kMaxLayers) return KR_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  unsigned char* pl = static_cast<unsigned char*>(plan);
+  // Grid sizes come from the same occupancy query the plan used (host-side, capture-safe).
+  PlanHeader h{};
+  h.threads = cfg->threads;
+  if (cfg->threads == 64)
+    grids<64>(h, max_layers);
+  else
+    grids<128>(h, max_layers);
+  batch_reset_kernel<<<148, 128, 0, st>>>(pl, chi_grad);
+  kr_status s = check_launch("kr_batch_launch: reset");
+  if (s != KR_OK) return s;
+  batch_prep_kernel<<<148 * 16, 64, 0, st>>>(pl, layers, p);
+  s = check_launch("kr_batch_launch: prep");
+  if (s != KR_OK) return s;
+  const double2* w = reinterpret_cast<const double2*>(omega);
+  const size_t gsmem = sizeof(double) * (cfg->threads / 32 * 4 + 4 * (size_t)max_layers + 1);
+  if (cfg->threads == 64) {
+    batch_forward_kernel<64><<<h.grid_fwd, 64, 0, st>>>(pl, w, reinterpret_cast<double2*>(R));
+    s = check_launch("kr_batch_launch: forward");
+    if (s != KR_OK) return s;
+    batch_gradient_kernel<64><<<h.grid_grad, 64, gsmem, st>>>(
+        pl, w, reinterpret_cast<const double2*>(R_obs), reinterpret_cast<double2*>(R), chi_grad);
+  } else {
+    batch_forward_kernel<128><<<h.grid_fwd, 128, 0, st>>>(pl, w, reinterpret_cast<double2*>(R));
+    s = check_launch("kr_batch_launch: forward");
+    if (s != KR_OK) return s;
+    batch_gradient_kernel<128><<<h.grid_grad, 128, gsmem, st>>>(
+        pl, w, reinterpret_cast<const double2*>(R_obs), reinterpret_cast<double2*>(R), chi_grad);
+  }
+  return check_launch("kr_batch_launch: gradient");
+}

@@ -6,35 +6,90 @@
 // matrix in registers, applies the ocean phase / free-surface operator and writes
 // R[p][omega] (coalesced along omega).  FP64 CUDA cores; no tensor-core work exists here
 // (2x2 complex algebra per thread is not a contraction).
+#include <stdlib.h>
+
 #include "kr_internal.cuh"
 
 namespace kr {
 
 constexpr int kFwdThreads = 128;
 
-__global__ void __launch_bounds__(kFwdThreads)
+template <int MINB>
+__global__ void __launch_bounds__(kFwdThreads, MINB)
 reflectivity_kernel(const double* __restrict__ tab, int n_layers, const double* __restrict__ p,
                     int n_p, const double2* __restrict__ omega, int n_w, int n_wtiles,
-                    int free_surface, double2* __restrict__ R) {
+                    int tiles_per_block, int free_surface, double2* __restrict__ R) {
   extern __shared__ __align__(16) unsigned char smem[];
   LayerP* s_layer = reinterpret_cast<LayerP*>(smem);
   Iface* s_iface = reinterpret_cast<Iface*>(smem + sizeof(LayerP) * n_layers);
-  const int ip = blockIdx.x / n_wtiles;
-  const int iw = (blockIdx.x % n_wtiles) * kFwdThreads + threadIdx.x;
-  const double pj = p[ip];
-  block_prologue(tab, n_layers, pj, s_layer, s_iface);
-  if (iw >= n_w) return;
-  const double2 wv = omega[iw];
-  const cd w = mk(wv.x, wv.y);
-  cd rpp = sweep(w, n_layers, s_layer, s_iface);
-  cd e0 = cexp_(w * s_layer[0].ca);
-  cd out = pp_surface(rpp, e0, free_surface != 0);
-  R[(size_t)ip * n_w + iw] = make_double2(out.x, out.y);
+  const int groups = (n_wtiles + tiles_per_block - 1) / tiles_per_block;
+  const int ip = blockIdx.x / groups;
+  const int t0 = (blockIdx.x % groups) * tiles_per_block;
+  const int t1 = min(n_wtiles, t0 + tiles_per_block);
+  block_prologue(tab, n_layers, p[ip], s_layer, s_iface);
+  for (int t = t0; t < t1; ++t) {
+    const int iw = t * kFwdThreads + threadIdx.x;
+    if (iw >= n_w) break;
+    const double2 wv = omega[iw];
+    const cd w = mk(wv.x, wv.y);
+    const cd rpp = sweep(w, n_layers, s_layer, s_iface);
+    const cd out = pp_surface(rpp, cexp_(w * s_layer[0].ca), free_surface != 0);
+    R[(size_t)ip * n_w + iw] = make_double2(out.x, out.y);
+  }
+}
+
+// Frequency tiles one block sweeps after its prologue: enough to amortise the prologue
+// (the block's threads wait at its barrier while ~L of them compute coefficients) while
+// keeping at least ~8 waves of blocks on 148 SMs.
+static int tiles_per_block(long long n_p, int n_wtiles) {
+  const long long target_blocks = 148LL * 6 * 8;
+  long long t = (n_p * n_wtiles) / target_blocks;
+  if (t < 1) t = 1;
+  if (t > n_wtiles) t = n_wtiles;
+  return (int)t;
+}
+
+// Register budget of the forward kernel: blocks of 128 threads resident per SM the compiler
+// must allow (4 -> 128 registers, 5 -> 102, 6 -> 85).  Chosen by kr_set_forward_variant (the
+// autotuner) or the KR_FWD_MINB environment variable; default 4.
+static int g_fwd_minb = 0;
+
+static int forward_minb() {
+  if (g_fwd_minb == 0) {
+    const char* e = getenv("KR_FWD_MINB");
+    int v = e ? atoi(e) : 4;
+    g_fwd_minb = (v == 5 || v == 6) ? v : 4;
+  }
+  return g_fwd_minb;
+}
+
+template <int MINB>
+static kr_status launch_forward(const double* layers, int n_layers, const double* p, int n_p,
+                                const double* omega, int n_w, int n_wtiles, size_t smem,
+                                uint32_t flags, double* R, cudaStream_t st) {
+  const int tpb = tiles_per_block(n_p, n_wtiles);
+  const long long blocks = (long long)n_p * ((n_wtiles + tpb - 1) / tpb);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(reflectivity_kernel<MINB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) {
+      set_last_error("kr_reflectivity: smem attribute", e);
+      return KR_ERR_CUDA;
+    }
+  }
+  reflectivity_kernel<MINB><<<(unsigned)blocks, kFwdThreads, smem, st>>>(
+      layers, n_layers, p, n_p, reinterpret_cast<const double2*>(omega), n_w, n_wtiles, tpb,
+      (flags & KR_FREE_SURFACE) ? 1 : 0, reinterpret_cast<double2*>(R));
+  return check_launch("kr_reflectivity");
 }
 
 }  // namespace kr
 
 using namespace kr;
+
+extern "C" void kr_set_forward_variant(int32_t min_blocks_per_sm) {
+  g_fwd_minb = (min_blocks_per_sm == 5 || min_blocks_per_sm == 6) ? min_blocks_per_sm : 4;
+}
 
 extern "C" kr_status kr_reflectivity(const double* layers, int32_t n_layers, const double* p,
                                      int32_t n_p, const double* omega, int32_t n_w,
@@ -48,16 +103,16 @@ extern "C" kr_status kr_reflectivity(const double* layers, int32_t n_layers, con
   const long long blocks = (long long)n_p * n_wtiles;
   if (blocks > 0x7fffffffLL) return KR_ERR_TOO_LARGE;
   const size_t smem = prologue_smem_bytes(n_layers);
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(reflectivity_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) {
-      set_last_error("kr_reflectivity: smem attribute", e);
-      return KR_ERR_CUDA;
-    }
+  cudaStream_t st = (cudaStream_t)stream;
+  switch (forward_minb()) {
+    case 6:
+      return launch_forward<6>(layers, n_layers, p, n_p, omega, n_w, n_wtiles, smem, flags, R,
+                               st);
+    case 5:
+      return launch_forward<5>(layers, n_layers, p, n_p, omega, n_w, n_wtiles, smem, flags, R,
+                               st);
+    default:
+      return launch_forward<4>(layers, n_layers, p, n_p, omega, n_w, n_wtiles, smem, flags, R,
+                               st);
   }
-  reflectivity_kernel<<<(unsigned)blocks, kFwdThreads, smem, (cudaStream_t)stream>>>(
-      layers, n_layers, p, n_p, reinterpret_cast<const double2*>(omega), n_w, n_wtiles,
-      (flags & KR_FREE_SURFACE) ? 1 : 0, reinterpret_cast<double2*>(R));
-  return check_launch("kr_reflectivity");
 }

@@ -1,0 +1,298 @@
+"""Continuous-batching request loop for forward and forward+gradient solves.
+
+Clients ``submit`` requests of any size (a model, its slowness and frequency grids, and for
+gradient requests the observed R) from any thread; each returns a ``Request`` whose
+``done`` event is the host-visible completion flag.  A scheduler thread:
+
+* admits pending requests in arrival order while the device-memory footprint of everything
+  admitted stays within ``hbm_budget_bytes`` and the batch has free slots
+  (``max_batch_requests``); a request that can never fit is rejected, one that cannot fit
+  *now* waits (no request is dropped silently);
+* launches each admitted group as one persistent batched launch (``ModelBatch``) on one of
+  ``n_streams`` streams, keeping up to ``max_inflight`` batches on the GPU at once, so
+  requests that arrive while others run are batched into the next launch and their work
+  overlaps on the device;
+* polls completion events, marks requests done (results stay on the device as tensors, in
+  the batch's buffers, until the client drops them) and returns their memory to the budget.
+
+The executor is pluggable (``executor=``); the default runs ``ModelBatch`` on the GPU.
+Latency is measured from ``submit`` to the moment the scheduler sets ``done``.
+"""
+
+from __future__ import annotations
+
+import collections
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .layer_model import LayerModel, pack_layers
+
+__all__ = ["Request", "KennettServer", "GpuBatchExecutor", "request_bytes",
+           "RequestRejected"]
+
+
+class RequestRejected(Exception):
+    """The request can never be served (invalid, larger than the budget, queue full)."""
+
+
+@dataclass
+class Request:
+    model: LayerModel
+    p: np.ndarray
+    omega: np.ndarray
+    gradient: bool = False
+    R_obs: np.ndarray | None = None
+    free_surface: bool = False
+    # filled by the server
+    id: int = -1
+    t_submit: float = 0.0
+    t_admit: float = 0.0
+    t_done: float = 0.0
+    nbytes: int = 0
+    done: threading.Event = field(default_factory=threading.Event)
+    result: dict | None = None
+    error: BaseException | None = None
+    cancelled: bool = False
+
+    def wait(self, timeout: float | None = None) -> dict:
+        if not self.done.wait(timeout):
+            raise TimeoutError(f"request {self.id} not done after {timeout} s")
+        if self.error is not None:
+            raise self.error
+        return self.result
+
+    @property
+    def latency(self) -> float:
+        return self.t_done - self.t_submit
+
+
+def request_bytes(model: LayerModel, n_p: int, n_w: int, gradient: bool) -> int:
+    """Device bytes one request occupies while admitted: inputs, outputs and its share of
+    the batch plan (per-slowness coefficient blocks)."""
+    L = model.n_layers
+    I = L - 1
+    b = 48 * L + 8 * n_p + 16 * n_w + 16 * n_p * n_w  # layers, p, omega, R
+    coef = 88 * L + 160 * I + 512
+    if gradient:
+        b += 16 * n_p * n_w + 8 * (4 * L + 1)  # R_obs, chi_grad
+        coef += 112 * L + 960 * I + 256
+    return int(b + n_p * coef + 64)
+
+
+class GpuBatchExecutor:
+    """Runs an admitted group as one ModelBatch launch on a stream; ``ready`` polls its event."""
+
+    def __init__(self, device=None, n_streams: int = 2, schedule=(128, 256)):
+        import torch
+
+        from . import device as D
+
+        self.torch = torch
+        self.dev = D.require_cuda(device)
+        self.streams = [torch.cuda.Stream(self.dev) for _ in range(n_streams)]
+        self.schedule = schedule
+        self._k = 0
+
+    def launch(self, reqs: list[Request]):
+        from .batch import BatchItem, ModelBatch
+
+        torch = self.torch
+        s = self.streams[self._k % len(self.streams)]
+        self._k += 1
+        with torch.cuda.stream(s):
+            items = [BatchItem(r.model, r.p, r.omega, gradient=r.gradient, R_obs=r.R_obs,
+                               free_surface=r.free_surface, store_R=r.gradient) for r in reqs]
+            batch = ModelBatch(items, schedule=self.schedule, device=self.dev)
+            batch.launch()
+            ev = torch.cuda.Event()
+            ev.record(s)
+        return (batch, ev)
+
+    def ready(self, handle) -> bool:
+        return handle[1].query()
+
+    def results(self, handle, reqs: list[Request]) -> list[dict]:
+        batch, _ = handle
+        out = []
+        for b, r in enumerate(reqs):
+            res = {"R": batch.reflectivity(b)}
+            if r.gradient:
+                chi, g = batch.misfit_gradient(b)
+                res["chi"], res["grad"] = chi, g
+            out.append(res)
+        return out
+
+
+class KennettServer:
+    """Continuous-batching server; see the module docstring."""
+
+    def __init__(self, executor=None, hbm_budget_bytes: int = 120 * 10**9,
+                 max_batch_requests: int = 256, max_inflight: int = 2,
+                 max_pending: int = 1_000_000, poll_interval: float = 50e-6,
+                 min_batch_wait: float = 0.0):
+        self.executor = executor if executor is not None else GpuBatchExecutor()
+        self.budget = int(hbm_budget_bytes)
+        self.max_batch = int(max_batch_requests)
+        self.max_inflight = int(max_inflight)
+        self.max_pending = int(max_pending)
+        self.poll = float(poll_interval)
+        self.min_batch_wait = float(min_batch_wait)
+        self._pending: collections.deque[Request] = collections.deque()
+        self._inflight: list[tuple[object, list[Request]]] = []
+        self._used = 0
+        self._lock = threading.Lock()
+        self._wake = threading.Condition(self._lock)
+        self._stop = False
+        self._next_id = 0
+        self.completed: list[Request] = []
+        self.batches_launched = 0
+        self.peak_bytes = 0
+        self._thread = threading.Thread(target=self._loop, name="kennett-server", daemon=True)
+        self._thread.start()
+
+    # -- client side ---------------------------------------------------------------------
+    def submit(self, model: LayerModel, p, omega, gradient: bool = False, R_obs=None,
+               free_surface: bool = False) -> Request:
+        p = np.ascontiguousarray(np.atleast_1d(p), dtype=np.float64)
+        omega = np.ascontiguousarray(np.atleast_1d(omega), dtype=np.complex128)
+        req = Request(model, p, omega, gradient, R_obs, free_surface)
+        req.t_submit = time.perf_counter()
+        try:
+            pack_layers(model)
+            if gradient:
+                if R_obs is None or np.shape(R_obs) != (len(p), len(omega)):
+                    raise ValueError("gradient request needs R_obs of shape (n_p, n_omega)")
+            if len(p) == 0 or len(omega) == 0:
+                raise ValueError("empty slowness or frequency grid")
+            req.nbytes = request_bytes(model, len(p), len(omega), gradient)
+            if req.nbytes > self.budget:
+                raise RequestRejected(f"request needs {req.nbytes} B > budget {self.budget} B")
+        except (ValueError, RequestRejected) as e:
+            req.error = e if isinstance(e, RequestRejected) else RequestRejected(str(e))
+            req.t_done = time.perf_counter()
+            req.done.set()
+            return req
+        with self._lock:
+            if len(self._pending) >= self.max_pending:
+                req.error = RequestRejected("queue full")
+                req.t_done = time.perf_counter()
+                req.done.set()
+                return req
+            req.id = self._next_id
+            self._next_id += 1
+            self._pending.append(req)
+            self._wake.notify()
+        return req
+
+    def cancel(self, req: Request) -> bool:
+        """Cancel a request that has not been admitted yet (True if it was)."""
+        with self._lock:
+            if req in self._pending:
+                self._pending.remove(req)
+                req.cancelled = True
+                req.error = RequestRejected("cancelled")
+                req.t_done = time.perf_counter()
+                req.done.set()
+                return True
+        return False
+
+    def close(self, timeout: float = 60.0) -> None:
+        with self._lock:
+            self._stop = True
+            self._wake.notify()
+        self._thread.join(timeout)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- scheduler -----------------------------------------------------------------------
+    def _admit(self) -> list[Request]:
+        group: list[Request] = []
+        while self._pending and len(group) < self.max_batch:
+            r = self._pending[0]
+            if self._used + r.nbytes > self.budget:
+                break  # FIFO: wait for memory to free up
+            self._pending.popleft()
+            self._used += r.nbytes
+            r.t_admit = time.perf_counter()
+            group.append(r)
+        self.peak_bytes = max(self.peak_bytes, self._used)
+        return group
+
+    def _complete(self) -> None:
+        still = []
+        for handle, reqs in self._inflight:
+            if self.executor.ready(handle):
+                try:
+                    res = self.executor.results(handle, reqs)
+                    err = None
+                except BaseException as e:  # device-side failure reported by the library
+                    res, err = [None] * len(reqs), e
+                now = time.perf_counter()
+                with self._lock:
+                    for r, x in zip(reqs, res):
+                        r.result, r.error, r.t_done = x, err, now
+                        self._used -= r.nbytes
+                        r.done.set()
+                        self.completed.append(r)
+            else:
+                still.append((handle, reqs))
+        self._inflight = still
+
+    def _loop(self) -> None:
+        while True:
+            self._complete()
+            with self._lock:
+                if self._stop and not self._pending and not self._inflight:
+                    return
+                group = []
+                if len(self._inflight) < self.max_inflight and self._pending:
+                    if self.min_batch_wait > 0 and not self._inflight:
+                        age = time.perf_counter() - self._pending[0].t_submit
+                        if age < self.min_batch_wait and len(self._pending) < self.max_batch:
+                            self._wake.wait(self.min_batch_wait - age)
+                            continue
+                    group = self._admit()
+                if not group and not self._inflight and not self._stop:
+                    self._wake.wait(0.01)
+                    continue
+            if group:
+                try:
+                    handle = self.executor.launch(group)
+                    self._inflight.append((handle, group))
+                    self.batches_launched += 1
+                except BaseException as e:
+                    now = time.perf_counter()
+                    with self._lock:
+                        for r in group:
+                            r.error, r.t_done = e, now
+                            self._used -= r.nbytes
+                            r.done.set()
+            elif self._inflight:
+                time.sleep(self.poll)
+
+    # -- statistics ----------------------------------------------------------------------
+    def stats(self, since: float = 0.0) -> dict:
+        with self._lock:
+            done = [r for r in self.completed if r.t_submit >= since and r.error is None]
+            waiting = len(self._pending)
+        if not done:
+            return {"completed": 0, "waiting": waiting}
+        lat = np.array([r.latency for r in done])
+        span = max(r.t_done for r in done) - min(r.t_submit for r in done)
+        return {
+            "completed": len(done),
+            "waiting": waiting,
+            "throughput_rps": len(done) / span if span > 0 else float("nan"),
+            "p50_ms": float(np.percentile(lat, 50) * 1e3),
+            "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "mean_ms": float(lat.mean() * 1e3),
+            "batches": self.batches_launched,
+            "peak_admitted_bytes": self.peak_bytes,
+        }

@@ -1,0 +1,120 @@
+"""Batched uneven models (kr_batch_*): every model's result equals the single-model entry
+points (forward: bit-identical, same arithmetic; gradient: 1e-12 relative, the batch adds
+block partials with atomics), for every schedule, through CUDA-graph replay and after
+in-place parameter updates; a sample of the uneven-batching workload against the oracle."""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_err
+from oracle import kennett_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _items(seed=0, n=36):
+    from seismicinversion_b200 import device as D
+    from seismicinversion_b200.batch import BatchItem
+    from seismicinversion_b200.earth_models import random_layered_model
+
+    rng = np.random.default_rng(seed)
+    items = []
+    for b in range(n):
+        n_sub = int(rng.choice([1, 2, 4, 20, 63]))
+        m = random_layered_model(n_sub, seed=1000 + b)
+        n_p = int(rng.choice([1, 3, 16]))
+        n_w = int(rng.choice([1, 7, 256, 300]))
+        p = np.sort(rng.uniform(0.0, 0.9, n_p))
+        w = np.arange(1, n_w + 1) * (2 * np.pi / 64) + (1j * np.pi / 64 if b % 3 == 0 else 0)
+        grad = b % 2 == 1
+        fs = b % 4 == 0
+        R_obs = None
+        if grad:
+            R_obs = D.reflectivity(D.layer_table(m), p, w, fs).cpu().numpy() * (1 + 0.05j)
+        items.append(BatchItem(m, p, w, gradient=grad, R_obs=R_obs, free_surface=fs,
+                               store_R=grad and b % 3 == 1))
+    return items
+
+
+def _check(batch, items):
+    from seismicinversion_b200 import device as D
+
+    for b, it in enumerate(items):
+        tab = D.layer_table(it.model)
+        if not it.gradient or it.store_R:
+            R1 = D.reflectivity(tab, it.p, it.omega, it.free_surface)
+            assert torch.equal(batch.reflectivity(b), R1), b
+        if it.gradient:
+            out, _ = D.misfit_gradient(tab, it.p, it.omega, it.R_obs, it.free_surface)
+            chi, g = batch.misfit_gradient(b)
+            L = it.model.n_layers
+            assert abs(float(chi) - float(out[4 * L])) <= 1e-12 * abs(float(out[4 * L])), b
+            assert rel_err(g.cpu().numpy(), out[:4 * L].cpu().numpy()) < 1e-12, b
+
+
+@pytest.mark.parametrize("schedule", [(64, 64), (128, 256), (128, 512)])
+def test_batch_matches_single_calls(schedule):
+    from seismicinversion_b200.batch import ModelBatch
+
+    items = _items()
+    batch = ModelBatch(items, schedule=schedule)
+    batch.launch()
+    torch.cuda.synchronize()
+    _check(batch, items)
+
+
+def test_graph_replay_and_inplace_update():
+    from seismicinversion_b200.batch import ModelBatch
+    from seismicinversion_b200.layer_model import LayerModel
+
+    items = _items(seed=1, n=20)
+    batch = ModelBatch(items, schedule=(128, 128))
+    batch.capture()
+    batch.run()
+    torch.cuda.synchronize()
+    _check(batch, items)
+    # perturb every model (same shapes), replay the same graph
+    new = []
+    for it in items:
+        m = it.model
+        new_m = LayerModel(m.alpha * 1.01, m.beta * 0.99, m.rho * 1.02, m.thickness, m.Q_alpha,
+                           m.Q_beta)
+        it.model = new_m
+        new.append(new_m)
+    batch.update_layers(new)
+    batch.run()
+    batch.run()
+    torch.cuda.synchronize()
+    _check(batch, items)
+
+
+def test_uneven_workload_sample_vs_oracle():
+    from seismicinversion_b200.batch import BatchItem, ModelBatch, autotune
+    from seismicinversion_b200.earth_models import uneven_batch_specs
+
+    specs = uneven_batch_specs(48, seed=3)
+    items = [BatchItem(m, p, w) for (m, p, w) in specs]
+    batch = ModelBatch(items)
+    best, times = autotune(batch, reps=1)
+    assert best in times and all(t > 0 for t in times.values())
+    batch.launch()
+    torch.cuda.synchronize()
+    small = sorted(range(len(specs)), key=lambda b: specs[b][0].n_layers * len(specs[b][1]) * len(specs[b][2]))[:6]
+    for b in small:
+        m, p, w = specs[b]
+        Ro = O.reflectivity(m.alpha, m.beta, m.rho, m.thickness, m.Q_alpha, m.Q_beta, p, w)
+        Rb = batch.reflectivity(b).cpu().numpy()
+        for j in range(len(p)):
+            assert rel_err(Rb[j], Ro[j]) < 1e-10, (b, j)
+
+
+def test_invalid_batches_rejected():
+    from seismicinversion_b200.batch import BatchItem, ModelBatch
+    from seismicinversion_b200.earth_models import random_layered_model
+
+    m = random_layered_model(3, seed=0)
+    with pytest.raises(ValueError):
+        ModelBatch([BatchItem(m, np.array([0.1]), np.array([1.0]), gradient=True)])
+    with pytest.raises(ValueError):
+        ModelBatch([BatchItem(m, np.array([0.1]), np.array([1.0]))], schedule=(96, 128))

@@ -1,0 +1,65 @@
+"""Serving on the GPU: a Poisson-like mix of forward and forward+gradient requests of uneven
+size; every result equals the single-call entry point (forward bit-identical, gradient
+1e-12), and one request gives the same result alone and inside the mix."""
+
+import time
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests(n, seed):
+    from seismicinversion_b200 import device as D
+    from seismicinversion_b200.earth_models import uneven_batch_specs
+
+    specs = uneven_batch_specs(n, seed=seed, nw_choices=(64, 128, 256), np_range=(4, 32))
+    out = []
+    for b, (m, p, w) in enumerate(specs):
+        grad = b % 2 == 1
+        obs = D.reflectivity(D.layer_table(m), p, w).cpu().numpy() * 0.98 if grad else None
+        out.append((m, p, w, grad, obs))
+    return out
+
+
+def _check(req):
+    from seismicinversion_b200 import device as D
+
+    res = req.wait(60)
+    tab = D.layer_table(req.model)
+    if req.gradient:
+        out, R = D.misfit_gradient(tab, req.p, req.omega, req.R_obs, want_R=True)
+        L = req.model.n_layers
+        assert rel_err(res["grad"].cpu().numpy(), out[:4 * L].cpu().numpy()) < 1e-12
+        assert torch.equal(res["R"], R)
+    else:
+        assert torch.equal(res["R"], D.reflectivity(tab, req.p, req.omega))
+    return res
+
+
+def test_mix_matches_single_calls_and_alone_vs_mix():
+    from seismicinversion_b200.serve import KennettServer
+
+    reqs = _requests(60, seed=5)
+    with KennettServer(max_batch_requests=16, max_inflight=2) as srv:
+        # the probe request, alone
+        m, p, w, g, o = reqs[1]
+        alone = srv.submit(m, p, w, gradient=g, R_obs=o)
+        a = _check(alone)
+        # ... and inside a stream of arrivals (exponential gaps, ~5k req/s)
+        rng = np.random.default_rng(0)
+        handles = []
+        for k, (m2, p2, w2, g2, o2) in enumerate(reqs):
+            handles.append(srv.submit(m2, p2, w2, gradient=g2, R_obs=o2))
+            time.sleep(rng.exponential(2e-4))
+        for h in handles:
+            _check(h)
+        mixed = handles[1]
+        assert rel_err(mixed.result["grad"].cpu().numpy(), a["grad"].cpu().numpy()) < 1e-12
+        assert torch.equal(mixed.result["R"], a["R"])
+        st = srv.stats()
+        assert st["completed"] == 61 and st["batches"] >= 2
