@@ -56,6 +56,10 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=0, help="slownesses in the CPU sample")
     ap.add_argument("--profile", action="store_true",
                     help="device steps only (no e2e, CPU baseline or peak probe): for ncu")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the inversion / batching / serving measurements")
+    ap.add_argument("--profile-kernel", choices=["inversion", "batch"], default=None,
+                    help="run only a small case of that workload (for ncu), no JSON line")
     return ap.parse_args()
 
 
@@ -129,6 +133,209 @@ def fp64_peak(torch, dev):
         b.synchronize()
         best = max(best, h.kr_bench_fp64_fma_flops(blocks, iters) / (a.elapsed_time(b) * 1e-3))
     return best / 1e12
+
+
+def _events(torch, st, fn, reps):
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fn()
+    a.record(st)
+    for _ in range(reps):
+        fn()
+    b.record(st)
+    b.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def bench_inversion(torch, dev, reps):
+    """tau-p inversion workload: 21-layer model (79 packed parameters), 64 slownesses on
+    [0.05, 0.6], omega_k = k 2pi/64 (k = 1..1024), start = true * exp(0.1 N(0,1)) (seed 2)."""
+    from seismicinversion_b200 import device as D
+    from seismicinversion_b200.earth_models import random_layered_model
+    from seismicinversion_b200.kennett_torch import model_to_tensors
+    from seismicinversion_b200.taup_inversion import invert_taup
+
+    true = random_layered_model(20, seed=2)
+    rng = np.random.default_rng(2)
+    start = random_layered_model(20, seed=2)
+    for name in ("alpha", "beta", "rho"):
+        getattr(start, name)[1:] *= np.exp(0.1 * rng.standard_normal(20))
+    start.thickness[1:-1] *= np.exp(0.1 * rng.standard_normal(19))
+    p = np.linspace(0.05, 0.6, 64)
+    w = np.arange(1, 1025) * (2 * np.pi / 64)
+    st = torch.cuda.current_stream(dev)
+    tab_true, tab = D.layer_table(true, dev), D.layer_table(start, dev)
+    p_t, w_t = torch.as_tensor(p, device=dev), torch.as_tensor(w, device=dev).to(torch.complex128)
+    R_obs = D.reflectivity(tab_true, p_t, w_t)
+    ms_grad = _events(torch, st, lambda: D.misfit_gradient(tab, p_t, w_t, R_obs), reps)
+    ms_jac = _events(torch, st, lambda: D.jacobian(tab, p_t, w_t, want_R=False), reps)
+    ms_fwd = _events(torch, st, lambda: D.reflectivity(tab, p_t, w_t), reps)
+    upd = 64 * 1024 * 20
+    t = model_to_tensors(true)
+    init = np.concatenate([start.alpha[1:], start.beta[1:], start.rho[1:], start.thickness[1:-1]])
+    out = {"workload": "tau-p LM, 21 layers / 79 params, 64 p x 1024 omega",
+           "grad_evals_per_s": 1e3 / ms_grad, "ms_per_grad_eval": ms_grad,
+           "adjoint_updates_per_s": upd / (ms_grad * 1e-3),
+           "ms_per_jacobian": ms_jac, "ms_per_forward": ms_fwd}
+    for hess in ("gauss-newton", "exact"):
+        its = 10 if hess == "gauss-newton" else 2
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = invert_taup(true, list(p), nfreq=1024, max_iter=its, hessian=hess,
+                          initial_params=init, tol=0.0)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        out[f"lm_{hess}"] = {"iterations": res.n_iterations, "seconds": dt,
+                             "s_per_iteration": dt / max(res.n_iterations, 1),
+                             "param_err_first_last": [res.param_error_history[0],
+                                                      res.param_error_history[-1]]}
+    return out
+
+
+def bench_batched(torch, dev, reps, n_models=4096):
+    """Uneven batching workload: 4096 models, total layers U{3..64}, n_omega in
+    {256, 512, 1024, 2048}, n_p U{16..256} on (0, 0.8] (seed 3); odd models ask for forward +
+    gradient against the R of an independently perturbed model (seed 4)."""
+    from seismicinversion_b200 import device as D
+    from seismicinversion_b200.batch import BatchItem, ModelBatch, autotune
+    from seismicinversion_b200.earth_models import uneven_batch_specs
+    from seismicinversion_b200.layer_model import LayerModel
+
+    specs = uneven_batch_specs(n_models, seed=3)
+    rng = np.random.default_rng(4)
+    perturbed = []
+    for m, p, w in specs:
+        f = np.exp(0.03 * rng.standard_normal(m.n_layers))
+        perturbed.append(LayerModel(m.alpha * f, m.beta * f, m.rho, m.thickness, m.Q_alpha, m.Q_beta))
+    obs_batch = ModelBatch([BatchItem(perturbed[b], specs[b][1], specs[b][2])
+                            for b in range(1, n_models, 2)], device=dev)
+    obs_batch.launch()
+    items = []
+    for b, (m, p, w) in enumerate(specs):
+        if b % 2:
+            items.append(BatchItem(m, p, w, gradient=True, R_obs=obs_batch.reflectivity(b // 2)))
+        else:
+            items.append(BatchItem(m, p, w))
+    batch = ModelBatch(items, device=dev)
+    best, times = autotune(batch, candidates=[(64, 128), (128, 256), (128, 512)], reps=1)
+    batch.capture()
+    st = torch.cuda.current_stream(dev)
+    ms = _events(torch, st, batch.run, reps)
+    work = batch.work()
+    # plain per-call paths on samples: one call per model (all slownesses), and one call per
+    # (model, slowness) as the reference's API issues them; synchronised after each call
+    # odd stride: the sample alternates forward and forward+gradient models like the batch
+    sample = list(range(0, n_models, 31))[:128]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for b in sample:
+        it = items[b]
+        tab = D.layer_table(it.model, dev)
+        if it.gradient:
+            D.misfit_gradient(tab, it.p, it.omega, it.R_obs.reshape(len(it.p), -1))
+        else:
+            D.reflectivity(tab, it.p, it.omega)
+        torch.cuda.synchronize()
+    per_model = (time.perf_counter() - t0) / len(sample)
+    sample_p = sample[:16]  # 8 forward + 8 gradient models
+    calls = 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for b in sample_p:
+        it = items[b]
+        tab = D.layer_table(it.model, dev)
+        Ro = it.R_obs.reshape(len(it.p), -1) if it.gradient else None
+        for j in range(len(it.p)):
+            if it.gradient:
+                D.misfit_gradient(tab, it.p[j:j + 1], it.omega, Ro[j:j + 1])
+            else:
+                D.reflectivity(tab, it.p[j:j + 1], it.omega)
+            torch.cuda.synchronize()
+            calls += 1
+    per_pair_call = (time.perf_counter() - t0) / calls
+    n_pairs = sum(len(it.p) for it in items)
+    batched_models_per_s = n_models / (ms * 1e-3)
+    return {"workload": "4096 uneven models, half forward+gradient", "schedule": list(best),
+            "autotune_ms": {str(k): v for k, v in times.items()}, "ms_per_batch": ms,
+            "models_per_s": batched_models_per_s, **work,
+            "updates_per_s": (work["forward_updates"] + work["gradient_updates"]) / (ms * 1e-3),
+            "plain_per_model_call_models_per_s": 1.0 / per_model,
+            "plain_per_slowness_call_models_per_s": n_models / (per_pair_call * n_pairs),
+            "speedup_vs_per_model_calls": batched_models_per_s * per_model,
+            "speedup_vs_per_slowness_calls": batched_models_per_s * per_pair_call * n_pairs / n_models,
+            "graph_captured": True}
+
+
+def bench_serving(torch, dev, rates=(100, 1000, 3000, 10000, 20000), duration=1.0,
+                  max_requests=3000):
+    """Serving workload: Poisson arrivals (seed 7) of requests drawn as in the batching
+    workload (50/50 forward / forward+gradient), device-resident inputs, 120 GB budget."""
+    from seismicinversion_b200 import device as D
+    from seismicinversion_b200.earth_models import uneven_batch_specs
+    from seismicinversion_b200.serve import KennettServer
+
+    specs = uneven_batch_specs(256, seed=5)
+    pool = []
+    for b, (m, p, w) in enumerate(specs):
+        p_t = torch.as_tensor(p, device=dev)
+        w_t = torch.as_tensor(w, device=dev).to(torch.complex128)
+        obs = None
+        if b % 2:
+            obs = D.reflectivity(D.layer_table(m, dev), p_t, w_t) * 1.01
+        pool.append((m, p_t, w_t, b % 2 == 1, obs))
+    torch.cuda.synchronize()
+    rng = np.random.default_rng(7)
+    out = {"workload": "Poisson stream, uneven models as the batching workload, 50/50 fwd/grad"}
+    # warm-up: streams, kernel modules and pinned staging buffers of the server path
+    with KennettServer(hbm_budget_bytes=120 * 10**9, max_batch_requests=64, max_inflight=2) as srv:
+        for k in range(8):
+            m, p_t, w_t, g, obs = pool[k]
+            srv.submit(m, p_t, w_t, gradient=g, R_obs=obs).wait(60)
+    for lam in rates:
+        n = int(min(max_requests, lam * duration))
+        gaps = rng.exponential(1.0 / lam, n)
+        with KennettServer(hbm_budget_bytes=120 * 10**9, max_batch_requests=64,
+                           max_inflight=2) as srv:
+            t_start = time.perf_counter()
+            t_next = t_start
+            reqs = []
+            for k in range(n):
+                t_next += gaps[k]
+                dt = t_next - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)  # releases the GIL to the scheduler thread
+                m, p_t, w_t, g, obs = pool[k % len(pool)]
+                reqs.append(srv.submit(m, p_t, w_t, gradient=g, R_obs=obs))
+            for r in reqs:
+                r.wait(120)
+            stats = srv.stats(since=t_start)
+        out[f"rate_{lam}"] = {k: stats[k] for k in ("completed", "throughput_rps", "p50_ms",
+                                                     "p99_ms", "batches")}
+    # plain per-request path (one launch + sync per request, FIFO) at a moderate rate
+    lam = 300
+    n = int(lam * duration)
+    gaps = rng.exponential(1.0 / lam, n)
+    lat = []
+    t_next = time.perf_counter()
+    arrivals = []
+    for k in range(n):
+        t_next += gaps[k]
+        arrivals.append(t_next)
+    for k in range(n):
+        while time.perf_counter() < arrivals[k]:
+            pass
+        m, p_t, w_t, g, obs = pool[k % len(pool)]
+        tab = D.layer_table(m, dev)
+        if g:
+            D.misfit_gradient(tab, p_t, w_t, obs)
+        else:
+            D.reflectivity(tab, p_t, w_t)
+        torch.cuda.synchronize()
+        lat.append(time.perf_counter() - arrivals[k])
+    lat = np.array(lat)
+    out["plain_per_request_rate_300"] = {"p50_ms": float(np.percentile(lat, 50) * 1e3),
+                                         "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                                         "throughput_rps": n / (time.perf_counter() - arrivals[0])}
+    return out
 
 
 def run_ours(args, rank, world, local):
@@ -295,6 +502,12 @@ def run_ours(args, rank, world, local):
                "seconds": samples[-1]}
         cpu_base.close()
 
+    extra = {}
+    if world == 1 and not args.no_extra:
+        extra["inversion"] = bench_inversion(torch, dev, max(args.steps, 3))
+        extra["batched"] = bench_batched(torch, dev, max(args.steps, 2))
+        extra["serving"] = bench_serving(torch, dev)
+
     if rank == 0:
         line = {
             "metric": "(omega,p,interface) reflectivity updates/s, 21-layer gather workload (R grid + J0 gather + traces)",
@@ -309,6 +522,7 @@ def run_ours(args, rank, world, local):
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": 5 * args.steps, "clocks": clocks, "kernels": kernels,
             "max_rel_err_vs_oracle_sample": accuracy,
+            **extra,
         }
         print(json.dumps(line))
     if dist:
@@ -355,8 +569,48 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+def profile_case(kind):
+    """Small cases for ncu captures: the inversion gradient / Jacobian (64 p x 1024 omega,
+    21 layers) or a 256-model uneven batch (seed 3, half gradient)."""
+    import torch
+
+    from seismicinversion_b200 import device as D
+
+    dev = D.require_cuda()
+    if kind == "inversion":
+        from seismicinversion_b200.earth_models import random_layered_model
+
+        true, start = random_layered_model(20, seed=2), random_layered_model(20, seed=2)
+        start.alpha[1:] *= 1.05
+        p = torch.as_tensor(np.linspace(0.05, 0.6, 64), device=dev)
+        w = torch.as_tensor(np.arange(1, 1025) * (2 * np.pi / 64), device=dev).to(torch.complex128)
+        R_obs = D.reflectivity(D.layer_table(true, dev), p, w)
+        tab = D.layer_table(start, dev)
+        for _ in range(3):
+            D.misfit_gradient(tab, p, w, R_obs)
+            D.jacobian(tab, p, w, want_R=False)
+    else:
+        from seismicinversion_b200.batch import BatchItem, ModelBatch
+        from seismicinversion_b200.earth_models import uneven_batch_specs
+
+        items = []
+        for b, (m, p, w) in enumerate(uneven_batch_specs(256, seed=3)):
+            if b % 2:
+                Ro = D.reflectivity(D.layer_table(m, dev), p, w) * 1.01
+                items.append(BatchItem(m, p, w, gradient=True, R_obs=Ro))
+            else:
+                items.append(BatchItem(m, p, w))
+        batch = ModelBatch(items, schedule=(128, 512), device=dev)
+        for _ in range(2):
+            batch.launch()
+    torch.cuda.synchronize()
+
+
 def main():
     args = parse()
+    if args.profile_kernel:
+        profile_case(args.profile_kernel)
+        return
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)

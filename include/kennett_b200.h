@@ -259,6 +259,13 @@ kr_status kr_batch_launch(void* plan, const kr_batch_config* cfg, int32_t max_la
  */
 void kr_set_forward_variant(int32_t min_blocks_per_sm);
 
+/*
+ * Tuning knob (no counterpart in the reference): register budget of the kr_jacobian /
+ * kr_misfit_gradient sweep kernel as 128-thread blocks per SM (2 -> up to 255 registers,
+ * 3 -> 168; other values select 2).  Process-wide; results do not depend on it.
+ */
+void kr_set_deriv_variant(int32_t min_blocks_per_sm);
+
 #ifdef __cplusplus
 }
 #endif

@@ -66,6 +66,7 @@ _SIGNATURES = {
     "kr_traces_workspace_bytes": (_size_t, [_i32, _i32]),
     "kr_traces": (_i32, [_vp, _vp, _i32, _i32, _vp, _vp, _vp, _size_t, _vp]),
     "kr_set_forward_variant": (None, [_i32]),
+    "kr_set_deriv_variant": (None, [_i32]),
     "kr_batch_plan_bytes": (_size_t, [_vp, _i32, _vp]),
     "kr_batch_plan": (_i32, [_vp, _i32, _vp, _vp, _size_t, _vp]),
     "kr_batch_plan_meta_bytes": (_size_t, [_vp, _i32, _vp]),

@@ -51,8 +51,28 @@ class BatchItem:
     store_R: bool = False
 
 
+def _flat(x, dtype) -> torch.Tensor:
+    """1-D tensor view of x (numpy or torch, host or device) in the given dtype."""
+    if isinstance(x, torch.Tensor):
+        return x.detach().to(dtype).reshape(-1)
+    return torch.as_tensor(np.ascontiguousarray(x)).to(dtype).reshape(-1)
+
+
+def _cat(parts, dtype, dev) -> torch.Tensor:
+    """Concatenate on the device (host parts are copied once, device parts stay put)."""
+    if not parts:
+        return torch.zeros(1, dtype=dtype, device=dev)
+    host = [t for t in parts if not t.is_cuda]
+    if len(host) == len(parts):
+        return torch.cat(parts).to(dev, non_blocking=False)
+    return torch.cat([t.to(dev) for t in parts])
+
+
 class ModelBatch:
-    """Device-resident packed batch with its plan; see the module docstring."""
+    """Device-resident packed batch with its plan; see the module docstring.
+
+    ``p``, ``omega`` and ``R_obs`` of the items may be NumPy arrays or (CUDA) tensors; device
+    tensors are concatenated on the device without a host round trip."""
 
     def __init__(self, items: list[BatchItem], schedule: tuple[int, int] | None = None,
                  device=None):
@@ -67,39 +87,41 @@ class ModelBatch:
             tab = pack_layers(it.model)
             D.validate_table(tab)
             L = tab.shape[1]
-            p = np.ascontiguousarray(it.p, dtype=np.float64).reshape(-1)
-            w = np.ascontiguousarray(it.omega, dtype=np.complex128).reshape(-1)
+            p = _flat(it.p, torch.float64)
+            w = _flat(it.omega, torch.complex128)
+            n_p, n_w = p.numel(), w.numel()
             flags = _lib.KR_FREE_SURFACE if it.free_surface else 0
             if it.gradient:
                 if it.R_obs is None:
                     raise ValueError(f"batch item {b}: gradient requested without R_obs")
-                o = np.ascontiguousarray(it.R_obs, dtype=np.complex128).reshape(len(p), len(w))
+                o = _flat(it.R_obs, torch.complex128)
+                if o.numel() != n_p * n_w:
+                    raise ValueError(f"batch item {b}: R_obs must have shape ({n_p}, {n_w})")
                 flags |= _lib.KR_BATCH_GRADIENT | (_lib.KR_BATCH_STORE_R if it.store_R else 0)
             d = desc[b]
-            d["n_layers"], d["n_p"], d["n_w"], d["flags"] = L, len(p), len(w), flags
+            d["n_layers"], d["n_p"], d["n_w"], d["flags"] = L, n_p, n_w, flags
             d["layers_off"], d["p_off"], d["omega_off"] = lo, po, wo
             tabs.append(tab.ravel())
             ps.append(p)
             ws.append(w)
             lo += tab.size
-            po += len(p)
-            wo += len(w)
+            po += n_p
+            wo += n_w
             if (not it.gradient) or it.store_R:
                 d["R_off"] = ro
-                ro += len(p) * len(w)
+                ro += n_p * n_w
             if it.gradient:
                 d["obs_off"], d["grad_off"] = oo, go
-                obs.append(o.ravel())
-                oo += o.size
+                obs.append(o)
+                oo += o.numel()
                 go += 4 * L + 1
             self.max_layers = max(self.max_layers, L)
         self.desc = desc
         dev = self.dev
         self.layers = torch.as_tensor(np.concatenate(tabs) if tabs else np.zeros(1), device=dev)
-        self.p = torch.as_tensor(np.concatenate(ps) if ps else np.zeros(1), device=dev)
-        self.omega = torch.as_tensor(np.concatenate(ws) if ws else np.zeros(1, np.complex128),
-                                     device=dev)
-        self.R_obs = torch.as_tensor(np.concatenate(obs), device=dev) if obs else None
+        self.p = _cat(ps, torch.float64, dev)
+        self.omega = _cat(ws, torch.complex128, dev)
+        self.R_obs = _cat(obs, torch.complex128, dev) if obs else None
         self.R = torch.empty(max(ro, 1), dtype=torch.complex128, device=dev)
         self.chi_grad = torch.zeros(max(go, 1), dtype=torch.float64, device=dev)
         self.graph = None

@@ -152,6 +152,13 @@ KR_HD void kennett_step_reverse(const M2& r, cd ea, cd eb, const Iface& f, const
   cbar[9] = Tdb.d;
 }
 
+// Bytes of one slowness's derivative data in shared memory (layer terms, layer derivative
+// factors, interface coefficients, coefficient tangents), 16-byte aligned sections.
+KR_HD size_t pair_smem_bytes(int L) {
+  return sizeof(LayerP) * (size_t)L + sizeof(LayerD) * (size_t)L +
+         sizeof(Iface) * (size_t)(L - 1) + sizeof(ScatTan) * (size_t)(L - 1);
+}
+
 // dR/d(alpha, beta, rho, h) of one layer.
 struct Acc {
   cd a, b, r, h;
@@ -222,20 +229,24 @@ KR_HD void jacobian_pair(int L, cd w, bool free_surface, int seg, const LayerP* 
   cur.a = f0 * dlay[0].ca_alpha;
   cur.h = f0 * dlay[0].ca_h;
   M2 sg[kSegMax];
+  cd sea[kSegMax], seb[kSegMax];
   const int ncp = nsteps > 0 ? (nsteps + seg - 1) / seg : 0;
   for (int q = ncp - 1; q >= 0; --q) {
     const int s0 = q * seg;
     const int s1 = s0 + seg < nsteps ? s0 + seg : nsteps;
     M2 x = cp[q];
+    // recompute the segment's step inputs and phase factors from its checkpoint
     for (int s = s0; s < s1; ++s) {
-      sg[s - s0] = x;
       const int i = I - 2 - s;
-      if (s + 1 < s1)
-        x = kennett_step(x, cexp_(w * lay[i + 1].ca), cexp_(w * lay[i + 1].cb), coef[i]);
+      const cd ea = cexp_(w * lay[i + 1].ca), eb = cexp_(w * lay[i + 1].cb);
+      sg[s - s0] = x;
+      sea[s - s0] = ea;
+      seb[s - s0] = eb;
+      if (s + 1 < s1) x = kennett_step(x, ea, eb, coef[i]);
     }
     for (int s = s1 - 1; s >= s0; --s) {
       const int i = I - 2 - s;  // interface i, lower layer i + 1
-      const cd ea = cexp_(w * lay[i + 1].ca), eb = cexp_(w * lay[i + 1].cb);
+      const cd ea = sea[s - s0], eb = seb[s - s0];
       M2 rb;
       cd eab, ebb, cbar[10];
       kennett_step_reverse(sg[s - s0], ea, eb, coef[i], ob, rb, eab, ebb, cbar);

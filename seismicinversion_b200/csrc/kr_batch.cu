@@ -135,6 +135,7 @@ template <int THREADS>
 __global__ void __launch_bounds__(THREADS)
 batch_forward_kernel(unsigned char* plan, const double2* __restrict__ omega_all,
                      double2* __restrict__ R_all) {
+  extern __shared__ __align__(16) unsigned char s_pair[];  // layer terms + coefficients
   PlanHeader* h = reinterpret_cast<PlanHeader*>(plan);
   const kr_model_desc* models = reinterpret_cast<const kr_model_desc*>(plan + h->off_models);
   const PairRec* pairs = reinterpret_cast<const PairRec*>(plan + h->off_pairs);
@@ -148,27 +149,31 @@ batch_forward_kernel(unsigned char* plan, const double2* __restrict__ omega_all,
     const kr_model_desc d = models[pr.model];
     const PairView v = pair_view(plan, pr, d);
     const bool fs = (d.flags & KR_FREE_SURFACE) != 0;
+    LayerP* lay = reinterpret_cast<LayerP*>(s_pair);
+    Iface* coef = reinterpret_cast<Iface*>(s_pair + sizeof(LayerP) * d.n_layers);
+    copy16(lay, v.lay, sizeof(LayerP) * d.n_layers);
+    copy16(coef, v.coef, sizeof(Iface) * (d.n_layers - 1));
+    __syncthreads();
     for (int k = threadIdx.x; k < item.nw; k += THREADS) {
       const int iw = item.w0 + k;
       const double2 wv = omega_all[d.omega_off + iw];
       const cd w = mk(wv.x, wv.y);
-      const cd rpp = sweep(w, d.n_layers, v.lay, v.coef);
-      const cd out = pp_surface(rpp, cexp_(w * v.lay[0].ca), fs);
+      const cd rpp = sweep(w, d.n_layers, lay, coef);
+      const cd out = pp_surface(rpp, cexp_(w * lay[0].ca), fs);
       R_all[d.R_off + (size_t)pr.j * d.n_w + iw] = make_double2(out.x, out.y);
     }
   }
 }
 
-// Per-thread sink for gradient items: accumulates 2 Re(conj(res) dR/dtheta) per layer into
-// block shared memory (warp shuffles, then warps in order).
+// Per-thread sink for gradient items: 2 Re(conj(res) dR/dtheta) per layer, reduced over the
+// warp by shuffles into the warp's own accumulator row (no block barrier inside the sweep).
 template <int THREADS>
 struct BatchGradSink {
   bool valid;
   cd res;
   const double2* obs;
   double2* R_out;
-  double* s_acc;   // [4L + 1]
-  double* s_warp;  // [THREADS / 32 * 4]
+  double* row;  // this warp's [4L + 1] accumulators
   int L;
   __device__ void reflectivity(cd R) {
     res = mk(0.0, 0.0);
@@ -188,16 +193,8 @@ struct BatchGradSink {
 #pragma unroll
     for (int k = 0; k < 4; ++k)
       for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
-    const int warp = threadIdx.x >> 5;
     if ((threadIdx.x & 31) == 0)
-      for (int k = 0; k < 4; ++k) s_warp[warp * 4 + k] = v[k];
-    __syncthreads();
-    if (threadIdx.x < 4) {
-      double t = 0.0;
-      for (int w = 0; w < THREADS / 32; ++w) t += s_warp[w * 4 + threadIdx.x];
-      s_acc[threadIdx.x * L + l] += t;
-    }
-    __syncthreads();
+      for (int k = 0; k < 4; ++k) row[k * L + l] += v[k];
   }
 };
 
@@ -205,10 +202,9 @@ template <int THREADS>
 __global__ void __launch_bounds__(THREADS)
 batch_gradient_kernel(unsigned char* plan, const double2* __restrict__ omega_all,
                       const double2* __restrict__ obs_all, double2* __restrict__ R_all,
-                      double* __restrict__ chi_grad) {
-  extern __shared__ double s_dyn[];
-  double* s_warp = s_dyn;                    // [THREADS / 32 * 4]
-  double* s_acc = s_dyn + THREADS / 32 * 4;  // [4L + 1]
+                      double* __restrict__ chi_grad, int stage) {
+  // [THREADS / 32][4L + 1] accumulators (padded to 16 bytes), then the item's slowness data
+  extern __shared__ __align__(16) double s_wacc[];
   PlanHeader* h = reinterpret_cast<PlanHeader*>(plan);
   const kr_model_desc* models = reinterpret_cast<const kr_model_desc*>(plan + h->off_models);
   const PairRec* pairs = reinterpret_cast<const PairRec*>(plan + h->off_pairs);
@@ -220,10 +216,28 @@ batch_gradient_kernel(unsigned char* plan, const double2* __restrict__ omega_all
     const ItemRec item = items[it];
     const PairRec pr = pairs[item.pair];
     const kr_model_desc d = models[pr.model];
-    const PairView v = pair_view(plan, pr, d);
+    PairView v = pair_view(plan, pr, d);
     const int L = d.n_layers;
-    for (int k = threadIdx.x; k < 4 * L + 1; k += THREADS) s_acc[k] = 0.0;
+    const int nv = 4 * L + 1;
+    for (int k = threadIdx.x; k < (THREADS / 32) * nv; k += THREADS) s_wacc[k] = 0.0;
+    if (stage) {
+      unsigned char* b = reinterpret_cast<unsigned char*>(s_wacc + ((THREADS / 32) * nv + 1) / 2 * 2);
+      ScatTan* st = reinterpret_cast<ScatTan*>(b);
+      Iface* sc = reinterpret_cast<Iface*>(b + sizeof(ScatTan) * (L - 1));
+      LayerP* sl = reinterpret_cast<LayerP*>(b + (sizeof(ScatTan) + sizeof(Iface)) * (L - 1));
+      LayerD* sd = reinterpret_cast<LayerD*>(reinterpret_cast<unsigned char*>(sl) +
+                                             sizeof(LayerP) * L);
+      copy16(st, v.tan, sizeof(ScatTan) * (L - 1));
+      copy16(sc, v.coef, sizeof(Iface) * (L - 1));
+      copy16(sl, v.lay, sizeof(LayerP) * L);
+      copy16(sd, v.dlay, sizeof(LayerD) * L);
+      v.tan = st;
+      v.coef = sc;
+      v.lay = sl;
+      v.dlay = sd;
+    }
     __syncthreads();
+    double* row = s_wacc + (threadIdx.x >> 5) * nv;
     const int seg = checkpoint_spacing(L - 2 > 0 ? L - 2 : 1);
     const bool fs = (d.flags & KR_FREE_SURFACE) != 0;
     for (int k0 = 0; k0 < item.nw; k0 += THREADS) {
@@ -237,25 +251,21 @@ batch_gradient_kernel(unsigned char* plan, const double2* __restrict__ omega_all
       BatchGradSink<THREADS> sink;
       sink.valid = valid;
       sink.L = L;
-      sink.s_acc = s_acc;
-      sink.s_warp = s_warp;
+      sink.row = row;
       const size_t e = (size_t)pr.j * d.n_w + (valid ? iw : 0);
       sink.obs = obs_all + d.obs_off + e;
       sink.R_out = (d.flags & KR_BATCH_STORE_R) ? R_all + d.R_off + e : nullptr;
       jacobian_pair(L, w, fs, seg, v.lay, v.dlay, v.coef, v.tan, sink);
       double c2 = valid ? (sink.res.x * sink.res.x + sink.res.y * sink.res.y) : 0.0;
       for (int o = 16; o > 0; o >>= 1) c2 += __shfl_down_sync(0xffffffffu, c2, o);
-      if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = c2;
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int wi = 0; wi < THREADS / 32; ++wi) t += s_warp[wi];
-        s_acc[4 * L] += t;
-      }
-      __syncthreads();
+      if ((threadIdx.x & 31) == 0) row[4 * L] += c2;
     }
-    for (int k = threadIdx.x; k < 4 * L + 1; k += THREADS)
-      atomicAdd(chi_grad + d.grad_off + k, s_acc[k]);
+    __syncthreads();
+    for (int k = threadIdx.x; k < nv; k += THREADS) {
+      double t = 0.0;
+      for (int wi = 0; wi < THREADS / 32; ++wi) t += s_wacc[wi * nv + k];
+      atomicAdd(chi_grad + d.grad_off + k, t);
+    }
   }
 }
 
@@ -355,11 +365,35 @@ static kr_status layout(const kr_model_desc* descs, int n_models, const kr_batch
   return KR_OK;
 }
 
+constexpr size_t kBatchStageMax = 160 * 1024;
+
+static size_t fwd_smem(int max_layers) {
+  return sizeof(LayerP) * (size_t)max_layers + sizeof(Iface) * (size_t)(max_layers - 1);
+}
+
+// gradient kernel dynamic smem and whether the slowness data is staged
+static size_t grad_smem(int threads, int max_layers, int* stage) {
+  const size_t acc = sizeof(double) * (((size_t)(threads / 32) * (4 * max_layers + 1) + 1) / 2 * 2);
+  const size_t pair = pair_smem_bytes(max_layers);
+  *stage = (acc + pair <= kBatchStageMax) ? 1 : 0;
+  return acc + (*stage ? pair : 0);
+}
+
 template <int THREADS>
-static void grids(PlanHeader& h, int max_layers) {
-  h.grid_fwd = occupancy_grid((const void*)batch_forward_kernel<THREADS>, THREADS, 0);
-  const size_t smem = sizeof(double) * (THREADS / 32 * 4 + 4 * (size_t)max_layers + 1);
-  h.grid_grad = occupancy_grid((const void*)batch_gradient_kernel<THREADS>, THREADS, smem);
+static kr_status grids(PlanHeader& h, int max_layers, size_t* fsm, size_t* gsm, int* stage) {
+  *fsm = fwd_smem(max_layers);
+  *gsm = grad_smem(THREADS, max_layers, stage);
+  if (*fsm > 48 * 1024 &&
+      cudaFuncSetAttribute(batch_forward_kernel<THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)*fsm) != cudaSuccess)
+    return KR_ERR_CUDA;
+  if (*gsm > 48 * 1024 &&
+      cudaFuncSetAttribute(batch_gradient_kernel<THREADS>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*gsm) != cudaSuccess)
+    return KR_ERR_CUDA;
+  h.grid_fwd = occupancy_grid((const void*)batch_forward_kernel<THREADS>, THREADS, *fsm);
+  h.grid_grad = occupancy_grid((const void*)batch_gradient_kernel<THREADS>, THREADS, *gsm);
+  return KR_OK;
 }
 
 }  // namespace kr
@@ -448,33 +482,37 @@ extern "C" kr_status kr_batch_launch(void* plan, const kr_batch_config* cfg, int
   if (max_layers < 2 || max_layers > kMaxLayers) return KR_ERR_INVALID_ARGUMENT;
   cudaStream_t st = (cudaStream_t)stream;
   unsigned char* pl = static_cast<unsigned char*>(plan);
-  // Grid sizes come from the same occupancy query the plan used (host-side, capture-safe).
+  // Grid sizes from an occupancy query (host-side, capture-safe).
   PlanHeader h{};
-  h.threads = cfg->threads;
-  if (cfg->threads == 64)
-    grids<64>(h, max_layers);
-  else
-    grids<128>(h, max_layers);
+  size_t fsm = 0, gsm = 0;
+  int stage = 0;
+  kr_status s = (cfg->threads == 64) ? grids<64>(h, max_layers, &fsm, &gsm, &stage)
+                                     : grids<128>(h, max_layers, &fsm, &gsm, &stage);
+  if (s != KR_OK) {
+    set_last_error_msg("kr_batch_launch: shared-memory attribute");
+    return s;
+  }
   batch_reset_kernel<<<148, 128, 0, st>>>(pl, chi_grad);
-  kr_status s = check_launch("kr_batch_launch: reset");
+  s = check_launch("kr_batch_launch: reset");
   if (s != KR_OK) return s;
   batch_prep_kernel<<<148 * 16, 64, 0, st>>>(pl, layers, p);
   s = check_launch("kr_batch_launch: prep");
   if (s != KR_OK) return s;
   const double2* w = reinterpret_cast<const double2*>(omega);
-  const size_t gsmem = sizeof(double) * (cfg->threads / 32 * 4 + 4 * (size_t)max_layers + 1);
   if (cfg->threads == 64) {
-    batch_forward_kernel<64><<<h.grid_fwd, 64, 0, st>>>(pl, w, reinterpret_cast<double2*>(R));
+    batch_forward_kernel<64><<<h.grid_fwd, 64, fsm, st>>>(pl, w, reinterpret_cast<double2*>(R));
     s = check_launch("kr_batch_launch: forward");
     if (s != KR_OK) return s;
-    batch_gradient_kernel<64><<<h.grid_grad, 64, gsmem, st>>>(
-        pl, w, reinterpret_cast<const double2*>(R_obs), reinterpret_cast<double2*>(R), chi_grad);
+    batch_gradient_kernel<64><<<h.grid_grad, 64, gsm, st>>>(
+        pl, w, reinterpret_cast<const double2*>(R_obs), reinterpret_cast<double2*>(R), chi_grad,
+        stage);
   } else {
-    batch_forward_kernel<128><<<h.grid_fwd, 128, 0, st>>>(pl, w, reinterpret_cast<double2*>(R));
+    batch_forward_kernel<128><<<h.grid_fwd, 128, fsm, st>>>(pl, w, reinterpret_cast<double2*>(R));
     s = check_launch("kr_batch_launch: forward");
     if (s != KR_OK) return s;
-    batch_gradient_kernel<128><<<h.grid_grad, 128, gsmem, st>>>(
-        pl, w, reinterpret_cast<const double2*>(R_obs), reinterpret_cast<double2*>(R), chi_grad);
+    batch_gradient_kernel<128><<<h.grid_grad, 128, gsm, st>>>(
+        pl, w, reinterpret_cast<const double2*>(R_obs), reinterpret_cast<double2*>(R), chi_grad,
+        stage);
   }
   return check_launch("kr_batch_launch: gradient");
 }

@@ -15,6 +15,8 @@
 // Replaces the torch autograd graph of kennett_reflectivity_torch (kennett_torch.py:312-480),
 // jacobian (:611-641) and the per-slowness gradient of taup_misfit_grad_hessian
 // (taup_inversion.py:112-187).
+#include <stdlib.h>
+
 #include "kr_adjoint.cuh"
 #include "kr_internal.cuh"
 
@@ -78,7 +80,7 @@ __global__ void deriv_iface_kernel(const double* __restrict__ p, int n_p, int L,
 template <bool GRAD>
 __device__ __forceinline__ void finalize_layer(int l, int L, const Acc& acc, bool valid, cd res,
                                                int ip, int iw, int n_w, double2* __restrict__ J,
-                                               double* s_grad, double* s_warp) {
+                                               double* s_wacc) {
   if (!GRAD) {
     if (valid) {
       const size_t base = ((size_t)ip * 4 * L) * n_w + iw;
@@ -88,7 +90,8 @@ __device__ __forceinline__ void finalize_layer(int l, int L, const Acc& acc, boo
       J[base + (size_t)(3 * L + l) * n_w] = make_double2(acc.h.x, acc.h.y);
     }
   } else {
-    // d chi / d theta = 2 Re(conj(res) dR/dtheta) = 2 (res.x dR.x + res.y dR.y)
+    // d chi / d theta = 2 Re(conj(res) dR/dtheta) = 2 (res.x dR.x + res.y dR.y), reduced over
+    // the warp by shuffles and added to this warp's own accumulator row (no block barrier).
     double v[4] = {0.0, 0.0, 0.0, 0.0};
     if (valid) {
       v[0] = 2.0 * (res.x * acc.a.x + res.y * acc.a.y);
@@ -99,16 +102,10 @@ __device__ __forceinline__ void finalize_layer(int l, int L, const Acc& acc, boo
 #pragma unroll
     for (int k = 0; k < 4; ++k)
       for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0)
-      for (int k = 0; k < 4; ++k) s_warp[warp * 4 + k] = v[k];
-    __syncthreads();
-    if (threadIdx.x < 4) {
-      double t = 0.0;
-      for (int w = 0; w < kDerThreads / 32; ++w) t += s_warp[w * 4 + threadIdx.x];
-      s_grad[threadIdx.x * L + l] += t;
+    if ((threadIdx.x & 31) == 0) {
+      double* row = s_wacc + (threadIdx.x >> 5) * (4 * L + 1);
+      for (int k = 0; k < 4; ++k) row[k * L + l] += v[k];
     }
-    __syncthreads();
   }
 }
 
@@ -120,8 +117,7 @@ struct PairSink {
   const double2* R_obs;
   double2* R_out;
   double2* J;
-  double* s_grad;
-  double* s_warp;
+  double* s_wacc;
   cd res;
   __device__ void reflectivity(cd R) {
     res = mk(0.0, 0.0);
@@ -133,33 +129,57 @@ struct PairSink {
     }
   }
   __device__ void layer(int l, const Acc& acc) {
-    finalize_layer<GRAD>(l, L, acc, valid, res, ip, iw, n_w, J, s_grad, s_warp);
+    finalize_layer<GRAD>(l, L, acc, valid, res, ip, iw, n_w, J, s_wacc);
   }
 };
 
-template <bool GRAD>
-__global__ void __launch_bounds__(kDerThreads)
+template <bool GRAD, int MINB>
+__global__ void __launch_bounds__(kDerThreads, MINB)
 deriv_sweep_kernel(int L, const double* __restrict__ p, int n_p,
                    const double2* __restrict__ omega, int n_w, int n_wtiles, int free_surface,
-                   int seg, const LayerP* __restrict__ lay_all, const LayerD* __restrict__ dlay_all,
-                   const Iface* __restrict__ coef_all, const ScatTan* __restrict__ tan_all,
-                   const double2* __restrict__ R_obs, double2* __restrict__ R_out,
-                   double2* __restrict__ J, double* __restrict__ partial) {
-  extern __shared__ double s_dyn[];
-  double* s_grad = s_dyn;                 // [4L + 1]
-  double* s_warp = s_dyn + 4 * L + 1;     // [warps * 4]
+                   int seg, int stage, const LayerP* __restrict__ lay_all,
+                   const LayerD* __restrict__ dlay_all, const Iface* __restrict__ coef_all,
+                   const ScatTan* __restrict__ tan_all, const double2* __restrict__ R_obs,
+                   double2* __restrict__ R_out, double2* __restrict__ J,
+                   double* __restrict__ partial) {
+  // dynamic smem: [warps][4L + 1] per-warp accumulators (GRAD), then, if `stage`, this
+  // block's slowness data (tangents, coefficients, layer terms, layer derivatives)
+  extern __shared__ __align__(16) double s_wacc[];
   const int ip = blockIdx.x / n_wtiles;
   const int iw = (blockIdx.x % n_wtiles) * kDerThreads + threadIdx.x;
   const bool valid = iw < n_w;
   const int I = L - 1;
+  const int nv = 4 * L + 1;
   if (GRAD) {
-    for (int k = threadIdx.x; k < 4 * L + 1; k += blockDim.x) s_grad[k] = 0.0;
+    for (int k = threadIdx.x; k < (kDerThreads / 32) * nv; k += blockDim.x) s_wacc[k] = 0.0;
     __syncthreads();
   }
   cd w = mk(0.0, 0.0);
   if (valid) {
     const double2 wv = omega[iw];
     w = mk(wv.x, wv.y);
+  }
+  const ScatTan* tan = tan_all + (size_t)ip * I;
+  const Iface* coef = coef_all + (size_t)ip * I;
+  const LayerP* lay = lay_all + (size_t)ip * L;
+  const LayerD* dlay = dlay_all + (size_t)ip * L;
+  if (stage) {
+    unsigned char* b = reinterpret_cast<unsigned char*>(s_wacc) +
+                       (GRAD ? sizeof(double) * (((kDerThreads / 32) * nv + 1) / 2 * 2) : 0);
+    ScatTan* st = reinterpret_cast<ScatTan*>(b);
+    Iface* sc = reinterpret_cast<Iface*>(b + sizeof(ScatTan) * I);
+    LayerP* sl = reinterpret_cast<LayerP*>(b + (sizeof(ScatTan) + sizeof(Iface)) * I);
+    LayerD* sd = reinterpret_cast<LayerD*>(b + (sizeof(ScatTan) + sizeof(Iface)) * I +
+                                           sizeof(LayerP) * L);
+    copy16(st, tan, sizeof(ScatTan) * I);
+    copy16(sc, coef, sizeof(Iface) * I);
+    copy16(sl, lay, sizeof(LayerP) * L);
+    copy16(sd, dlay, sizeof(LayerD) * L);
+    __syncthreads();
+    tan = st;
+    coef = sc;
+    lay = sl;
+    dlay = sd;
   }
   PairSink<GRAD> sink;
   sink.L = L;
@@ -170,35 +190,85 @@ deriv_sweep_kernel(int L, const double* __restrict__ p, int n_p,
   sink.R_obs = R_obs;
   sink.R_out = R_out;
   sink.J = J;
-  sink.s_grad = s_grad;
-  sink.s_warp = s_warp;
-  jacobian_pair(L, w, free_surface != 0, seg, lay_all + (size_t)ip * L,
-                dlay_all + (size_t)ip * L, coef_all + (size_t)ip * I, tan_all + (size_t)ip * I,
-                sink);
+  sink.s_wacc = s_wacc;
+  jacobian_pair(L, w, free_surface != 0, seg, lay, dlay, coef, tan, sink);
   if (GRAD) {
     const cd res = sink.res;
     double c2 = valid ? (res.x * res.x + res.y * res.y) : 0.0;
     for (int o = 16; o > 0; o >>= 1) c2 += __shfl_down_sync(0xffffffffu, c2, o);
-    if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = c2;
+    if ((threadIdx.x & 31) == 0) s_wacc[(threadIdx.x >> 5) * nv + 4 * L] += c2;
     __syncthreads();
-    if (threadIdx.x == 0) {
+    double* dst = partial + (size_t)blockIdx.x * nv;
+    for (int k = threadIdx.x; k < nv; k += blockDim.x) {
       double t = 0.0;
-      for (int wi = 0; wi < kDerThreads / 32; ++wi) t += s_warp[wi];
-      s_grad[4 * L] = t;
+      for (int wi = 0; wi < kDerThreads / 32; ++wi) t += s_wacc[wi * nv + k];
+      dst[k] = t;
     }
-    __syncthreads();
-    double* dst = partial + (size_t)blockIdx.x * (4 * L + 1);
-    for (int k = threadIdx.x; k < 4 * L + 1; k += blockDim.x) dst[k] = s_grad[k];
   }
 }
 
-__global__ void reduce_partials_kernel(const double* __restrict__ partial, int n_blocks, int n,
-                                       double* __restrict__ out) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
+// out[k] = sum_b partial[b][k]: one block per k, fixed-shape tree (deterministic).
+__global__ void __launch_bounds__(256)
+reduce_partials_kernel(const double* __restrict__ partial, int n_blocks, int n,
+                       double* __restrict__ out) {
+  __shared__ double s[256];
+  const int k = blockIdx.x;
   double t = 0.0;
-  for (int b = 0; b < n_blocks; ++b) t += partial[(size_t)b * n + k];
-  out[k] = t;
+  for (int b = threadIdx.x; b < n_blocks; b += 256) t += partial[(size_t)b * n + k];
+  s[threadIdx.x] = t;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) s[threadIdx.x] += s[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[k] = s[0];
+}
+
+// Shared memory the sweep may use for staging one slowness's data (per block).
+constexpr size_t kStageSmemMax = 160 * 1024;
+
+// Register budget of the sweep kernel: blocks of 128 threads per SM (2 -> up to 255
+// registers, 3 -> 168).  KR_DERIV_MINB or kr_set_deriv_variant; default 2.
+static int g_deriv_minb = 0;
+
+static int deriv_minb() {
+  if (g_deriv_minb == 0) {
+    const char* e = getenv("KR_DERIV_MINB");
+    g_deriv_minb = (e && atoi(e) == 3) ? 3 : 2;
+  }
+  return g_deriv_minb;
+}
+
+template <bool GRAD, int MINB>
+static kr_status launch_sweep_v(unsigned blocks, size_t smem, cudaStream_t st, int L,
+                                const double* p, int n_p, const double2* omega, int n_w,
+                                int n_wtiles, int fs, int seg, int stage, const LayerP* lay,
+                                const LayerD* dlay, const Iface* coef, const ScatTan* tan,
+                                const double2* R_obs, double2* R, double2* J, double* partial) {
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(deriv_sweep_kernel<GRAD, MINB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) {
+      set_last_error("kr_deriv: smem attribute", e);
+      return KR_ERR_CUDA;
+    }
+  }
+  deriv_sweep_kernel<GRAD, MINB><<<blocks, kDerThreads, smem, st>>>(
+      L, p, n_p, omega, n_w, n_wtiles, fs, seg, stage, lay, dlay, coef, tan, R_obs, R, J, partial);
+  return KR_OK;
+}
+
+template <bool GRAD>
+static kr_status launch_sweep(int minb, unsigned blocks, size_t smem, cudaStream_t st, int L,
+                              const double* p, int n_p, const double2* omega, int n_w,
+                              int n_wtiles, int fs, int seg, int stage, const LayerP* lay,
+                              const LayerD* dlay, const Iface* coef, const ScatTan* tan,
+                              const double2* R_obs, double2* R, double2* J, double* partial) {
+  if (minb == 3)
+    return launch_sweep_v<GRAD, 3>(blocks, smem, st, L, p, n_p, omega, n_w, n_wtiles, fs, seg,
+                                   stage, lay, dlay, coef, tan, R_obs, R, J, partial);
+  return launch_sweep_v<GRAD, 2>(blocks, smem, st, L, p, n_p, omega, n_w, n_wtiles, fs, seg,
+                                 stage, lay, dlay, coef, tan, R_obs, R, J, partial);
 }
 
 template <bool GRAD>
@@ -221,16 +291,21 @@ static kr_status launch_deriv(const double* layers, int L, const double* p, int 
   s = check_launch("kr_deriv: interfaces");
   if (s != KR_OK) return s;
   const int seg = checkpoint_spacing(I - 1 > 0 ? I - 1 : 1);
-  const size_t smem = sizeof(double) * ((size_t)4 * L + 1 + (kDerThreads / 32) * 4);
-  deriv_sweep_kernel<GRAD><<<(unsigned)n_blocks, kDerThreads, smem, st>>>(
-      L, p, n_p, reinterpret_cast<const double2*>(omega), n_w, n_wtiles,
-      (flags & KR_FREE_SURFACE) ? 1 : 0, seg, w.lay, w.dlay, w.coef, w.tan,
-      reinterpret_cast<const double2*>(R_obs), reinterpret_cast<double2*>(R),
-      reinterpret_cast<double2*>(J), w.partial);
+  // accumulators: [warps][4L + 1] doubles, padded to 16 bytes
+  const size_t acc = GRAD ? sizeof(double) * (((size_t)(kDerThreads / 32) * (4 * L + 1) + 1) / 2 * 2) : 0;
+  const size_t pair = pair_smem_bytes(L);
+  const int stage = (acc + pair <= kStageSmemMax) ? 1 : 0;
+  const size_t smem = acc + (stage ? pair : 0);
+  s = launch_sweep<GRAD>(deriv_minb(), (unsigned)n_blocks, smem, st, L, p, n_p,
+                         reinterpret_cast<const double2*>(omega), n_w, n_wtiles,
+                         (flags & KR_FREE_SURFACE) ? 1 : 0, seg, stage, w.lay, w.dlay, w.coef,
+                         w.tan, reinterpret_cast<const double2*>(R_obs),
+                         reinterpret_cast<double2*>(R), reinterpret_cast<double2*>(J), w.partial);
+  if (s != KR_OK) return s;
   s = check_launch("kr_deriv: sweep");
   if (s != KR_OK || !GRAD) return s;
   const int n = 4 * L + 1;
-  reduce_partials_kernel<<<(n + 127) / 128, 128, 0, st>>>(w.partial, (int)n_blocks, n, chi_grad);
+  reduce_partials_kernel<<<n, 256, 0, st>>>(w.partial, (int)n_blocks, n, chi_grad);
   return check_launch("kr_deriv: reduce");
 }
 
@@ -246,6 +321,10 @@ static kr_status deriv_args(const double* layers, int L, const double* p, int n_
 }  // namespace kr
 
 using namespace kr;
+
+extern "C" void kr_set_deriv_variant(int32_t min_blocks_per_sm) {
+  g_deriv_minb = (min_blocks_per_sm == 3) ? 3 : 2;
+}
 
 extern "C" size_t kr_jacobian_workspace_bytes(int32_t n_layers, int32_t n_p, int32_t n_w) {
   if (n_layers < 2 || n_p <= 0 || n_w <= 0) return 0;

@@ -64,4 +64,11 @@ __device__ __forceinline__ cd sweep(cd w, int n_layers, const LayerP* s_layer,
   return r.a;
 }
 
+// Block-cooperative copy of n bytes (multiple of 16, 16-byte aligned) into shared memory.
+__device__ __forceinline__ void copy16(void* dst, const void* src, size_t n) {
+  double2* d = reinterpret_cast<double2*>(dst);
+  const double2* s = reinterpret_cast<const double2*>(src);
+  for (size_t k = threadIdx.x; k < n / 16; k += blockDim.x) d[k] = s[k];
+}
+
 }  // namespace kr

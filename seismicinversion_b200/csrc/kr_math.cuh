@@ -106,6 +106,7 @@ struct LayerP {
   cd ca;     // i * eta * h   (0 for the half-space: phase factor exactly 1)
   cd cb;     // i * neta * h
   double rho;
+  double pad;  // 96 bytes: arrays of LayerP are whole 16-byte units (vector copies)
 };
 
 // Layer table layout (device or host): 6 rows of n_layers doubles:
@@ -131,6 +132,7 @@ KR_HD LayerP layer_terms(const double* tab, int n_layers, int l, double p) {
     o.cb = mk(-o.neta.y * h, o.neta.x * h);
   }
   o.rho = rho;
+  o.pad = 0.0;
   return o;
 }
 

@@ -133,7 +133,10 @@ class KennettServer:
                  max_batch_requests: int = 256, max_inflight: int = 2,
                  max_pending: int = 1_000_000, poll_interval: float = 50e-6,
                  min_batch_wait: float = 0.0):
-        self.executor = executor if executor is not None else GpuBatchExecutor()
+        # one more stream than batches in flight: the stream a new batch is built on has
+        # always finished its previous batch, so host-side uploads never wait on the GPU
+        self.executor = (executor if executor is not None
+                         else GpuBatchExecutor(n_streams=int(max_inflight) + 1))
         self.budget = int(hbm_budget_bytes)
         self.max_batch = int(max_batch_requests)
         self.max_inflight = int(max_inflight)
@@ -156,14 +159,16 @@ class KennettServer:
     # -- client side ---------------------------------------------------------------------
     def submit(self, model: LayerModel, p, omega, gradient: bool = False, R_obs=None,
                free_surface: bool = False) -> Request:
-        p = np.ascontiguousarray(np.atleast_1d(p), dtype=np.float64)
-        omega = np.ascontiguousarray(np.atleast_1d(omega), dtype=np.complex128)
+        if not hasattr(p, "is_cuda"):
+            p = np.ascontiguousarray(np.atleast_1d(p), dtype=np.float64)
+        if not hasattr(omega, "is_cuda"):
+            omega = np.ascontiguousarray(np.atleast_1d(omega), dtype=np.complex128)
         req = Request(model, p, omega, gradient, R_obs, free_surface)
         req.t_submit = time.perf_counter()
         try:
             pack_layers(model)
             if gradient:
-                if R_obs is None or np.shape(R_obs) != (len(p), len(omega)):
+                if R_obs is None or tuple(R_obs.shape) != (len(p), len(omega)):
                     raise ValueError("gradient request needs R_obs of shape (n_p, n_omega)")
             if len(p) == 0 or len(omega) == 0:
                 raise ValueError("empty slowness or frequency grid")
