@@ -338,6 +338,110 @@ def bench_serving(torch, dev, rates=(100, 1000, 3000, 10000, 20000), duration=1.
     return out
 
 
+def run_sharded(args, rank, world, local):
+    """N > 1: one gather, slowness sum sharded over the ranks, NCCL all-reduce of U per step
+    (strong scaling: total work fixed).  Timed per step with CUDA events, max over ranks."""
+    import torch
+    import torch.distributed as dist
+
+    from seismicinversion_b200 import device as D
+    from seismicinversion_b200.earth_models import damped_gather_grid, random_layered_model
+    from seismicinversion_b200.sharded import DeviceGatherBackend, gather_sharded, shard_range
+    from seismicinversion_b200.source import ricker_10hz
+
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                            device_id=torch.device("cuda", local))
+    dev = D.require_cuda(torch.device("cuda", local))
+    W = WORKLOAD
+    model = random_layered_model(W["n_sub"], seed=W["seed"])
+    T, nw, npp, pmax = W["T"], W["nw"], W["n_p"], W["p_max"]
+    offsets = np.arange(1, W["n_offsets"] + 1) * W["dr"]
+    om, omd, p, dp, taper, gamma = damped_gather_grid(T, nw, npp, pmax)
+    S = ricker_10hz(om, nw * (2 * np.pi / T))
+    decay = np.exp(-gamma * np.arange(2 * nw) * (T / (2 * nw)))
+    j0, j1 = shard_range(npp, rank, world)
+    tab = D.layer_table(model, dev)
+    p_t = torch.as_tensor(p[j0:j1], device=dev)
+    pw_t = torch.as_tensor((taper * p)[j0:j1], device=dev)
+    w_t = torch.as_tensor(omd, device=dev)
+    wr_t = torch.as_tensor(om, device=dev)
+    off_t = torch.as_tensor(offsets, device=dev)
+    S_t, dec_t = torch.as_tensor(S, device=dev), torch.as_tensor(decay, device=dev)
+    R = torch.empty((j1 - j0, nw - 1), dtype=torch.complex128, device=dev)
+    U = torch.empty((len(offsets), nw - 1), dtype=torch.complex128, device=dev)
+    G = torch.empty((len(offsets), 2 * nw), dtype=torch.float64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    st = torch.cuda.current_stream(dev)
+
+    def step(ev):
+        ev[0].record(st)
+        D.reflectivity(tab, p_t, w_t, True, out=R)
+        D.bessel_sum(R, p_t, pw_t, dp, wr_t, off_t, out=U)
+        dist.all_reduce(torch.view_as_real(U), op=dist.ReduceOp.SUM)
+        D.traces(U, nw, S=S_t, decay=dec_t, out=G)
+        ev[1].record(st)
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        step([torch.cuda.Event(enable_timing=True) for _ in range(2)])
+    torch.cuda.synchronize()
+    dist.barrier()
+    torch.cuda.synchronize()
+    clk = Clocks(local)
+    clk.start()
+    evs = []
+    for _ in range(args.steps):
+        flush.zero_()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        step(ev)
+        evs.append(ev)
+    torch.cuda.synchronize()
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = float(np.mean([e[0].elapsed_time(e[1]) for e in evs]))
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t[0])
+    # end to end: host model in, the rank's R rows and the traces back to pinned host memory
+    backend = DeviceGatherBackend(dev)
+    Rh = torch.empty((j1 - j0, nw - 1), dtype=torch.complex128, pin_memory=True)
+    Gh = torch.empty((len(offsets), 2 * nw), dtype=torch.float64, pin_memory=True)
+    e2e = []
+    for k in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        dist.barrier()
+        t0 = time.perf_counter()
+        _, g, Rs, _ = gather_sharded(model, offsets, T=T, nw=nw, np_slow=npp, p_max=pmax,
+                                     source_func=ricker_10hz, free_surface=True, backend=backend)
+        Rh.copy_(Rs, non_blocking=True)
+        Gh.copy_(g, non_blocking=True)
+        torch.cuda.synchronize()
+        if k >= args.warmup:
+            e2e.append(time.perf_counter() - t0)
+    t = torch.tensor([statistics.mean(e2e)], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_s = float(t[0])
+    upd = (nw - 1) * npp * (W["layers"] - 1)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "(omega,p,interface) reflectivity updates/s, 21-layer gather workload (R grid + J0 gather + traces)",
+            "value": upd / (ms * 1e-3), "unit": "updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64 (complex128)",
+            "data": "synthetic (seeded random 21-layer model; no dataset exists)",
+            "config": {**W, "parallelism": f"slowness-sharded x{world} + NCCL all-reduce of U",
+                       "l2": "flushed between steps (256 MB write) and R grid > L2"},
+            "e2e": {"value": upd / e2e_s, "unit": "updates/s", "seconds_per_step": e2e_s,
+                    "h2d_bytes_per_step": int(tab.numel() * 8 + offsets.nbytes),
+                    "d2h_bytes_per_step": int(Rh.numel() * 16 + Gh.numel() * 8)},
+            "gpu_launches": 5 * args.steps, "clocks": clocks,
+        }))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
 def run_ours(args, rank, world, local):
     import torch
 
@@ -346,13 +450,7 @@ def run_ours(args, rank, world, local):
     from seismicinversion_b200.kennett_gather_gpu import compute_gather_gpu
     from seismicinversion_b200.source import ricker_10hz
 
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+    dist = None  # single GPU (N > 1 runs run_sharded)
     dev = D.require_cuda(torch.device("cuda", local))
     torch.cuda.set_device(dev)
     W = WORKLOAD
@@ -614,6 +712,8 @@ def main():
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif world > 1:
+        run_sharded(args, rank, world, local)
     else:
         run_ours(args, rank, world, local)
 
