@@ -129,6 +129,42 @@ class ModelBatch:
         self.plan = None
         self.set_schedule(schedule or (128, 256))
 
+    @classmethod
+    def from_tables(cls, tables: np.ndarray, p, omega, free_surface: bool = False,
+                    schedule: tuple[int, int] | None = None, device=None) -> "ModelBatch":
+        """Forward batch of same-shape models from layer tables [n, 6, L] on one shared
+        slowness / frequency grid (vectorised packing; R of model b is
+        ``R[b*n_p*n_w:(b+1)*n_p*n_w]``)."""
+        tables = np.ascontiguousarray(tables, dtype=np.float64)
+        n, six, L = tables.shape
+        if six != 6:
+            raise ValueError("tables must have shape [n, 6, n_layers]")
+        for b in range(n):
+            D.validate_table(tables[b])
+        p = np.ascontiguousarray(p, dtype=np.float64).reshape(-1)
+        w = np.ascontiguousarray(omega, dtype=np.complex128).reshape(-1)
+        self = cls.__new__(cls)
+        self.dev = D.require_cuda(device)
+        self.items = None
+        desc = np.zeros(n, dtype=_lib.MODEL_DESC_FIELDS)
+        desc["n_layers"], desc["n_p"], desc["n_w"] = L, len(p), len(w)
+        desc["flags"] = _lib.KR_FREE_SURFACE if free_surface else 0
+        desc["layers_off"] = np.arange(n) * 6 * L
+        desc["R_off"] = np.arange(n) * len(p) * len(w)
+        self.desc = desc
+        self.max_layers = L
+        self.layers = torch.as_tensor(tables.reshape(-1), device=self.dev)
+        self.p = torch.as_tensor(p, device=self.dev)
+        self.omega = torch.as_tensor(w, device=self.dev)
+        self.R_obs = None
+        self.R = torch.empty(max(n * len(p) * len(w), 1), dtype=torch.complex128, device=self.dev)
+        self.chi_grad = torch.zeros(1, dtype=torch.float64, device=self.dev)
+        self.graph = None
+        self.schedule = None
+        self.plan = None
+        self.set_schedule(schedule or (128, 128))
+        return self
+
     # -- planning ------------------------------------------------------------------------
     def _cfg(self, schedule):
         return _lib.BatchConfig(int(schedule[0]), int(schedule[1]), 0, 0)

@@ -29,6 +29,27 @@ def _model_arrays(m):
                 Q_alpha=m.Q_alpha, Q_beta=m.Q_beta)
 
 
+def training_data_golden(ref_root: str) -> None:
+    """Reference NeuralInversion.generate_training_data on a small config (GMM forward)."""
+    import tempfile
+
+    import torch
+
+    sys.path.insert(0, ref_root)
+    from NeuralInversion.inference_config import DataGenConfig
+    from NeuralInversion.inference_data import generate_training_data
+
+    cfg = DataGenConfig(n_train=12, n_val=4, n_test=4, nfreq=32, seed=42)
+    with tempfile.TemporaryDirectory() as d:
+        paths = generate_training_data(d, cfg)
+        out = {}
+        for split, path in paths.items():
+            data = torch.load(path, weights_only=True)
+            out[f"{split}_log_params"] = data["log_params"].numpy()
+            out[f"{split}_reflectivity"] = data["reflectivity"].numpy()
+    np.savez_compressed(HERE / "training_data_small.npz", **out)
+
+
 def main(ref_root: str) -> None:
     sys.path.insert(0, ref_root)
     os.environ.setdefault("TQDM_DISABLE", "1")
@@ -181,4 +202,9 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if "--training-data-only" in sys.argv:
+        training_data_golden(root)
+    else:
+        main(root)
+        training_data_golden(root)
