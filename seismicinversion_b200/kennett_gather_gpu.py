@@ -73,21 +73,63 @@ def _pinned(shape, dtype) -> torch.Tensor:
 def compute_gather_gpu(model: LayerModel, offsets, T: float = 64.0, nw: int = 2048,
                        np_slow: int = 4096, p_max: float = 1.2, gamma=None, source_func=None,
                        free_surface: bool = False, device=None,
-                       return_reflectivity: bool = False):
+                       return_reflectivity: bool = False, copy_chunks: int = 4):
     """``(time, offsets, gather)`` exactly as ``compute_gather_gpu`` (``kennett_gather_gpu.py:169-284``).
 
     With ``return_reflectivity=True`` the full R(p, omega + i gamma) grid is returned as a
-    fourth element (copied once through a pinned host buffer).  Returned arrays may share
-    that pinned buffer with the next call; copy them to keep them.
+    fourth element.  The grid is computed in ``copy_chunks`` slowness blocks and each block is
+    copied to a pinned host buffer on a second stream while the later blocks and the Bessel
+    sum run, so the host copy overlaps the compute.  Returned arrays may share that pinned
+    buffer with the next call; copy them to keep them.
     """
-    time, R, _, g = gather_device(model, offsets, T, nw, np_slow, p_max, gamma, source_func,
-                                  free_surface, device)
+    dev = _dev.require_cuda(device)
+    if gamma is None:
+        gamma = np.pi / T
+    dw = 2.0 * np.pi / T
+    omega = np.arange(1, nw, dtype=np.float64) * dw
+    wmax = nw * dw
+    S = ricker_spectrum(omega, wmax) if source_func is None else source_func(omega, wmax)
+    nt = 2 * nw
+    time = np.arange(nt, dtype=np.float64) * (T / float(nt))
+    dp = p_max / np_slow
+    p = np.arange(1, np_slow + 1, dtype=np.float64) * dp
+    taper = 0.5 * (1.0 + np.cos(np.pi * p / p_max))
+    main = torch.cuda.current_stream(dev)
+    tab = _dev.layer_table(model, dev)
+    p_t = torch.as_tensor(p, device=dev)
+    w_t = torch.as_tensor(omega + 1j * gamma, device=dev)
+    R = torch.empty((np_slow, nw - 1), dtype=torch.complex128, device=dev)
+    Rh = _pinned((np_slow, nw - 1), torch.complex128) if return_reflectivity else None
+    copy = _copy_stream(dev) if return_reflectivity else None
+    n_chunks = max(1, min(copy_chunks, np_slow)) if return_reflectivity else 1
+    bounds = np.linspace(0, np_slow, n_chunks + 1).astype(int)
+    for a, b in zip(bounds[:-1], bounds[1:]):
+        _dev.reflectivity(tab, p_t[a:b], w_t, free_surface, out=R[a:b])
+        if return_reflectivity:
+            ev = torch.cuda.Event()
+            ev.record(main)
+            copy.wait_event(ev)
+            with torch.cuda.stream(copy):
+                Rh[a:b].copy_(R[a:b], non_blocking=True)
+    U = _dev.bessel_sum(R, p_t, taper * p, dp, omega, offsets)
+    g = _dev.traces(U, nw, S=np.asarray(S, dtype=np.complex128), decay=np.exp(-gamma * time))
     gh = _pinned(tuple(g.shape), g.dtype)
     gh.copy_(g, non_blocking=True)
     if return_reflectivity:
-        Rh = _pinned(tuple(R.shape), R.dtype)
-        Rh.copy_(R, non_blocking=True)
-    torch.cuda.current_stream(g.device).synchronize()
+        R.record_stream(copy)
+        copy.synchronize()
+    main.synchronize()
     if return_reflectivity:
         return time, np.asarray(offsets), gh.numpy(), Rh.numpy()
     return time, np.asarray(offsets), gh.numpy().copy()
+
+
+_COPY_STREAMS: dict = {}
+
+
+def _copy_stream(dev) -> torch.cuda.Stream:
+    s = _COPY_STREAMS.get(dev)
+    if s is None:
+        s = torch.cuda.Stream(dev)
+        _COPY_STREAMS[dev] = s
+    return s

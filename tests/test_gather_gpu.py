@@ -119,3 +119,21 @@ def test_full_size_gather_stagewise():
     gamma = np.pi / T
     S = ricker_10hz(om, nw * dw)
     assert rel_err(gh, O.hermitian_traces(Uh * S, nw, np.exp(-gamma * time))) < 1e-12
+
+
+def test_gather_returning_reflectivity_overlapped_copy():
+    """The chunked, copy-overlapped path returns the same R grid as the batch call and the
+    same traces as the plain call."""
+    from seismicinversion_b200 import compute_gather_gpu, kennett_reflectivity_batch
+    from seismicinversion_b200.earth_models import damped_gather_grid, random_layered_model
+
+    m = random_layered_model(7, seed=12)
+    offs = np.array([0.5, 3.0, 12.0, 30.0])
+    t, _, g, R = compute_gather_gpu(m, offs, T=32.0, nw=512, np_slow=1031, p_max=1.1,
+                                    free_surface=True, return_reflectivity=True, copy_chunks=5)
+    t2, _, g2 = compute_gather_gpu(m, offs, T=32.0, nw=512, np_slow=1031, p_max=1.1,
+                                   free_surface=True)
+    _, omd, p, _, _, _ = damped_gather_grid(32.0, 512, 1031, 1.1)
+    Rb = kennett_reflectivity_batch(m, p, omd, free_surface=True)
+    assert np.array_equal(R, Rb)
+    assert np.array_equal(g, g2) and np.array_equal(t, t2)
