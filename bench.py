@@ -285,16 +285,20 @@ def bench_serving(torch, dev, rates=(100, 1000, 3000, 10000, 20000), duration=1.
     torch.cuda.synchronize()
     rng = np.random.default_rng(7)
     out = {"workload": "Poisson stream, uneven models as the batching workload, 50/50 fwd/grad"}
-    # warm-up: streams, kernel modules and pinned staging buffers of the server path
-    with KennettServer(hbm_budget_bytes=120 * 10**9, max_batch_requests=64, max_inflight=2) as srv:
-        for k in range(8):
+    # warm-up: kernel modules, streams, allocator segments, pinned staging buffers
+    with KennettServer(hbm_budget_bytes=120 * 10**9, max_batch_requests=64, max_inflight=2,
+                       prewarm_bytes=4 << 30) as srv:
+        for k in range(len(pool)):
             m, p_t, w_t, g, obs = pool[k]
-            srv.submit(m, p_t, w_t, gradient=g, R_obs=obs).wait(60)
+            srv.submit(m, p_t, w_t, gradient=g, R_obs=obs)
+        for r in list(srv.completed):
+            pass
+    torch.cuda.synchronize()
     for lam in rates:
         n = int(min(max_requests, lam * duration))
         gaps = rng.exponential(1.0 / lam, n)
         with KennettServer(hbm_budget_bytes=120 * 10**9, max_batch_requests=64,
-                           max_inflight=2) as srv:
+                           max_inflight=2, prewarm_bytes=4 << 30) as srv:
             t_start = time.perf_counter()
             t_next = t_start
             reqs = []
@@ -309,7 +313,8 @@ def bench_serving(torch, dev, rates=(100, 1000, 3000, 10000, 20000), duration=1.
                 r.wait(120)
             stats = srv.stats(since=t_start)
         out[f"rate_{lam}"] = {k: stats[k] for k in ("completed", "throughput_rps", "p50_ms",
-                                                     "p99_ms", "batches")}
+                                                     "p99_ms", "batches", "mean_queue_ms",
+                                                     "mean_build_launch_ms", "mean_device_ms")}
     # plain per-request path (one launch + sync per request, FIFO) at a moderate rate
     lam = 300
     n = int(lam * duration)

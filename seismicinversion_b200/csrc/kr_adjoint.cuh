@@ -186,18 +186,22 @@ KR_HD void contract(const ScatTan& t, const cd cbar[10], Acc& up, Acc& lo) {
   lo.r = lo.r + s[5];
 }
 
-constexpr int kSegMax = 16;  // checkpoint spacing cap: (I - 1) <= 16 * 16 covers 256 layers
-constexpr int kCpMax = 16;
+constexpr int kSegMax = 24;  // steps kept per segment (inputs + phase factors)
+constexpr int kCpMax = 16;   // checkpoints: (I - 1) <= 16 * 16 covers 256 layers
 
+// Steps per segment: one segment (a full tape, no recomputation) when the pair's steps fit
+// the segment buffer, else ~sqrt(steps) (checkpoints every `seg` steps).
 KR_HD int checkpoint_spacing(int nsteps) {
+  if (nsteps <= kSegMax) return nsteps > 0 ? nsteps : 1;
   int s = 1;
   while (s * s < nsteps) ++s;
   return s;
 }
 
 // R and dR/dtheta for one (omega, p) pair.  Forward sweep storing the state every `seg`
-// steps, then the reverse sweep top-down, each segment recomputed from its checkpoint
-// (memory O(sqrt(I)) states instead of I).  sink.reflectivity(R) is called once before
+// steps (and recording the top segment's step inputs and phases outright), then the reverse
+// sweep top-down, every other segment recomputed from its checkpoint (memory
+// O(sqrt(I)) states instead of I; no recomputation at all when the steps fit one segment).  sink.reflectivity(R) is called once before
 // the reverse pass, sink.layer(l, acc) once per layer l (in order 0, 1, ..., L-1) with
 // the finished dR/d(alpha_l, beta_l, rho_l, h_l).
 #ifdef __CUDACC__
@@ -208,12 +212,22 @@ KR_HD void jacobian_pair(int L, cd w, bool free_surface, int seg, const LayerP* 
                          const LayerD* dlay, const Iface* coef, const ScatTan* tan, Sink& sink) {
   const int I = L - 1;
   const int nsteps = I - 1;  // step s applies interface i = I - 2 - s
+  const int ncp = nsteps > 0 ? (nsteps + seg - 1) / seg : 0;
+  const int top0 = (ncp - 1) * seg;  // first step of the top segment (reversed first)
   M2 cp[kCpMax];
+  M2 sg[kSegMax];
+  cd sea[kSegMax], seb[kSegMax];
   M2 r = m2(coef[I - 1].rd11, coef[I - 1].rd12, coef[I - 1].rd12, coef[I - 1].rd22);
   for (int s = 0; s < nsteps; ++s) {
     if (s % seg == 0) cp[s / seg] = r;
     const int i = I - 2 - s;
-    r = kennett_step(r, cexp_(w * lay[i + 1].ca), cexp_(w * lay[i + 1].cb), coef[i]);
+    const cd ea = cexp_(w * lay[i + 1].ca), eb = cexp_(w * lay[i + 1].cb);
+    if (s >= top0) {  // the top segment is recorded now and never recomputed
+      sg[s - top0] = r;
+      sea[s - top0] = ea;
+      seb[s - top0] = eb;
+    }
+    r = kennett_step(r, ea, eb, coef[i]);
   }
   const cd e0 = cexp_(w * lay[0].ca);
   sink.reflectivity(pp_surface(r.a, e0, free_surface));
@@ -228,21 +242,20 @@ KR_HD void jacobian_pair(int L, cd w, bool free_surface, int seg, const LayerP* 
   Acc cur = acc_zero(), nxt = acc_zero();
   cur.a = f0 * dlay[0].ca_alpha;
   cur.h = f0 * dlay[0].ca_h;
-  M2 sg[kSegMax];
-  cd sea[kSegMax], seb[kSegMax];
-  const int ncp = nsteps > 0 ? (nsteps + seg - 1) / seg : 0;
   for (int q = ncp - 1; q >= 0; --q) {
     const int s0 = q * seg;
     const int s1 = s0 + seg < nsteps ? s0 + seg : nsteps;
-    M2 x = cp[q];
-    // recompute the segment's step inputs and phase factors from its checkpoint
-    for (int s = s0; s < s1; ++s) {
-      const int i = I - 2 - s;
-      const cd ea = cexp_(w * lay[i + 1].ca), eb = cexp_(w * lay[i + 1].cb);
-      sg[s - s0] = x;
-      sea[s - s0] = ea;
-      seb[s - s0] = eb;
-      if (s + 1 < s1) x = kennett_step(x, ea, eb, coef[i]);
+    if (q != ncp - 1) {
+      // recompute this segment's step inputs and phase factors from its checkpoint
+      M2 x = cp[q];
+      for (int s = s0; s < s1; ++s) {
+        const int i = I - 2 - s;
+        const cd ea = cexp_(w * lay[i + 1].ca), eb = cexp_(w * lay[i + 1].cb);
+        sg[s - s0] = x;
+        sea[s - s0] = ea;
+        seb[s - s0] = eb;
+        if (s + 1 < s1) x = kennett_step(x, ea, eb, coef[i]);
+      }
     }
     for (int s = s1 - 1; s >= s0; --s) {
       const int i = I - 2 - s;  // interface i, lower layer i + 1

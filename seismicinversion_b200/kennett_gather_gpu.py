@@ -17,7 +17,7 @@ from .earth_models import default_ocean_crust_model
 from .layer_model import LayerModel
 from .source import ricker_spectrum
 
-__all__ = ["compute_gather_gpu", "default_ocean_crust_model", "gather_device"]
+__all__ = ["compute_gather_gpu", "default_ocean_crust_model", "gather_device", "save_gather_npz"]
 
 
 def _gpu_bessel_summation(R, p_samples, omega_real, offsets, dp, device=None):
@@ -133,3 +133,51 @@ def _copy_stream(dev) -> torch.cuda.Stream:
         s = torch.cuda.Stream(dev)
         _COPY_STREAMS[dev] = s
     return s
+
+
+def save_gather_npz(path, time, offsets, gather):
+    """Write a gather as ``.npz`` with keys ``time``, ``offsets``, ``gather`` -- the file the
+    reference CLI writes (``kennett_gather_gpu.py:429-436``).  Returns the path written."""
+    from pathlib import Path
+
+    out = Path(path).with_suffix(".npz")
+    np.savez(out, time=np.asarray(time), offsets=np.asarray(offsets), gather=np.asarray(gather))
+    return out
+
+
+def main(argv=None) -> None:
+    """Command line as ``python -m Kennett_Reflectivity.kennett_gather_gpu``
+    (``kennett_gather_gpu.py:287-436``): default 5-layer model, writes ``<output>.npz``.
+    Plotting is not provided (the reference skips it too when matplotlib is missing)."""
+    import argparse
+    import logging
+
+    ap = argparse.ArgumentParser(description="Seismogram gather via Kennett reflectivity (B200).")
+    ap.add_argument("--r-min", type=float, default=0.5)
+    ap.add_argument("--r-max", type=float, default=50.0)
+    ap.add_argument("--dr", type=float, default=0.5)
+    ap.add_argument("-T", "--duration", type=float, default=64.0)
+    ap.add_argument("-n", "--nw", type=int, default=2048)
+    ap.add_argument("--np", dest="np_slow", type=int, default=4096)
+    ap.add_argument("--p-max", type=float, default=1.2)
+    ap.add_argument("--gamma", type=float, default=None)
+    ap.add_argument("--t-max", type=float, default=30.0)
+    ap.add_argument("-o", "--output", default="gather_gpu.png")
+    ap.add_argument("--no-plot", action="store_true")
+    ap.add_argument("--free-surface", action="store_true")
+    ap.add_argument("--device", default=None)
+    args = ap.parse_args(argv)
+    offsets = np.arange(args.r_min, args.r_max + args.dr / 2, args.dr)
+    device = args.device if args.device not in (None, "mps", "cpu") else None
+    time, offs, gather = compute_gather_gpu(default_ocean_crust_model(), offsets, T=args.duration,
+                                            nw=args.nw, np_slow=args.np_slow, p_max=args.p_max,
+                                            gamma=args.gamma, free_surface=args.free_surface,
+                                            device=device)
+    if not args.no_plot:
+        logging.getLogger(__name__).warning("plotting is not provided; writing data only")
+    out = save_gather_npz(args.output, time, offs, gather)
+    logging.getLogger(__name__).info("Data saved to %s", out)
+
+
+if __name__ == "__main__":
+    main()

@@ -9,7 +9,7 @@ from .earth_models import default_ocean_crust_model
 from .layer_model import LayerModel
 from .source import ricker_spectrum
 
-__all__ = ["compute_seismogram", "default_ocean_crust_model"]
+__all__ = ["compute_seismogram", "default_ocean_crust_model", "save_seismogram_txt"]
 
 
 def compute_seismogram(model: LayerModel, p: float, T: float = 64.0, nw: int = 2048,
@@ -27,3 +27,32 @@ def compute_seismogram(model: LayerModel, p: float, T: float = 64.0, nw: int = 2
     decay = None if eps == 0.0 else np.exp(eps * time)
     tr = _dev.traces(R, nw, S=np.asarray(S, dtype=np.complex128), decay=decay)
     return time, tr[0].cpu().numpy()
+
+
+def save_seismogram_txt(path, time, seismogram) -> None:
+    """Two columns (time, amplitude) as ``%.8e`` text -- the file the reference CLI writes
+    (``kennett_seismogram.py:294-296``)."""
+    np.savetxt(path, np.column_stack([time, seismogram]), fmt="%.8e")
+
+
+def main(argv=None) -> None:
+    """Command line as ``python -m Kennett_Reflectivity.kennett_seismogram``
+    (``kennett_seismogram.py:153-296``): default 5-layer model, writes
+    ``seismogram_p<p>.txt``.  Plotting is not provided."""
+    import argparse
+
+    ap = argparse.ArgumentParser(description="Synthetic seismogram via Kennett reflectivity (B200).")
+    ap.add_argument("-p", "--slowness", type=float, default=0.2)
+    ap.add_argument("-T", "--duration", type=float, default=64.0)
+    ap.add_argument("-n", "--nw", type=int, default=2048)
+    ap.add_argument("-o", "--output", default="seismogram_verification.png")
+    ap.add_argument("--no-plot", action="store_true")
+    ap.add_argument("--free-surface", action="store_true")
+    args = ap.parse_args(argv)
+    time, seis = compute_seismogram(default_ocean_crust_model(), args.slowness, T=args.duration,
+                                    nw=args.nw, free_surface=args.free_surface)
+    save_seismogram_txt(f"seismogram_p{args.slowness:.4f}.txt", time, seis)
+
+
+if __name__ == "__main__":
+    main()

@@ -50,6 +50,7 @@ class Request:
     id: int = -1
     t_submit: float = 0.0
     t_admit: float = 0.0
+    t_launched: float = 0.0
     t_done: float = 0.0
     nbytes: int = 0
     done: threading.Event = field(default_factory=threading.Event)
@@ -96,6 +97,25 @@ class GpuBatchExecutor:
         self.schedule = schedule
         self._k = 0
 
+    def prewarm(self, device_bytes: int, host_bytes: int = 16 << 20) -> None:
+        """Reserve caching-allocator segments on every stream (and pinned host blocks) so
+        that steady-state batches reuse cached memory instead of calling cudaMalloc /
+        cudaHostAlloc, which are slow and (cudaMalloc) synchronise the device."""
+        torch = self.torch
+        for s in self.streams:
+            with torch.cuda.stream(s):
+                x = torch.empty(int(device_bytes), dtype=torch.uint8, device=self.dev)
+                del x
+        # one pinned block per power-of-two size class from 1 KB up (the host caching
+        # allocator serves plan images and staging copies from these)
+        sizes, b = [], 1024
+        while b <= int(host_bytes):
+            sizes.append(b)
+            b *= 2
+        blocks = [torch.empty(n, dtype=torch.uint8, pin_memory=True) for n in sizes for _ in range(4)]
+        del blocks
+        torch.cuda.synchronize(self.dev)
+
     def launch(self, reqs: list[Request]):
         from .batch import BatchItem, ModelBatch
 
@@ -132,11 +152,13 @@ class KennettServer:
     def __init__(self, executor=None, hbm_budget_bytes: int = 120 * 10**9,
                  max_batch_requests: int = 256, max_inflight: int = 2,
                  max_pending: int = 1_000_000, poll_interval: float = 50e-6,
-                 min_batch_wait: float = 0.0):
+                 min_batch_wait: float = 0.0, prewarm_bytes: int = 0):
         # one more stream than batches in flight: the stream a new batch is built on has
         # always finished its previous batch, so host-side uploads never wait on the GPU
         self.executor = (executor if executor is not None
                          else GpuBatchExecutor(n_streams=int(max_inflight) + 1))
+        if prewarm_bytes and hasattr(self.executor, "prewarm"):
+            self.executor.prewarm(min(int(prewarm_bytes), int(hbm_budget_bytes)))
         self.budget = int(hbm_budget_bytes)
         self.max_batch = int(max_batch_requests)
         self.max_inflight = int(max_inflight)
@@ -153,6 +175,11 @@ class KennettServer:
         self.completed: list[Request] = []
         self.batches_launched = 0
         self.peak_bytes = 0
+        # long-lived objects (models, pools, the caller's data) move to the permanent
+        # generation so periodic collections stay short while requests stream through
+        import gc
+
+        gc.freeze()
         self._thread = threading.Thread(target=self._loop, name="kennett-server", daemon=True)
         self._thread.start()
 
@@ -270,6 +297,9 @@ class KennettServer:
             if group:
                 try:
                     handle = self.executor.launch(group)
+                    t_l = time.perf_counter()
+                    for r in group:
+                        r.t_launched = t_l
                     self._inflight.append((handle, group))
                     self.batches_launched += 1
                 except BaseException as e:
@@ -291,6 +321,9 @@ class KennettServer:
             return {"completed": 0, "waiting": waiting}
         lat = np.array([r.latency for r in done])
         span = max(r.t_done for r in done) - min(r.t_submit for r in done)
+        wait = np.array([r.t_admit - r.t_submit for r in done])
+        build = np.array([r.t_launched - r.t_admit for r in done])
+        run = np.array([r.t_done - r.t_launched for r in done])
         return {
             "completed": len(done),
             "waiting": waiting,
@@ -300,4 +333,7 @@ class KennettServer:
             "mean_ms": float(lat.mean() * 1e3),
             "batches": self.batches_launched,
             "peak_admitted_bytes": self.peak_bytes,
+            "mean_queue_ms": float(wait.mean() * 1e3),
+            "mean_build_launch_ms": float(build.mean() * 1e3),
+            "mean_device_ms": float(run.mean() * 1e3),
         }

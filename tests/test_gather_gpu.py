@@ -137,3 +137,23 @@ def test_gather_returning_reflectivity_overlapped_copy():
     Rb = kennett_reflectivity_batch(m, p, omd, free_surface=True)
     assert np.array_equal(R, Rb)
     assert np.array_equal(g, g2) and np.array_equal(t, t2)
+
+
+def test_cli_output_files(tmp_path, monkeypatch):
+    """The command lines write the reference's file formats (.npz gather, two-column text)."""
+    from seismicinversion_b200 import compute_gather_gpu, compute_seismogram
+    from seismicinversion_b200.earth_models import default_ocean_crust_model
+    from seismicinversion_b200.kennett_gather_gpu import main as gather_main
+    from seismicinversion_b200.kennett_seismogram import main as seis_main
+
+    monkeypatch.chdir(tmp_path)
+    gather_main(["--r-min", "1", "--r-max", "3", "--dr", "1", "-n", "128", "--np", "64",
+                 "-T", "32", "-o", "g.png", "--no-plot", "--free-surface"])
+    z = np.load(tmp_path / "g.npz")
+    t, offs, g = compute_gather_gpu(default_ocean_crust_model(), np.arange(1.0, 3.5, 1.0),
+                                    T=32.0, nw=128, np_slow=64, free_surface=True)
+    assert np.array_equal(z["gather"], g) and np.array_equal(z["offsets"], offs)
+    seis_main(["-p", "0.25", "-n", "256", "--no-plot"])
+    d = np.loadtxt(tmp_path / "seismogram_p0.2500.txt")
+    t, s = compute_seismogram(default_ocean_crust_model(), 0.25, nw=256)
+    assert d.shape == (512, 2) and np.allclose(d[:, 1], s, rtol=1e-7, atol=1e-7 * np.abs(s).max())
