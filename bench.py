@@ -42,6 +42,12 @@ WORKLOAD = dict(workload="kennett_gather_21layer", layers=21, n_sub=20, seed=1, 
 FLOPS_PER_UPDATE = 340.0          # reference-literal count per (omega, p, interface) update
 FLOPS_PER_PAIR_FS = 25.0          # free-surface epilogue per (omega, p)
 FLOPS_PER_BESSEL_TERM = 6.0       # per (r, omega, p), J0 evaluation counted separately
+# Adjoint (gradient / Jacobian) update, literal count of the code with the same convention
+# (cmul 6, cadd 2, reciprocal 6): forward step 340 + reverse of the step 920 (13 products of
+# 2x2 complex matrices at 56, entry-wise phase / determinant terms) + coefficient-tangent
+# contraction 480 (10 x 6 complex multiply-adds) + phase-derivative terms 56 + residual
+# contraction 16 = 1812.
+FLOPS_PER_ADJOINT_UPDATE = 1812.0
 L2_FLUSH_BYTES = 256 << 20
 NOMINAL_FP64_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
 
@@ -172,9 +178,12 @@ def bench_inversion(torch, dev, reps):
     upd = 64 * 1024 * 20
     t = model_to_tensors(true)
     init = np.concatenate([start.alpha[1:], start.beta[1:], start.rho[1:], start.thickness[1:-1]])
+    peak = fp64_peak(torch, dev)
+    alg = FLOPS_PER_ADJOINT_UPDATE * upd / (ms_grad * 1e-3) / 1e12
     out = {"workload": "tau-p LM, 21 layers / 79 params, 64 p x 1024 omega",
            "grad_evals_per_s": 1e3 / ms_grad, "ms_per_grad_eval": ms_grad,
            "adjoint_updates_per_s": upd / (ms_grad * 1e-3),
+           "adjoint_alg_tflops": alg, "adjoint_frac_of_fp64_peak": alg / peak,
            "ms_per_jacobian": ms_jac, "ms_per_forward": ms_fwd}
     for hess in ("gauss-newton", "exact"):
         its = 10 if hess == "gauss-newton" else 2
@@ -254,10 +263,14 @@ def bench_batched(torch, dev, reps, n_models=4096):
     per_pair_call = (time.perf_counter() - t0) / calls
     n_pairs = sum(len(it.p) for it in items)
     batched_models_per_s = n_models / (ms * 1e-3)
+    alg = (FLOPS_PER_UPDATE * work["forward_updates"]
+           + FLOPS_PER_ADJOINT_UPDATE * work["gradient_updates"]) / (ms * 1e-3) / 1e12
+    peak = fp64_peak(torch, dev)
     return {"workload": "4096 uneven models, half forward+gradient", "schedule": list(best),
             "autotune_ms": {str(k): v for k, v in times.items()}, "ms_per_batch": ms,
             "models_per_s": batched_models_per_s, **work,
             "updates_per_s": (work["forward_updates"] + work["gradient_updates"]) / (ms * 1e-3),
+            "alg_tflops": alg, "frac_of_fp64_peak": alg / peak,
             "plain_per_model_call_models_per_s": 1.0 / per_model,
             "plain_per_slowness_call_models_per_s": n_models / (per_pair_call * n_pairs),
             "speedup_vs_per_model_calls": batched_models_per_s * per_model,

@@ -49,6 +49,21 @@ __host__ __device__ constexpr double hankel_a(int k) {
 __host__ __device__ constexpr double hankel_p(int m) { return (m % 2 ? -1.0 : 1.0) * hankel_a(2 * m); }
 __host__ __device__ constexpr double hankel_q(int m) { return (m % 2 ? -1.0 : 1.0) * hankel_a(2 * m + 1); }
 
+// J0 from cos x, sin x, amp = sqrt(1 / (pi x)) and y = 1 / x with the first NT terms of P
+// and Q (NT = 7: x >= 25, NT = 5: x >= 60, NT = 4: x >= 100, each < 1e-16 absolute).
+template <int NT>
+__device__ __forceinline__ double j0_asym_terms(double amp, double y, double c, double s) {
+  const double q = y * y;
+  double P = hankel_p(NT - 1), Q = hankel_q(NT - 1);
+#pragma unroll
+  for (int m = NT - 2; m >= 0; --m) {
+    P = fma(P, q, hankel_p(m));
+    Q = fma(Q, q, hankel_q(m));
+  }
+  Q *= y;
+  return amp * fma(P + Q, c, (P - Q) * s);
+}
+
 // J0(x) for x >= kJ0X0 given c = cos x, s = sin x.
 __device__ __forceinline__ double j0_asymptotic(double x, double c, double s) {
   const double amp = rsqrt(3.14159265358979323846 * x);  // sqrt(1 / (pi x))
@@ -69,6 +84,34 @@ constexpr int kRotSteps = 32;
 // Slownesses staged per shared-memory chunk (p_j and pw_j * dp side by side).
 constexpr int kChunk = 256;
 
+// Terms of one fast chunk for one thread: exact cos / sin anchor every kRotSteps, rotation
+// in between; 1 / x and sqrt(1 / (pi x)) from the staged per-slowness reciprocals.
+template <int NT>
+__device__ __forceinline__ void fast_chunk(const double2* s_pf, const double2* s_ip, int n,
+                                           double om, double r, double inv_omr, double isq_pomr,
+                                           double cdl, double sd, int n_w, const double2*& Rp,
+                                           double& ax, double& ay) {
+  double c, s;
+  for (int g = 0; g < n; g += kRotSteps) {
+    const int m = min(kRotSteps, n - g);
+    sincos((om * s_pf[g].x) * r, &s, &c);
+#pragma unroll 4
+    for (int k = g; k < g + m; ++k) {
+      const double f = s_pf[k].y;
+      const double2 ip = s_ip[k];
+      const double2 rv = __ldg(Rp);
+      Rp += n_w;
+      const double jv = j0_asym_terms<NT>(ip.y * isq_pomr, ip.x * inv_omr, c, s);
+      const double c2 = fma(c, cdl, -s * sd);
+      s = fma(s, cdl, c * sd);
+      c = c2;
+      const double t = jv * f;
+      ax = fma(t, rv.x, ax);
+      ay = fma(t, rv.y, ay);
+    }
+  }
+}
+
 // One thread per (omega, offset) and slowness slice.  Per chunk of the slice, the block
 // stages (p_j, pw_j dp) in shared memory and checks once whether the chunk continues the
 // slice's arithmetic progression (to 4.5 ulp); inside such a chunk cos / sin of
@@ -80,7 +123,8 @@ bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ 
                       const double* __restrict__ omega, int n_w,
                       const double* __restrict__ offsets, int n_r, int p_per_slice,
                       double2* __restrict__ partial) {
-  __shared__ double2 s_pf[kChunk];
+  __shared__ double2 s_pf[kChunk];  // (p_j, pw_j dp)
+  __shared__ double2 s_ip[kChunk];  // (1 / p_j, 1 / sqrt(p_j))
   const int tid = threadIdx.y * kBsW + threadIdx.x;
   const int iw = blockIdx.x * kBsW + threadIdx.x;
   const int ir = blockIdx.y * kBsR + threadIdx.y;
@@ -90,6 +134,9 @@ bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ 
   const double om = active ? omega[iw] : 0.0;
   const double r = active ? offsets[ir] : 0.0;
   const double omr = om * r;
+  // per-thread factors of 1 / x and sqrt(1 / (pi x)) with x = omr p (used where x >= 25)
+  const double inv_omr = omr > 0.0 ? 1.0 / omr : 0.0;
+  const double isq_pomr = omr > 0.0 ? rsqrt(3.14159265358979323846 * omr) : 0.0;
   // Linear model of the slice's slownesses: p_j ~ p0 + (j - j_begin) * step.
   const double p0 = __ldg(p + j_begin);
   const double step =
@@ -108,6 +155,7 @@ bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ 
       const int j = jc + tid;
       const double pj = __ldg(p + j);
       s_pf[tid] = make_double2(pj, __ldg(pw + j) * dp);
+      s_ip[tid] = make_double2(1.0 / pj, rsqrt(pj));
       const double lin = fma((double)(j - j_begin), step, p0);
       ok = fabs(pj - lin) <= 1e-15 * fabs(pj);
     }
@@ -116,25 +164,16 @@ bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ 
     if (!active) continue;
     // Fast chunk: slownesses in arithmetic progression with x increasing from >= 25, so every
     // term takes the asymptotic branch; anchor cos / sin exactly every kRotSteps terms and
-    // rotate in between (no data-dependent branches in the inner loop).
-    if (uniform && step > 0.0 && omr > 0.0 && (om * s_pf[0].x) * r >= kJ0X0) {
-      for (int g = 0; g < n; g += kRotSteps) {
-        const int m = min(kRotSteps, n - g);
-        sincos((om * s_pf[g].x) * r, &s, &c);
-#pragma unroll 4
-        for (int k = g; k < g + m; ++k) {
-          const double2 pf = s_pf[k];
-          const double2 rv = __ldg(Rp);
-          Rp += n_w;
-          const double jv = j0_asymptotic((om * pf.x) * r, c, s);
-          const double c2 = fma(c, cdl, -s * sd);
-          s = fma(s, cdl, c * sd);
-          c = c2;
-          const double t = jv * pf.y;
-          ax = fma(t, rv.x, ax);
-          ay = fma(t, rv.y, ay);
-        }
-      }
+    // rotate in between (no data-dependent branches in the inner loop).  The number of
+    // expansion terms follows from the chunk's smallest argument.
+    const double x_first = (om * s_pf[0].x) * r;
+    if (uniform && step > 0.0 && omr > 0.0 && x_first >= kJ0X0) {
+      if (x_first >= 100.0)
+        fast_chunk<4>(s_pf, s_ip, n, om, r, inv_omr, isq_pomr, cdl, sd, n_w, Rp, ax, ay);
+      else if (x_first >= 60.0)
+        fast_chunk<5>(s_pf, s_ip, n, om, r, inv_omr, isq_pomr, cdl, sd, n_w, Rp, ax, ay);
+      else
+        fast_chunk<7>(s_pf, s_ip, n, om, r, inv_omr, isq_pomr, cdl, sd, n_w, Rp, ax, ay);
       since = kRotSteps;
       continue;
     }
