@@ -158,8 +158,9 @@ batch_forward_kernel(unsigned char* plan, const double2* __restrict__ omega_all,
       const int iw = item.w0 + k;
       const double2 wv = omega_all[d.omega_off + iw];
       const cd w = mk(wv.x, wv.y);
-      const cd rpp = sweep(w, d.n_layers, lay, coef);
-      const cd out = pp_surface(rpp, cexp_(w * lay[0].ca), fs);
+      cd e0;
+      const cd rpp = sweep(w, d.n_layers, lay, coef, &e0);
+      const cd out = pp_surface(rpp, e0, fs);
       R_all[d.R_off + (size_t)pr.j * d.n_w + iw] = make_double2(out.x, out.y);
     }
   }

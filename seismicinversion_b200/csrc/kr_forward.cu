@@ -32,8 +32,9 @@ reflectivity_kernel(const double* __restrict__ tab, int n_layers, const double* 
     if (iw >= n_w) break;
     const double2 wv = omega[iw];
     const cd w = mk(wv.x, wv.y);
-    const cd rpp = sweep(w, n_layers, s_layer, s_iface);
-    const cd out = pp_surface(rpp, cexp_(w * s_layer[0].ca), free_surface != 0);
+    cd e0;
+    const cd rpp = sweep(w, n_layers, s_layer, s_iface, &e0);
+    const cd out = pp_surface(rpp, e0, free_surface != 0);
     R[(size_t)ip * n_w + iw] = make_double2(out.x, out.y);
   }
 }

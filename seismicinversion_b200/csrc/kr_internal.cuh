@@ -45,9 +45,11 @@ __device__ __forceinline__ void block_prologue(const double* __restrict__ tab, i
 }
 
 // The full upward sweep for one (omega, p) with coefficients in shared memory.
-// Returns RRd_PP below the ocean.
+// Returns RRd_PP below the ocean and the ocean phase factor e0.  The phase factors of the
+// next layer are computed one step ahead, so their exp / sincos chains overlap the current
+// step's algebra; the last (ocean-bottom) step forms only RRd_00.
 __device__ __forceinline__ cd sweep(cd w, int n_layers, const LayerP* s_layer,
-                                    const Iface* s_iface) {
+                                    const Iface* s_iface, cd* e0_out) {
   const int I = n_layers - 1;
   // Bottom interface: RRd below it is 0, so RRd = Rd.
   M2 r;
@@ -55,13 +57,19 @@ __device__ __forceinline__ cd sweep(cd w, int n_layers, const LayerP* s_layer,
   r.b = s_iface[I - 1].rd12;
   r.c = s_iface[I - 1].rd12;
   r.d = s_iface[I - 1].rd22;
-  for (int i = I - 2; i >= 0; --i) {
-    const LayerP& lb = s_layer[i + 1];
-    cd ea = cexp_(w * lb.ca);
-    cd eb = cexp_(w * lb.cb);
-    r = kennett_step(r, ea, eb, s_iface[i]);
+  if (I == 1) {
+    *e0_out = cexp_(w * s_layer[0].ca);
+    return r.a;
   }
-  return r.a;
+  cd ea = cexp_(w * s_layer[I - 1].ca), eb = cexp_(w * s_layer[I - 1].cb);
+  for (int i = I - 2; i >= 1; --i) {
+    const cd ea_n = cexp_(w * s_layer[i].ca), eb_n = cexp_(w * s_layer[i].cb);
+    r = kennett_step(r, ea, eb, s_iface[i]);
+    ea = ea_n;
+    eb = eb_n;
+  }
+  *e0_out = cexp_(w * s_layer[0].ca);
+  return kennett_last_step_pp(r, ea, eb, s_iface[0]);
 }
 
 // Block-cooperative copy of n bytes (multiple of 16, 16-byte aligned) into shared memory.

@@ -24,7 +24,7 @@
 
 namespace kr {
 
-struct cd {
+struct alignas(16) cd {  // 16-byte aligned: one 128-bit load / store per complex value
   double x, y;
 };
 
@@ -282,6 +282,24 @@ KR_HD M2 kennett_step(const M2& r, cd ea, cd eb, const Iface& f) {
   o.c = f.rd12 + (z21 * f.td11 + z22 * f.td21);
   o.d = f.rd22 + (z21 * f.td12 + z22 * f.td22);
   return o;
+}
+
+// The last (ocean-bottom) step, returning only RRd_00: that interface's Rd has one entry and
+// Td one column (Td = [[t11, 0], [t21, 0]]), so RRd_00 = rd11 + t11 (x11 t11 + x12 t21)
+// + t21 (x21 t11 + x22 t21) with X = MT (I - Ru MT)^-1 (same products as kennett_step).
+KR_HD cd kennett_last_step_pp(const M2& r, cd ea, cd eb, const Iface& f) {
+  cd eaea = ea * ea, ebeb = eb * eb, eaeb = ea * eb;
+  cd m11 = eaea * r.a, m12 = eaeb * r.b, m21 = eaeb * r.c, m22 = ebeb * r.d;
+  cd n11 = 1.0 - (f.ru11 * m11 + f.ru12 * m21);
+  cd n12 = -(f.ru11 * m12 + f.ru12 * m22);
+  cd n21 = -(f.ru12 * m11 + f.ru22 * m21);
+  cd n22 = 1.0 - (f.ru12 * m12 + f.ru22 * m22);
+  cd idet = recip(n11 * n22 - n12 * n21);
+  cd u11 = n22 * idet, u12 = -(n12 * idet), u21 = -(n21 * idet), u22 = n11 * idet;
+  cd x11 = m11 * u11 + m12 * u21, x12 = m11 * u12 + m12 * u22;
+  cd x21 = m21 * u11 + m22 * u21, x22 = m21 * u12 + m22 * u22;
+  cd z11 = f.td11 * x11 + f.td21 * x21, z12 = f.td11 * x12 + f.td21 * x22;
+  return f.rd11 + (z11 * f.td11 + z12 * f.td21);
 }
 
 // PP reflectivity at the surface from RRd_PP below the ocean and the ocean phase e0.
