@@ -83,6 +83,8 @@ class ModelBatch:
         tabs, ps, ws, obs = [], [], [], []
         lo = po = wo = ro = oo = go = 0
         self.max_layers = 2
+        # items passing the very same p / omega / R_obs object share one device copy
+        seen_p, seen_w, seen_o = {}, {}, {}
         for b, it in enumerate(items):
             tab = pack_layers(it.model)
             D.validate_table(tab)
@@ -94,26 +96,38 @@ class ModelBatch:
             if it.gradient:
                 if it.R_obs is None:
                     raise ValueError(f"batch item {b}: gradient requested without R_obs")
-                o = _flat(it.R_obs, torch.complex128)
-                if o.numel() != n_p * n_w:
-                    raise ValueError(f"batch item {b}: R_obs must have shape ({n_p}, {n_w})")
                 flags |= _lib.KR_BATCH_GRADIENT | (_lib.KR_BATCH_STORE_R if it.store_R else 0)
             d = desc[b]
             d["n_layers"], d["n_p"], d["n_w"], d["flags"] = L, n_p, n_w, flags
-            d["layers_off"], d["p_off"], d["omega_off"] = lo, po, wo
+            d["layers_off"] = lo
             tabs.append(tab.ravel())
-            ps.append(p)
-            ws.append(w)
             lo += tab.size
-            po += n_p
-            wo += n_w
+            if id(it.p) in seen_p:
+                d["p_off"] = seen_p[id(it.p)]
+            else:
+                d["p_off"] = seen_p[id(it.p)] = po
+                ps.append(p)
+                po += n_p
+            if id(it.omega) in seen_w:
+                d["omega_off"] = seen_w[id(it.omega)]
+            else:
+                d["omega_off"] = seen_w[id(it.omega)] = wo
+                ws.append(w)
+                wo += n_w
             if (not it.gradient) or it.store_R:
                 d["R_off"] = ro
                 ro += n_p * n_w
             if it.gradient:
-                d["obs_off"], d["grad_off"] = oo, go
-                obs.append(o)
-                oo += o.numel()
+                if id(it.R_obs) in seen_o:
+                    d["obs_off"] = seen_o[id(it.R_obs)]
+                else:
+                    o = _flat(it.R_obs, torch.complex128)
+                    if o.numel() != n_p * n_w:
+                        raise ValueError(f"batch item {b}: R_obs must have shape ({n_p}, {n_w})")
+                    d["obs_off"] = seen_o[id(it.R_obs)] = oo
+                    obs.append(o)
+                    oo += o.numel()
+                d["grad_off"] = go
                 go += 4 * L + 1
             self.max_layers = max(self.max_layers, L)
         self.desc = desc

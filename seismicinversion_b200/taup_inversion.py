@@ -8,8 +8,8 @@ all slownesses are one launch of the adjoint kernel (``kr_misfit_gradient``) ins
 per-slowness autograd pass, and the Hessian is either
 
 * ``hessian="exact"`` (default): central differences of the exact adjoint gradient
-  (2P gradient launches, ~1e-8 relative), standing in for the reference's
-  ``torch.func.hessian``; or
+  (the 2P perturbed models are one batched gradient launch, ~1e-8 relative), standing in
+  for the reference's ``torch.func.hessian``; or
 * ``hessian="gauss-newton"``: 2 Re(J^H J) from one ``kr_jacobian`` launch.
 
 The LaTeX / TikZ / plotting writers of the reference module are presentation, not compute,
@@ -91,15 +91,37 @@ class _Problem:
         r = R - self.R_obs
         return float((r.real**2 + r.imag**2).sum())
 
+    def _models(self, rows: np.ndarray) -> list:
+        out = []
+        for m in rows:
+            a, b, r, h = _unpack_params(torch.as_tensor(m, dtype=_FDTYPE), *self.ref)
+            out.append(LayerModel(a.numpy(), b.numpy(), r.numpy(), h.numpy(), self.Q[0].numpy(),
+                                  self.Q[1].numpy()))
+        return out
+
     def hessian_exact(self, phys: np.ndarray, step: float = 1e-5) -> np.ndarray:
+        """Central differences of the exact adjoint gradient, all 2P perturbed models in one
+        batched launch (the batch is built on the first call and updated in place after)."""
+        from .batch import BatchItem, ModelBatch
+
         P = len(phys)
-        H = np.empty((P, P))
-        for j in range(P):
-            d = step * max(abs(phys[j]), 1e-3)
-            mp, mm = phys.copy(), phys.copy()
-            mp[j] += d
-            mm[j] -= d
-            H[:, j] = (self.chi_grad(mp)[1] - self.chi_grad(mm)[1]) / (2.0 * d)
+        d = step * np.maximum(np.abs(phys), 1e-3)
+        rows = np.repeat(phys[None, :], 2 * P, axis=0)
+        rows[np.arange(P), np.arange(P)] += d
+        rows[P + np.arange(P), np.arange(P)] -= d
+        models = self._models(rows)
+        batch = getattr(self, "_hbatch", None)
+        if batch is None or len(batch.desc) != 2 * P:
+            items = [BatchItem(m, self.p, self.omega, gradient=True, R_obs=self.R_obs)
+                     for m in models]
+            batch = self._hbatch = ModelBatch(items, device=self.dev)
+        else:
+            batch.update_layers(models)
+        batch.launch()
+        # every item is a gradient model with L layers: rows of 4L + 1 (gradient, chi) in order
+        rows = batch.chi_grad[:2 * P * (4 * self.L + 1)].view(2 * P, 4 * self.L + 1)
+        g = rows[:, self.idx].cpu().numpy()
+        H = (g[:P] - g[P:]).T / (2.0 * d[None, :])
         return 0.5 * (H + H.T)
 
     def hessian_gn(self, phys: np.ndarray) -> np.ndarray:

@@ -180,6 +180,42 @@ def test_hessian_vs_reference(golden):
     assert rel_err(H.numpy(), g["H_p0.2_alpha1x1.02"]) < 1e-6
 
 
+def test_batched_exact_hessian_matches_sequential_differences():
+    """The 2P-model batched Hessian equals central differences of single gradient launches."""
+    from seismicinversion_b200.earth_models import random_layered_model
+    from seismicinversion_b200.kennett_torch import _pack_params, model_to_tensors
+    from seismicinversion_b200.taup_inversion import _Problem
+
+    m = random_layered_model(6, seed=4)
+    t = model_to_tensors(m)
+    p = np.array([0.05, 0.15, 0.3])
+    w = torch.arange(1, 49, dtype=torch.float64) * (2 * np.pi / 64.0)
+    tab = torch.stack([t[k] for k in ("alpha", "beta", "rho", "thickness", "Q_alpha",
+                                      "Q_beta")]).cuda()
+    from seismicinversion_b200 import device as D
+
+    R_obs = D.reflectivity(tab, torch.as_tensor(p).cuda(), w.cuda().to(torch.complex128))
+    prob = _Problem(t["alpha"], t["beta"], t["rho"], t["thickness"], t["Q_alpha"], t["Q_beta"],
+                    p, w, R_obs)
+    base = _pack_params(t["alpha"], t["beta"], t["rho"], t["thickness"]).numpy()
+    phys = base * np.exp(0.03 * np.sin(np.arange(len(base))))
+    for _ in range(2):  # second call reuses the batch with updated layers
+        H = prob.hessian_exact(phys)
+        phys = phys * 1.01
+    phys = phys / 1.01
+    P = len(phys)
+    Hs = np.empty((P, P))
+    for j in range(P):
+        d = 1e-5 * max(abs(phys[j]), 1e-3)
+        mp, mm = phys.copy(), phys.copy()
+        mp[j] += d
+        mm[j] -= d
+        Hs[:, j] = (prob.chi_grad(mp)[1] - prob.chi_grad(mm)[1]) / (2 * d)
+    Hs = 0.5 * (Hs + Hs.T)
+    # same step, different kernels: the gradients agree to rounding, amplified by 1 / (2 d)
+    assert np.max(np.abs(H - Hs)) <= 1e-6 * np.max(np.abs(Hs))
+
+
 def test_invert_taup_matches_reference_run(golden):
     from seismicinversion_b200.earth_models import default_ocean_crust_model
     from seismicinversion_b200.taup_inversion import invert_taup
