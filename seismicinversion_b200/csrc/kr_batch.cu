@@ -24,6 +24,7 @@
 
 #include "kr_adjoint.cuh"
 #include "kr_internal.cuh"
+#include "kr_phase.cuh"
 
 namespace kr {
 
@@ -131,11 +132,16 @@ __device__ __forceinline__ int next_item(int* counter) {
   return s_item;
 }
 
+// Forward items: one (model, slowness) pair and a frequency range [w0, w0 + nw).  With
+// tab_entries > 0 the block tabulates the phase factors of the 128-frequency tiles the range
+// touches (kr_phase.cuh; same tiles and verdicts as kr_reflectivity, so the results are
+// bit-identical to a per-model call).
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS)
 batch_forward_kernel(unsigned char* plan, const double2* __restrict__ omega_all,
-                     double2* __restrict__ R_all) {
-  extern __shared__ __align__(16) unsigned char s_pair[];  // layer terms + coefficients
+                     double2* __restrict__ R_all, int tab_entries) {
+  extern __shared__ __align__(16) unsigned char s_pair[];  // layer terms + coefficients + table
+  __shared__ unsigned s_bad;
   PlanHeader* h = reinterpret_cast<PlanHeader*>(plan);
   const kr_model_desc* models = reinterpret_cast<const kr_model_desc*>(plan + h->off_models);
   const PairRec* pairs = reinterpret_cast<const PairRec*>(plan + h->off_pairs);
@@ -151,15 +157,26 @@ batch_forward_kernel(unsigned char* plan, const double2* __restrict__ omega_all,
     const bool fs = (d.flags & KR_FREE_SURFACE) != 0;
     LayerP* lay = reinterpret_cast<LayerP*>(s_pair);
     Iface* coef = reinterpret_cast<Iface*>(s_pair + sizeof(LayerP) * d.n_layers);
+    cd* s_ph = reinterpret_cast<cd*>(s_pair + prologue_smem_bytes(d.n_layers));
     copy16(lay, v.lay, sizeof(LayerP) * d.n_layers);
     copy16(coef, v.coef, sizeof(Iface) * (d.n_layers - 1));
     __syncthreads();
+    const double2* om = omega_all + d.omega_off;
+    const int u0 = item.w0 / kPhTile;
+    unsigned mask = 0u;
+    if (tab_entries > 0 && phase_table_model(d.n_layers))
+      mask = build_phase_table(om, d.n_w, grid_line(om, d.n_w), u0,
+                               (item.w0 + item.nw - 1) / kPhTile - u0 + 1, tab_entries,
+                               d.n_layers, lay, s_ph, &s_bad);
     for (int k = threadIdx.x; k < item.nw; k += THREADS) {
       const int iw = item.w0 + k;
-      const double2 wv = omega_all[d.omega_off + iw];
-      const cd w = mk(wv.x, wv.y);
-      cd e0;
-      const cd rpp = sweep(w, d.n_layers, lay, coef, &e0);
+      cd e0, rpp;
+      if ((mask >> (iw / kPhTile - u0)) & 1u) {
+        rpp = sweep_ph(d.n_layers, coef, phase_at(s_ph, tab_entries, iw, u0), &e0);
+      } else {
+        const double2 wv = om[iw];
+        rpp = sweep(mk(wv.x, wv.y), d.n_layers, lay, coef, &e0);
+      }
       const cd out = pp_surface(rpp, e0, fs);
       R_all[d.R_off + (size_t)pr.j * d.n_w + iw] = make_double2(out.x, out.y);
     }
@@ -372,6 +389,14 @@ static size_t fwd_smem(int max_layers) {
   return sizeof(LayerP) * (size_t)max_layers + sizeof(Iface) * (size_t)(max_layers - 1);
 }
 
+// Phase-table entries per phase for items of tile_w frequencies (0: direct exponentials for
+// every model).  Only models that tabulate in kr_reflectivity (phase_table_model) use the
+// table, so the smem reserved is that of the largest such model.
+static int fwd_table_entries(int tile_w) {
+  const int tiles = (tile_w + kPhTile - 1) / kPhTile + 1;
+  return tiles > kPhMaxTiles ? 0 : phase_entries(tiles);
+}
+
 // gradient kernel dynamic smem and whether the slowness data is staged
 static size_t grad_smem(int threads, int max_layers, int* stage) {
   const size_t acc = sizeof(double) * (((size_t)(threads / 32) * (4 * max_layers + 1) + 1) / 2 * 2);
@@ -381,8 +406,11 @@ static size_t grad_smem(int threads, int max_layers, int* stage) {
 }
 
 template <int THREADS>
-static kr_status grids(PlanHeader& h, int max_layers, size_t* fsm, size_t* gsm, int* stage) {
-  *fsm = fwd_smem(max_layers);
+static kr_status grids(PlanHeader& h, int max_layers, int tab_entries, size_t* fsm,
+                       size_t* gsm, int* stage) {
+  const int lt = std::min(max_layers, phase_table_max_layers());
+  *fsm = fwd_smem(max_layers) +
+         (tab_entries ? sizeof(cd) * (size_t)tab_entries * 2 * (size_t)(lt - 1) : 0);
   *gsm = grad_smem(THREADS, max_layers, stage);
   if (*fsm > 48 * 1024 &&
       cudaFuncSetAttribute(batch_forward_kernel<THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -487,8 +515,9 @@ extern "C" kr_status kr_batch_launch(void* plan, const kr_batch_config* cfg, int
   PlanHeader h{};
   size_t fsm = 0, gsm = 0;
   int stage = 0;
-  kr_status s = (cfg->threads == 64) ? grids<64>(h, max_layers, &fsm, &gsm, &stage)
-                                     : grids<128>(h, max_layers, &fsm, &gsm, &stage);
+  const int tab = fwd_table_entries(cfg->tile_w);
+  kr_status s = (cfg->threads == 64) ? grids<64>(h, max_layers, tab, &fsm, &gsm, &stage)
+                                     : grids<128>(h, max_layers, tab, &fsm, &gsm, &stage);
   if (s != KR_OK) {
     set_last_error_msg("kr_batch_launch: shared-memory attribute");
     return s;
@@ -501,14 +530,14 @@ extern "C" kr_status kr_batch_launch(void* plan, const kr_batch_config* cfg, int
   if (s != KR_OK) return s;
   const double2* w = reinterpret_cast<const double2*>(omega);
   if (cfg->threads == 64) {
-    batch_forward_kernel<64><<<h.grid_fwd, 64, fsm, st>>>(pl, w, reinterpret_cast<double2*>(R));
+    batch_forward_kernel<64><<<h.grid_fwd, 64, fsm, st>>>(pl, w, reinterpret_cast<double2*>(R), tab);
     s = check_launch("kr_batch_launch: forward");
     if (s != KR_OK) return s;
     batch_gradient_kernel<64><<<h.grid_grad, 64, gsm, st>>>(
         pl, w, reinterpret_cast<const double2*>(R_obs), reinterpret_cast<double2*>(R), chi_grad,
         stage);
   } else {
-    batch_forward_kernel<128><<<h.grid_fwd, 128, fsm, st>>>(pl, w, reinterpret_cast<double2*>(R));
+    batch_forward_kernel<128><<<h.grid_fwd, 128, fsm, st>>>(pl, w, reinterpret_cast<double2*>(R), tab);
     s = check_launch("kr_batch_launch: forward");
     if (s != KR_OK) return s;
     batch_gradient_kernel<128><<<h.grid_grad, 128, gsm, st>>>(

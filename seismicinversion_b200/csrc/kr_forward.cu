@@ -8,34 +8,52 @@
 // (2x2 complex algebra per thread is not a contraction).
 #include <stdlib.h>
 
-#include "kr_internal.cuh"
+#include "kr_phase.cuh"
 
 namespace kr {
 
 constexpr int kFwdThreads = 128;
 
+// Phase factors come from a per-block table (kr_phase.cuh) for the block's frequency tiles
+// when the grid is uniform, from direct exponentials otherwise.
+constexpr int kTabTiles = kFwdTabTiles;  // frequency tiles per block on the table path
+static_assert(kFwdThreads == kPhTile, "one forward tile is one phase-table tile");
+
 template <int MINB>
 __global__ void __launch_bounds__(kFwdThreads, MINB)
 reflectivity_kernel(const double* __restrict__ tab, int n_layers, const double* __restrict__ p,
                     int n_p, const double2* __restrict__ omega, int n_w, int n_wtiles,
-                    int tiles_per_block, int free_surface, double2* __restrict__ R) {
+                    int tiles_per_block, int free_surface, int use_table,
+                    double2* __restrict__ R) {
   extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ unsigned s_bad;
   LayerP* s_layer = reinterpret_cast<LayerP*>(smem);
   Iface* s_iface = reinterpret_cast<Iface*>(smem + sizeof(LayerP) * n_layers);
+  cd* s_ph = reinterpret_cast<cd*>(smem + prologue_smem_bytes(n_layers));
   const int groups = (n_wtiles + tiles_per_block - 1) / tiles_per_block;
   const int ip = blockIdx.x / groups;
   const int t0 = (blockIdx.x % groups) * tiles_per_block;
   const int t1 = min(n_wtiles, t0 + tiles_per_block);
   block_prologue(tab, n_layers, p[ip], s_layer, s_iface);
+  unsigned mask = 0u;
+  const int entries = phase_entries(kTabTiles);
+  if (use_table)
+    mask = build_phase_table(omega, n_w, grid_line(omega, n_w), t0, t1 - t0, entries,
+                             n_layers, s_layer, s_ph, &s_bad);
+  const bool fs = free_surface != 0;
+  double2* Rp = R + (size_t)ip * n_w;
   for (int t = t0; t < t1; ++t) {
     const int iw = t * kFwdThreads + threadIdx.x;
     if (iw >= n_w) break;
-    const double2 wv = omega[iw];
-    const cd w = mk(wv.x, wv.y);
-    cd e0;
-    const cd rpp = sweep(w, n_layers, s_layer, s_iface, &e0);
-    const cd out = pp_surface(rpp, e0, free_surface != 0);
-    R[(size_t)ip * n_w + iw] = make_double2(out.x, out.y);
+    cd e0, rpp;
+    if ((mask >> (t - t0)) & 1u) {
+      rpp = sweep_ph(n_layers, s_iface, phase_at(s_ph, entries, iw, t0), &e0);
+    } else {
+      const double2 wv = omega[iw];
+      rpp = sweep(mk(wv.x, wv.y), n_layers, s_layer, s_iface, &e0);
+    }
+    const cd out = pp_surface(rpp, e0, fs);
+    Rp[iw] = make_double2(out.x, out.y);
   }
 }
 
@@ -66,10 +84,17 @@ static int forward_minb() {
 
 template <int MINB>
 static kr_status launch_forward(const double* layers, int n_layers, const double* p, int n_p,
-                                const double* omega, int n_w, int n_wtiles, size_t smem,
-                                uint32_t flags, double* R, cudaStream_t st) {
-  const int tpb = tiles_per_block(n_p, n_wtiles);
+                                const double* omega, int n_w, int n_wtiles, uint32_t flags,
+                                double* R, cudaStream_t st) {
+  size_t smem = prologue_smem_bytes(n_layers);
+  int tpb = tiles_per_block(n_p, n_wtiles);
+  const bool table = phase_table_model(n_layers);  // <= 50 KB: 4 blocks of 128 per SM
+  if (table) {
+    smem += phase_table_bytes(n_layers, kTabTiles);
+    tpb = tpb < kTabTiles ? tpb : kTabTiles;
+  }
   const long long blocks = (long long)n_p * ((n_wtiles + tpb - 1) / tpb);
+  if (blocks > 0x7fffffffLL) return KR_ERR_TOO_LARGE;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(reflectivity_kernel<MINB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -80,7 +105,7 @@ static kr_status launch_forward(const double* layers, int n_layers, const double
   }
   reflectivity_kernel<MINB><<<(unsigned)blocks, kFwdThreads, smem, st>>>(
       layers, n_layers, p, n_p, reinterpret_cast<const double2*>(omega), n_w, n_wtiles, tpb,
-      (flags & KR_FREE_SURFACE) ? 1 : 0, reinterpret_cast<double2*>(R));
+      (flags & KR_FREE_SURFACE) ? 1 : 0, table ? 1 : 0, reinterpret_cast<double2*>(R));
   return check_launch("kr_reflectivity");
 }
 
@@ -101,19 +126,13 @@ extern "C" kr_status kr_reflectivity(const double* layers, int32_t n_layers, con
   if (n_p == 0 || n_w == 0) return KR_OK;
   if (!layers || !p || !omega || !R) return KR_ERR_INVALID_ARGUMENT;
   const int n_wtiles = (n_w + kFwdThreads - 1) / kFwdThreads;
-  const long long blocks = (long long)n_p * n_wtiles;
-  if (blocks > 0x7fffffffLL) return KR_ERR_TOO_LARGE;
-  const size_t smem = prologue_smem_bytes(n_layers);
   cudaStream_t st = (cudaStream_t)stream;
   switch (forward_minb()) {
     case 6:
-      return launch_forward<6>(layers, n_layers, p, n_p, omega, n_w, n_wtiles, smem, flags, R,
-                               st);
+      return launch_forward<6>(layers, n_layers, p, n_p, omega, n_w, n_wtiles, flags, R, st);
     case 5:
-      return launch_forward<5>(layers, n_layers, p, n_p, omega, n_w, n_wtiles, smem, flags, R,
-                               st);
+      return launch_forward<5>(layers, n_layers, p, n_p, omega, n_w, n_wtiles, flags, R, st);
     default:
-      return launch_forward<4>(layers, n_layers, p, n_p, omega, n_w, n_wtiles, smem, flags, R,
-                               st);
+      return launch_forward<4>(layers, n_layers, p, n_p, omega, n_w, n_wtiles, flags, R, st);
   }
 }

@@ -13,7 +13,7 @@ namespace kr {
 constexpr int kMaxLayers = KR_MAX_LAYERS;
 
 // Dynamic shared memory of the per-slowness prologue: layer terms + interface coefficients.
-inline size_t prologue_smem_bytes(int n_layers) {
+__host__ __device__ inline size_t prologue_smem_bytes(int n_layers) {
   return sizeof(LayerP) * (size_t)n_layers + sizeof(Iface) * (size_t)(n_layers - 1);
 }
 
@@ -44,12 +44,22 @@ __device__ __forceinline__ void block_prologue(const double* __restrict__ tab, i
   __syncthreads();
 }
 
-// The full upward sweep for one (omega, p) with coefficients in shared memory.
+// Phase factors exp(omega * i eta h) and exp(omega * i neta h) of layer l, evaluated directly.
+struct PhaseDirect {
+  cd w;
+  const LayerP* lay;
+  __device__ __forceinline__ cd a(int l) const { return cexp_(w * lay[l].ca); }
+  __device__ __forceinline__ cd b(int l) const { return cexp_(w * lay[l].cb); }
+};
+
+// The full upward sweep for one (omega, p) with coefficients in shared memory; `ph` supplies
+// the layer phase factors (PhaseDirect, or a tabulated source with the same a(l) / b(l)).
 // Returns RRd_PP below the ocean and the ocean phase factor e0.  The phase factors of the
-// next layer are computed one step ahead, so their exp / sincos chains overlap the current
-// step's algebra; the last (ocean-bottom) step forms only RRd_00.
-__device__ __forceinline__ cd sweep(cd w, int n_layers, const LayerP* s_layer,
-                                    const Iface* s_iface, cd* e0_out) {
+// next layer are fetched one step ahead, so their latency overlaps the current step's
+// algebra; the last (ocean-bottom) step forms only RRd_00.
+template <class Ph>
+__device__ __forceinline__ cd sweep_ph(int n_layers, const Iface* s_iface, const Ph& ph,
+                                       cd* e0_out) {
   const int I = n_layers - 1;
   // Bottom interface: RRd below it is 0, so RRd = Rd.
   M2 r;
@@ -58,18 +68,23 @@ __device__ __forceinline__ cd sweep(cd w, int n_layers, const LayerP* s_layer,
   r.c = s_iface[I - 1].rd12;
   r.d = s_iface[I - 1].rd22;
   if (I == 1) {
-    *e0_out = cexp_(w * s_layer[0].ca);
+    *e0_out = ph.a(0);
     return r.a;
   }
-  cd ea = cexp_(w * s_layer[I - 1].ca), eb = cexp_(w * s_layer[I - 1].cb);
+  cd ea = ph.a(I - 1), eb = ph.b(I - 1);
   for (int i = I - 2; i >= 1; --i) {
-    const cd ea_n = cexp_(w * s_layer[i].ca), eb_n = cexp_(w * s_layer[i].cb);
+    const cd ea_n = ph.a(i), eb_n = ph.b(i);
     r = kennett_step(r, ea, eb, s_iface[i]);
     ea = ea_n;
     eb = eb_n;
   }
-  *e0_out = cexp_(w * s_layer[0].ca);
+  *e0_out = ph.a(0);
   return kennett_last_step_pp(r, ea, eb, s_iface[0]);
+}
+
+__device__ __forceinline__ cd sweep(cd w, int n_layers, const LayerP* s_layer,
+                                    const Iface* s_iface, cd* e0_out) {
+  return sweep_ph(n_layers, s_iface, PhaseDirect{w, s_layer}, e0_out);
 }
 
 // Block-cooperative copy of n bytes (multiple of 16, 16-byte aligned) into shared memory.

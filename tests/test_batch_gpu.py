@@ -42,11 +42,17 @@ def _check(batch, items):
 
     for b, it in enumerate(items):
         tab = D.layer_table(it.model)
-        if not it.gradient or it.store_R:
-            R1 = D.reflectivity(tab, it.p, it.omega, it.free_surface)
+        R1 = D.reflectivity(tab, it.p, it.omega, it.free_surface)
+        if not it.gradient:
+            # same phase tiles and verdicts as the per-model forward kernel: identical bits
             assert torch.equal(batch.reflectivity(b), R1), b
         if it.gradient:
-            out, _ = D.misfit_gradient(tab, it.p, it.omega, it.R_obs, it.free_surface)
+            out, Rg = D.misfit_gradient(tab, it.p, it.omega, it.R_obs, it.free_surface,
+                                        want_R=True)
+            if it.store_R:
+                # the adjoint sweep's own R: identical to the per-model adjoint call
+                assert torch.equal(batch.reflectivity(b), Rg), b
+                assert rel_err(batch.reflectivity(b).cpu().numpy(), R1.cpu().numpy()) < 1e-12
             chi, g = batch.misfit_gradient(b)
             L = it.model.n_layers
             assert abs(float(chi) - float(out[4 * L])) <= 1e-12 * abs(float(out[4 * L])), b

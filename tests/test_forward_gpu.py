@@ -79,6 +79,35 @@ def test_c1_full_grid_sampled_rows():
     assert torch.equal(one, R[rows[0]])
 
 
+def test_phase_table_and_direct_exponentials_agree():
+    """Uniform frequency grids take the tabulated phase factors, non-uniform ones the direct
+    exponentials: a grid with neighbours swapped in every tile (direct) matches the uniform
+    grid (table) after unswapping; a descending grid and a grid with one perturbed tile also
+    match the oracle."""
+    from seismicinversion_b200 import kennett_reflectivity_batch
+    from seismicinversion_b200.earth_models import random_layered_model
+
+    m = random_layered_model(20, seed=1)
+    p = np.array([0.0, 0.02, 0.3, 0.55, 0.8, 1.2])
+    om = np.arange(1, 700) * (2 * np.pi / 64) + 1j * (np.pi / 64)
+    R_tab = kennett_reflectivity_batch(m, p, om, free_surface=True)
+    perm = np.arange(len(om))
+    perm[0:-1:2], perm[1::2] = perm[1::2].copy(), perm[0:-1:2].copy()
+    R_dir = kennett_reflectivity_batch(m, p, om[perm], free_surface=True)[:, np.argsort(perm)]
+    Ro = _oracle(m, p, om, True)
+    for i in range(len(p)):
+        assert rel_err(R_tab[i], Ro[i]) < TOL and rel_err(R_dir[i], Ro[i]) < TOL, p[i]
+        assert rel_err(R_tab[i], R_dir[i]) < 1e-12, p[i]
+    R_rev = kennett_reflectivity_batch(m, p, om[::-1].copy(), free_surface=True)[:, ::-1]
+    om2 = om.copy()
+    om2[300] += 1e-9
+    R_pert = kennett_reflectivity_batch(m, p, om2, free_surface=True)
+    Ro2 = _oracle(m, p, om2, True)
+    for i in range(len(p)):
+        assert rel_err(R_rev[i], Ro[i]) < TOL, p[i]
+        assert rel_err(R_pert[i], Ro2[i]) < TOL, p[i]
+
+
 @pytest.mark.parametrize("n_sub", [1, 2, 3, 8, 63, 255])
 def test_layer_counts(n_sub):
     from seismicinversion_b200 import kennett_reflectivity_batch
