@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "kr_internal.cuh"
+#include "kr_j0_table.h"
 
 namespace kr {
 
@@ -49,19 +50,20 @@ __host__ __device__ constexpr double hankel_a(int k) {
 __host__ __device__ constexpr double hankel_p(int m) { return (m % 2 ? -1.0 : 1.0) * hankel_a(2 * m); }
 __host__ __device__ constexpr double hankel_q(int m) { return (m % 2 ? -1.0 : 1.0) * hankel_a(2 * m + 1); }
 
-// J0 from cos x, sin x, amp = sqrt(1 / (pi x)) and y = 1 / x with the first NT terms of P
-// and Q (NT = 7: x >= 25, NT = 5: x >= 60, NT = 4: x >= 100, each < 1e-16 absolute).
+// sqrt(pi x) J0(x) = P u + Q v with u = cos x + sin x, v = cos x - sin x, y = 1 / x and
+// the first NT terms of P and Q.  The first omitted terms bound the truncation error
+// (A&S 9.2.10); the absolute J0 error is below 7e-16 for NT = 7 at x >= 25 and below 1e-16
+// for NT = 5 at x >= 60, NT = 4 at x >= 100, NT = 3 at x >= 300 and NT = 2 at x >= 3000.
 template <int NT>
-__device__ __forceinline__ double j0_asym_terms(double amp, double y, double c, double s) {
+__device__ __forceinline__ double j0_asym_scaled(double y, double u, double v) {
   const double q = y * y;
-  double P = hankel_p(NT - 1), Q = hankel_q(NT - 1);
+  double P = hankel_p(NT - 1), Qs = hankel_q(NT - 1);
 #pragma unroll
   for (int m = NT - 2; m >= 0; --m) {
     P = fma(P, q, hankel_p(m));
-    Q = fma(Q, q, hankel_q(m));
+    Qs = fma(Qs, q, hankel_q(m));
   }
-  Q *= y;
-  return amp * fma(P + Q, c, (P - Q) * s);
+  return fma(P, u, Qs * (y * v));
 }
 
 // J0(x) for x >= kJ0X0 given c = cos x, s = sin x.
@@ -79,56 +81,80 @@ __device__ __forceinline__ double j0_asymptotic(double x, double c, double s) {
   return amp * fma(P + Q, c, (P - Q) * s);
 }
 
+// J0(x) for 0 <= x < 25 from the piecewise Taylor table (kr_j0_table.h, staged in shared
+// memory with rows padded to kJ0Row doubles so that lanes on different intervals fall on
+// different banks): interval k = floor(x), t = x - (k + 1/2), degree-15 Horner in t.
+// Absolute error below 5e-16 against SciPy's j0 on [0, 25).
+constexpr int kJ0Row = kJ0TabDegree + 2;
+__device__ __forceinline__ double j0_table(const double* s_j0, double x) {
+  const int k = min((int)x, kJ0TabIntervals - 1);
+  const double t = x - ((double)k + 0.5);
+  const double* a = s_j0 + k * kJ0Row;
+  double v = a[kJ0TabDegree];
+#pragma unroll
+  for (int n = kJ0TabDegree - 1; n >= 0; --n) v = fma(v, t, a[n]);
+  return v;
+}
+
 // Slowness steps between exact sincos anchors when p is an arithmetic progression.
 constexpr int kRotSteps = 32;
-// Slownesses staged per shared-memory chunk (p_j and pw_j * dp side by side).
+// Slownesses staged per shared-memory chunk: (p_j, pw_j dp) and (1 / p_j, pw_j dp / sqrt p_j).
 constexpr int kChunk = 256;
 
 // Terms of one fast chunk for one thread: exact cos / sin anchor every kRotSteps, rotation
-// in between; 1 / x and sqrt(1 / (pi x)) from the staged per-slowness reciprocals.
+// of (u, v) = (cos + sin, cos - sin) in between.  The amplitude 1 / sqrt(pi omega r) is
+// common to the thread and applied to (ax, ay) by the caller; 1 / sqrt(p_j) is staged.
 template <int NT>
-__device__ __forceinline__ void fast_chunk(const double2* s_pf, const double2* s_ip, int n,
-                                           double om, double r, double inv_omr, double isq_pomr,
-                                           double cdl, double sd, int n_w, const double2*& Rp,
-                                           double& ax, double& ay) {
-  double c, s;
+__device__ __forceinline__ void fast_chunk(const double2* s_pf, const double2* s_ig, int n,
+                                           double om, double r, double inv_omr, double cdl,
+                                           double sd, int n_w, const double2*& Rp, double& ax,
+                                           double& ay) {
+  double u, v;
   for (int g = 0; g < n; g += kRotSteps) {
     const int m = min(kRotSteps, n - g);
+    double s, c;
     sincos((om * s_pf[g].x) * r, &s, &c);
-#pragma unroll 4
+    u = c + s;
+    v = c - s;
+#pragma unroll 8
     for (int k = g; k < g + m; ++k) {
-      const double f = s_pf[k].y;
-      const double2 ip = s_ip[k];
+      const double2 ig = s_ig[k];
       const double2 rv = __ldg(Rp);
       Rp += n_w;
-      const double jv = j0_asym_terms<NT>(ip.y * isq_pomr, ip.x * inv_omr, c, s);
-      const double c2 = fma(c, cdl, -s * sd);
-      s = fma(s, cdl, c * sd);
-      c = c2;
-      const double t = jv * f;
+      const double t = j0_asym_scaled<NT>(ig.x * inv_omr, u, v) * ig.y;
+      const double u2 = fma(u, cdl, v * sd);
+      v = fma(v, cdl, -u * sd);
+      u = u2;
       ax = fma(t, rv.x, ax);
       ay = fma(t, rv.y, ay);
     }
   }
 }
 
-// One thread per (omega, offset) and slowness slice.  Per chunk of the slice, the block
+// One thread per (omega, offset) and slowness slice.  Grid: x = slowness slice, y = offset
+// group, z = frequency tile, so the hardware starts the low-frequency tiles (small J0
+// arguments, the slowest blocks) first and the cheap high-frequency tiles fill the tail.  Per chunk of the slice, the block
 // stages (p_j, pw_j dp) in shared memory and checks once whether the chunk continues the
 // slice's arithmetic progression (to 4.5 ulp); inside such a chunk cos / sin of
 // x_j = (omega p_j) r advance by one rotation per slowness, with an exact sincos anchor every
 // kRotSteps.  omega is factored out of the weight: U = omega * sum_j J0(x_j) (pw_j dp) R_j.
-__global__ void __launch_bounds__(kBsW * kBsR)
+__global__ void __launch_bounds__(kBsW * kBsR, 2)
 bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ p,
                       const double* __restrict__ pw, int n_p, double dp,
                       const double* __restrict__ omega, int n_w,
                       const double* __restrict__ offsets, int n_r, int p_per_slice,
                       double2* __restrict__ partial) {
   __shared__ double2 s_pf[kChunk];  // (p_j, pw_j dp)
-  __shared__ double2 s_ip[kChunk];  // (1 / p_j, 1 / sqrt(p_j))
+  __shared__ double2 s_ig[kChunk];  // (1 / p_j, pw_j dp / sqrt(p_j))
+  __shared__ double s_j0[kJ0TabIntervals * kJ0Row];
   const int tid = threadIdx.y * kBsW + threadIdx.x;
-  const int iw = blockIdx.x * kBsW + threadIdx.x;
+  for (int e = tid; e < kJ0TabIntervals * kJ0Row; e += kBsW * kBsR) {
+    const int k = e / kJ0Row, n = e - k * kJ0Row;
+    s_j0[e] = n <= kJ0TabDegree ? kJ0Taylor[k][n] : 0.0;  // made visible by the chunk barrier
+  }
+  const int iw = blockIdx.z * kBsW + threadIdx.x;
   const int ir = blockIdx.y * kBsR + threadIdx.y;
-  const int j_begin = blockIdx.z * p_per_slice;
+  const int j_begin = blockIdx.x * p_per_slice;
   const int j_end = min(n_p, j_begin + p_per_slice);
   const bool active = iw < n_w && ir < n_r;
   const double om = active ? omega[iw] : 0.0;
@@ -145,7 +171,8 @@ bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ 
   sincos(omr * step, &sd, &cdl);
   double c = 0.0, s = 0.0;
   int since = kRotSteps;  // steps since the last exact anchor (kRotSteps: none valid)
-  double ax = 0.0, ay = 0.0;
+  double ax = 0.0, ay = 0.0;  // fast-chunk terms, without the factor 1 / sqrt(pi omega r)
+  double bx = 0.0, by = 0.0;  // other terms, complete
   const double2* Rp = R + (size_t)j_begin * n_w + (active ? iw : 0);
   for (int jc = j_begin; jc < j_end; jc += kChunk) {
     const int n = min(kChunk, j_end - jc);
@@ -154,8 +181,9 @@ bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ 
     if (tid < n) {
       const int j = jc + tid;
       const double pj = __ldg(p + j);
-      s_pf[tid] = make_double2(pj, __ldg(pw + j) * dp);
-      s_ip[tid] = make_double2(1.0 / pj, rsqrt(pj));
+      const double f = __ldg(pw + j) * dp;
+      s_pf[tid] = make_double2(pj, f);
+      s_ig[tid] = make_double2(1.0 / pj, f * rsqrt(pj));
       const double lin = fma((double)(j - j_begin), step, p0);
       ok = fabs(pj - lin) <= 1e-15 * fabs(pj);
     }
@@ -168,12 +196,16 @@ bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ 
     // expansion terms follows from the chunk's smallest argument.
     const double x_first = (om * s_pf[0].x) * r;
     if (uniform && step > 0.0 && omr > 0.0 && x_first >= kJ0X0) {
-      if (x_first >= 100.0)
-        fast_chunk<4>(s_pf, s_ip, n, om, r, inv_omr, isq_pomr, cdl, sd, n_w, Rp, ax, ay);
+      if (x_first >= 3000.0)
+        fast_chunk<2>(s_pf, s_ig, n, om, r, inv_omr, cdl, sd, n_w, Rp, ax, ay);
+      else if (x_first >= 300.0)
+        fast_chunk<3>(s_pf, s_ig, n, om, r, inv_omr, cdl, sd, n_w, Rp, ax, ay);
+      else if (x_first >= 100.0)
+        fast_chunk<4>(s_pf, s_ig, n, om, r, inv_omr, cdl, sd, n_w, Rp, ax, ay);
       else if (x_first >= 60.0)
-        fast_chunk<5>(s_pf, s_ip, n, om, r, inv_omr, isq_pomr, cdl, sd, n_w, Rp, ax, ay);
+        fast_chunk<5>(s_pf, s_ig, n, om, r, inv_omr, cdl, sd, n_w, Rp, ax, ay);
       else
-        fast_chunk<7>(s_pf, s_ip, n, om, r, inv_omr, isq_pomr, cdl, sd, n_w, Rp, ax, ay);
+        fast_chunk<7>(s_pf, s_ig, n, om, r, inv_omr, cdl, sd, n_w, Rp, ax, ay);
       since = kRotSteps;
       continue;
     }
@@ -185,7 +217,7 @@ bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ 
       const double x = (om * pf.x) * r;
       double jv;
       if (x < kJ0X0) {
-        jv = j0(x);
+        jv = x > -kJ0X0 ? j0_table(s_j0, fabs(x)) : j0(x);
         since = kRotSteps;
       } else {
         if (since < kRotSteps) {
@@ -200,11 +232,13 @@ bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ 
         jv = j0_asymptotic(x, c, s);
       }
       const double t = jv * pf.y;
-      ax = fma(t, rv.x, ax);
-      ay = fma(t, rv.y, ay);
+      bx = fma(t, rv.x, bx);
+      by = fma(t, rv.y, by);
     }
   }
-  if (active) partial[((size_t)blockIdx.z * n_r + ir) * n_w + iw] = make_double2(ax * om, ay * om);
+  if (active)
+    partial[((size_t)blockIdx.x * n_r + ir) * n_w + iw] =
+        make_double2(fma(ax, isq_pomr, bx) * om, fma(ay, isq_pomr, by) * om);
 }
 
 __global__ void reduce_slices_kernel(const double2* __restrict__ partial, int n_slices,
@@ -348,11 +382,12 @@ extern "C" kr_status kr_bessel_sum(const double* R, const double* p, const doubl
     return cuda_status(e);
   }
   if (!R || !p || !pw) return KR_ERR_INVALID_ARGUMENT;
-  if ((n_r + kBsR - 1) / kBsR > 65535) return KR_ERR_TOO_LARGE;
+  if ((n_r + kBsR - 1) / kBsR > 65535 || (n_w + kBsW - 1) / kBsW > 65535)
+    return KR_ERR_TOO_LARGE;
   BesselPlan b = bessel_plan(n_p, n_w, n_r);
   if (!workspace || workspace_bytes < b.partial_bytes) return KR_ERR_WORKSPACE;
   double2* partial = reinterpret_cast<double2*>(workspace);
-  dim3 grid((n_w + kBsW - 1) / kBsW, (n_r + kBsR - 1) / kBsR, b.n_slices);
+  dim3 grid(b.n_slices, (n_r + kBsR - 1) / kBsR, (n_w + kBsW - 1) / kBsW);
   bessel_partial_kernel<<<grid, dim3(kBsW, kBsR), 0, st>>>(
       reinterpret_cast<const double2*>(R), p, pw, n_p, dp, omega, n_w, offsets, n_r,
       b.p_per_slice, partial);
@@ -482,7 +517,8 @@ extern "C" kr_status kr_bessel_sum_noalloc(const double* R, const double* p, con
     set_last_error_msg(buf);
     return KR_ERR_TOO_LARGE;
   }
-  if ((n_r + kBsR - 1) / kBsR > 65535) return KR_ERR_TOO_LARGE;
+  if ((n_r + kBsR - 1) / kBsR > 65535 || (n_w + kBsW - 1) / kBsW > 65535)
+    return KR_ERR_TOO_LARGE;
   cudaStream_t st = (cudaStream_t)stream;
   if (n_p == 0) {
     cudaError_t e = cudaMemsetAsync(U, 0, (size_t)n_r * n_w * sizeof(double2), st);
@@ -502,7 +538,7 @@ extern "C" kr_status kr_bessel_sum_noalloc(const double* R, const double* p, con
   const int p_per_slice = (n_p + n_slices - 1) / n_slices;
   n_slices = (n_p + p_per_slice - 1) / p_per_slice;
   double2* partial = reinterpret_cast<double2*>(scratch);
-  dim3 grid((n_w + kBsW - 1) / kBsW, (n_r + kBsR - 1) / kBsR, n_slices);
+  dim3 grid(n_slices, (n_r + kBsR - 1) / kBsR, (n_w + kBsW - 1) / kBsW);
   bessel_partial_kernel<<<grid, dim3(kBsW, kBsR), 0, st>>>(
       reinterpret_cast<const double2*>(R), p, pw, n_p, dp, omega, n_w, offsets, n_r,
       p_per_slice, partial);
