@@ -126,12 +126,10 @@ KR_HD void kennett_step_reverse(const M2& r, cd ea, cd eb, const Iface& f, const
   // Z = Td^T X
   M2 Xb = mmul(Td, Zb);
   Tdb = madd(Tdb, mmul(X, mT(Zb)));
-  // X = m U
+  // X = m U: mb = Xb U^T, Ub = m^T Xb.  U = N^-1: Nb = -U^T Ub U^T = -(m U)^T (Xb U^T)
+  // = -X^T mb (before mb's second term below), two 2x2 products fewer than the literal form.
   M2 mb = mmul(Xb, mT(U));
-  M2 Ub = mmul(mT(m), Xb);
-  // U = N^-1
-  M2 UT = mT(U);
-  M2 Nb = mneg(mmul(mmul(UT, Ub), UT));
+  M2 Nb = mneg(mmul(mT(X), mb));
   // N = I - Ru m
   M2 Rub = mneg(mmul(Nb, mT(m)));
   mb = madd(mb, mneg(mmul(Ru, Nb)));
@@ -159,24 +157,37 @@ KR_HD size_t pair_smem_bytes(int L) {
          sizeof(Iface) * (size_t)(L - 1) + sizeof(ScatTan) * (size_t)(L - 1);
 }
 
-// dR/d(alpha, beta, rho, h) of one layer.
+// dR/d(alpha, beta, rho, h) of one layer (Jacobian mode: complex), or, when the reverse
+// sweep is seeded with 2 conj(R - R_obs), the misfit gradient's real contributions
+// 2 Re(conj(R - R_obs) dR/dtheta) (gradient mode: only real parts are ever formed).
 struct Acc {
   cd a, b, r, h;
 };
+struct AccR {
+  double a, b, r, h;
+};
 
+KR_HD void set_zero(cd& x) { x = mk(0.0, 0.0); }
+KR_HD void set_zero(double& x) { x = 0.0; }
+KR_HD void acc_zero(Acc& z) { z.a = z.b = z.r = z.h = mk(0.0, 0.0); }
+KR_HD void acc_zero(AccR& z) { z.a = z.b = z.r = z.h = 0.0; }
 KR_HD Acc acc_zero() {
   Acc z;
-  z.a = z.b = z.r = z.h = mk(0.0, 0.0);
+  acc_zero(z);
   return z;
 }
+// s += x y (complex), or s += Re(x y) (real: 2 FP64 operations instead of 4)
+KR_HD void acc_add(cd& s, cd x, cd y) { s = s + x * y; }
+KR_HD void acc_add(double& s, cd x, cd y) { s = fma(x.x, y.x, fma(-x.y, y.y, s)); }
 
 // Adds the coefficient-tangent contractions of one interface to its upper / lower layer.
-KR_HD void contract(const ScatTan& t, const cd cbar[10], Acc& up, Acc& lo) {
-  cd s[6];
-  for (int j = 0; j < 6; ++j) s[j] = mk(0.0, 0.0);
+template <class AccT>
+KR_HD void contract(const ScatTan& t, const cd cbar[10], AccT& up, AccT& lo) {
+  decltype(up.a) s[6];
+  for (int j = 0; j < 6; ++j) set_zero(s[j]);
   for (int k = 0; k < 10; ++k) {
     if (cbar[k].x == 0.0 && cbar[k].y == 0.0) continue;
-    for (int j = 0; j < 6; ++j) s[j] = s[j] + cbar[k] * t.t[k][j];
+    for (int j = 0; j < 6; ++j) acc_add(s[j], cbar[k], t.t[k][j]);
   }
   up.a = up.a + s[0];
   up.b = up.b + s[1];
@@ -198,7 +209,9 @@ KR_HD int checkpoint_spacing(int nsteps) {
   return s;
 }
 
-// R and dR/dtheta for one (omega, p) pair.  Forward sweep storing the state every `seg`
+// R and dR/dtheta for one (omega, p) pair.  The sink's reflectivity(R) returns the seed of
+// the reverse sweep (1 for dR/dtheta itself, 2 conj(R - R_obs) for the misfit gradient) and
+// its AccT picks complex or real accumulation.  Forward sweep storing the state every `seg`
 // steps (and recording the top segment's step inputs and phases outright), then the reverse
 // sweep top-down, every other segment recomputed from its checkpoint (memory
 // O(sqrt(I)) states instead of I; no recomputation at all when the steps fit one segment).  sink.reflectivity(R) is called once before
@@ -229,19 +242,27 @@ KR_HD void jacobian_pair(int L, cd w, bool free_surface, int seg, const LayerP* 
     }
     r = kennett_step(r, ea, eb, coef[i]);
   }
+  typedef typename Sink::AccT AccT;
   const cd e0 = cexp_(w * lay[0].ca);
-  sink.reflectivity(pp_surface(r.a, e0, free_surface));
+  const cd seed = sink.reflectivity(pp_surface(r.a, e0, free_surface));
   // top: R = E0^2 RRd_00, or y / (1 + y) with y = E0^2 RRd_00
   cd g = mk(1.0, 0.0);
   if (free_surface) {
     cd q = recip(1.0 + (e0 * e0) * r.a);
     g = q * q;
   }
-  M2 ob = m2((e0 * e0) * g, mk(0.0, 0.0), mk(0.0, 0.0), mk(0.0, 0.0));
-  const cd f0 = 2.0 * (e0 * r.a) * g * e0 * w;
-  Acc cur = acc_zero(), nxt = acc_zero();
-  cur.a = f0 * dlay[0].ca_alpha;
-  cur.h = f0 * dlay[0].ca_h;
+  cd ob0 = (e0 * e0) * g;
+  cd f0 = 2.0 * (e0 * r.a) * g * e0 * w;
+  if (Sink::kSeeded) {
+    ob0 = ob0 * seed;
+    f0 = f0 * seed;
+  }
+  M2 ob = m2(ob0, mk(0.0, 0.0), mk(0.0, 0.0), mk(0.0, 0.0));
+  AccT cur, nxt;
+  acc_zero(cur);
+  acc_zero(nxt);
+  acc_add(cur.a, f0, dlay[0].ca_alpha);
+  acc_add(cur.h, f0, dlay[0].ca_h);
   for (int q = ncp - 1; q >= 0; --q) {
     const int s0 = q * seg;
     const int s1 = s0 + seg < nsteps ? s0 + seg : nsteps;
@@ -266,12 +287,13 @@ KR_HD void jacobian_pair(int L, cd w, bool free_surface, int seg, const LayerP* 
       contract(tan[i], cbar, cur, nxt);
       const LayerD& d = dlay[i + 1];
       const cd fa = eab * ea * w, fb = ebb * eb * w;
-      nxt.a = nxt.a + fa * d.ca_alpha;
-      nxt.b = nxt.b + fb * d.cb_beta;
-      nxt.h = nxt.h + fa * d.ca_h + fb * d.cb_h;
+      acc_add(nxt.a, fa, d.ca_alpha);
+      acc_add(nxt.b, fb, d.cb_beta);
+      acc_add(nxt.h, fa, d.ca_h);
+      acc_add(nxt.h, fb, d.cb_h);
       sink.layer(i, cur);
       cur = nxt;
-      nxt = acc_zero();
+      acc_zero(nxt);
       ob = rb;
     }
   }

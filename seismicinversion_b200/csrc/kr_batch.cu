@@ -187,26 +187,29 @@ batch_forward_kernel(unsigned char* plan, const double2* __restrict__ omega_all,
 // warp by shuffles into the warp's own accumulator row (no block barrier inside the sweep).
 template <int THREADS>
 struct BatchGradSink {
+  typedef AccR AccT;  // reverse sweep seeded with 2 conj(res): real contributions only
+  static constexpr bool kSeeded = true;
   bool valid;
   cd res;
   const double2* obs;
   double2* R_out;
   double* row;  // this warp's [4L + 1] accumulators
   int L;
-  __device__ void reflectivity(cd R) {
+  __device__ cd reflectivity(cd R) {
     res = mk(0.0, 0.0);
-    if (!valid) return;
+    if (!valid) return mk(0.0, 0.0);
     if (R_out) *R_out = make_double2(R.x, R.y);
     const double2 o = *obs;
     res = mk(R.x - o.x, R.y - o.y);
+    return mk(2.0 * res.x, -2.0 * res.y);  // 2 conj(res)
   }
-  __device__ void layer(int l, const Acc& a) {
+  __device__ void layer(int l, const AccR& a) {
     double v[4] = {0.0, 0.0, 0.0, 0.0};
     if (valid) {
-      v[0] = 2.0 * (res.x * a.a.x + res.y * a.a.y);
-      v[1] = 2.0 * (res.x * a.b.x + res.y * a.b.y);
-      v[2] = 2.0 * (res.x * a.r.x + res.y * a.r.y);
-      v[3] = 2.0 * (res.x * a.h.x + res.y * a.h.y);
+      v[0] = a.a;
+      v[1] = a.b;
+      v[2] = a.r;
+      v[3] = a.h;
     }
 #pragma unroll
     for (int k = 0; k < 4; ++k)

@@ -17,6 +17,8 @@
 // (taup_inversion.py:112-187).
 #include <stdlib.h>
 
+#include <type_traits>
+
 #include "kr_adjoint.cuh"
 #include "kr_internal.cuh"
 
@@ -77,41 +79,44 @@ __global__ void deriv_iface_kernel(const double* __restrict__ p, int n_p, int L,
   interface_tangents(p[j], i, up, dlay[j * L + i], lo, dlay[j * L + i + 1], tan[idx]);
 }
 
-template <bool GRAD>
-__device__ __forceinline__ void finalize_layer(int l, int L, const Acc& acc, bool valid, cd res,
-                                               int ip, int iw, int n_w, double2* __restrict__ J,
+// Jacobian mode: writes dR/dtheta of layer l.
+__device__ __forceinline__ void finalize_layer(int l, int L, const Acc& acc, bool valid, int ip,
+                                               int iw, int n_w, double2* __restrict__ J) {
+  if (valid) {
+    const size_t base = ((size_t)ip * 4 * L) * n_w + iw;
+    J[base + (size_t)(0 * L + l) * n_w] = make_double2(acc.a.x, acc.a.y);
+    J[base + (size_t)(1 * L + l) * n_w] = make_double2(acc.b.x, acc.b.y);
+    J[base + (size_t)(2 * L + l) * n_w] = make_double2(acc.r.x, acc.r.y);
+    J[base + (size_t)(3 * L + l) * n_w] = make_double2(acc.h.x, acc.h.y);
+  }
+}
+
+// Gradient mode: acc already holds 2 Re(conj(res) dR/dtheta) (the reverse sweep was seeded
+// with 2 conj(res)); reduced over the warp by shuffles and added to this warp's own
+// accumulator row (no block barrier).
+__device__ __forceinline__ void finalize_layer(int l, int L, const AccR& acc, bool valid,
                                                double* s_wacc) {
-  if (!GRAD) {
-    if (valid) {
-      const size_t base = ((size_t)ip * 4 * L) * n_w + iw;
-      J[base + (size_t)(0 * L + l) * n_w] = make_double2(acc.a.x, acc.a.y);
-      J[base + (size_t)(1 * L + l) * n_w] = make_double2(acc.b.x, acc.b.y);
-      J[base + (size_t)(2 * L + l) * n_w] = make_double2(acc.r.x, acc.r.y);
-      J[base + (size_t)(3 * L + l) * n_w] = make_double2(acc.h.x, acc.h.y);
-    }
-  } else {
-    // d chi / d theta = 2 Re(conj(res) dR/dtheta) = 2 (res.x dR.x + res.y dR.y), reduced over
-    // the warp by shuffles and added to this warp's own accumulator row (no block barrier).
-    double v[4] = {0.0, 0.0, 0.0, 0.0};
-    if (valid) {
-      v[0] = 2.0 * (res.x * acc.a.x + res.y * acc.a.y);
-      v[1] = 2.0 * (res.x * acc.b.x + res.y * acc.b.y);
-      v[2] = 2.0 * (res.x * acc.r.x + res.y * acc.r.y);
-      v[3] = 2.0 * (res.x * acc.h.x + res.y * acc.h.y);
-    }
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  if (valid) {
+    v[0] = acc.a;
+    v[1] = acc.b;
+    v[2] = acc.r;
+    v[3] = acc.h;
+  }
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
-      for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
-    if ((threadIdx.x & 31) == 0) {
-      double* row = s_wacc + (threadIdx.x >> 5) * (4 * L + 1);
-      for (int k = 0; k < 4; ++k) row[k * L + l] += v[k];
-    }
+  for (int k = 0; k < 4; ++k)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  if ((threadIdx.x & 31) == 0) {
+    double* row = s_wacc + (threadIdx.x >> 5) * (4 * L + 1);
+    for (int k = 0; k < 4; ++k) row[k * L + l] += v[k];
   }
 }
 
 // Receives R and the per-layer derivatives of one thread's (omega, p) pair.
 template <bool GRAD>
 struct PairSink {
+  typedef typename std::conditional<GRAD, AccR, Acc>::type AccT;
+  static constexpr bool kSeeded = GRAD;
   int L, ip, iw, n_w;
   bool valid;
   const double2* R_obs;
@@ -119,17 +124,20 @@ struct PairSink {
   double2* J;
   double* s_wacc;
   cd res;
-  __device__ void reflectivity(cd R) {
+  __device__ cd reflectivity(cd R) {
     res = mk(0.0, 0.0);
-    if (!valid) return;
+    if (!valid) return mk(0.0, 0.0);
     if (R_out) R_out[(size_t)ip * n_w + iw] = make_double2(R.x, R.y);
-    if (GRAD) {
-      const double2 o = R_obs[(size_t)ip * n_w + iw];
-      res = mk(R.x - o.x, R.y - o.y);
-    }
+    if (!GRAD) return mk(1.0, 0.0);
+    const double2 o = R_obs[(size_t)ip * n_w + iw];
+    res = mk(R.x - o.x, R.y - o.y);
+    return mk(2.0 * res.x, -2.0 * res.y);  // 2 conj(res)
   }
-  __device__ void layer(int l, const Acc& acc) {
-    finalize_layer<GRAD>(l, L, acc, valid, res, ip, iw, n_w, J, s_wacc);
+  __device__ void layer(int l, const AccT& acc) {
+    if constexpr (GRAD)
+      finalize_layer(l, L, acc, valid, s_wacc);
+    else
+      finalize_layer(l, L, acc, valid, ip, iw, n_w, J);
   }
 };
 

@@ -32,10 +32,16 @@ extern "C" void emu_reflectivity(const double* tab, int L, const double* p, int 
 
 namespace {
 struct HostSink {
+  typedef Acc AccT;
+  static constexpr bool kSeeded = false;
   int L, nw, k;
   double* R;
   double* J;  // [4L][nw] complex for this slowness
-  void reflectivity(cd r) { R[2 * k] = r.x; R[2 * k + 1] = r.y; }
+  cd reflectivity(cd r) {
+    R[2 * k] = r.x;
+    R[2 * k + 1] = r.y;
+    return mk(1.0, 0.0);
+  }
   void layer(int l, const Acc& a) {
     const cd v[4] = {a.a, a.b, a.r, a.h};
     for (int q = 0; q < 4; ++q) {
