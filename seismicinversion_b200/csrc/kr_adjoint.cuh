@@ -209,7 +209,8 @@ KR_HD int checkpoint_spacing(int nsteps) {
   return s;
 }
 
-// R and dR/dtheta for one (omega, p) pair.  The sink's reflectivity(R) returns the seed of
+// R and dR/dtheta for one (omega, p) pair; `ph` supplies the layer phase factors at omega
+// (PhaseDirect or a tabulated source), `w` itself enters the phase derivatives.  The sink's reflectivity(R) returns the seed of
 // the reverse sweep (1 for dR/dtheta itself, 2 conj(R - R_obs) for the misfit gradient) and
 // its AccT picks complex or real accumulation.  Forward sweep storing the state every `seg`
 // steps (and recording the top segment's step inputs and phases outright), then the reverse
@@ -220,9 +221,10 @@ KR_HD int checkpoint_spacing(int nsteps) {
 #ifdef __CUDACC__
 #pragma nv_exec_check_disable
 #endif
-template <class Sink>
+template <class Sink, class Ph>
 KR_HD void jacobian_pair(int L, cd w, bool free_surface, int seg, const LayerP* lay,
-                         const LayerD* dlay, const Iface* coef, const ScatTan* tan, Sink& sink) {
+                         const LayerD* dlay, const Iface* coef, const ScatTan* tan, const Ph& ph,
+                         Sink& sink) {
   const int I = L - 1;
   const int nsteps = I - 1;  // step s applies interface i = I - 2 - s
   const int ncp = nsteps > 0 ? (nsteps + seg - 1) / seg : 0;
@@ -234,7 +236,7 @@ KR_HD void jacobian_pair(int L, cd w, bool free_surface, int seg, const LayerP* 
   for (int s = 0; s < nsteps; ++s) {
     if (s % seg == 0) cp[s / seg] = r;
     const int i = I - 2 - s;
-    const cd ea = cexp_(w * lay[i + 1].ca), eb = cexp_(w * lay[i + 1].cb);
+    const cd ea = ph.a(i + 1), eb = ph.b(i + 1);
     if (s >= top0) {  // the top segment is recorded now and never recomputed
       sg[s - top0] = r;
       sea[s - top0] = ea;
@@ -243,7 +245,7 @@ KR_HD void jacobian_pair(int L, cd w, bool free_surface, int seg, const LayerP* 
     r = kennett_step(r, ea, eb, coef[i]);
   }
   typedef typename Sink::AccT AccT;
-  const cd e0 = cexp_(w * lay[0].ca);
+  const cd e0 = ph.a(0);
   const cd seed = sink.reflectivity(pp_surface(r.a, e0, free_surface));
   // top: R = E0^2 RRd_00, or y / (1 + y) with y = E0^2 RRd_00
   cd g = mk(1.0, 0.0);
@@ -271,7 +273,7 @@ KR_HD void jacobian_pair(int L, cd w, bool free_surface, int seg, const LayerP* 
       M2 x = cp[q];
       for (int s = s0; s < s1; ++s) {
         const int i = I - 2 - s;
-        const cd ea = cexp_(w * lay[i + 1].ca), eb = cexp_(w * lay[i + 1].cb);
+        const cd ea = ph.a(i + 1), eb = ph.b(i + 1);
         sg[s - s0] = x;
         sea[s - s0] = ea;
         seb[s - s0] = eb;

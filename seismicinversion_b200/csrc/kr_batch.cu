@@ -223,9 +223,11 @@ template <int THREADS>
 __global__ void __launch_bounds__(THREADS)
 batch_gradient_kernel(unsigned char* plan, const double2* __restrict__ omega_all,
                       const double2* __restrict__ obs_all, double2* __restrict__ R_all,
-                      double* __restrict__ chi_grad, int stage) {
-  // [THREADS / 32][4L + 1] accumulators (padded to 16 bytes), then the item's slowness data
+                      double* __restrict__ chi_grad, int stage, int tab_entries) {
+  // [THREADS / 32][4L + 1] accumulators (padded to 16 bytes), then the item's slowness data,
+  // then (tab_entries > 0, models that tabulate) the phase table of the item's tiles
   extern __shared__ __align__(16) double s_wacc[];
+  __shared__ unsigned s_bad;
   PlanHeader* h = reinterpret_cast<PlanHeader*>(plan);
   const kr_model_desc* models = reinterpret_cast<const kr_model_desc*>(plan + h->off_models);
   const PairRec* pairs = reinterpret_cast<const PairRec*>(plan + h->off_pairs);
@@ -258,6 +260,16 @@ batch_gradient_kernel(unsigned char* plan, const double2* __restrict__ omega_all
       v.dlay = sd;
     }
     __syncthreads();
+    const double2* om = omega_all + d.omega_off;
+    const int u0 = item.w0 / kPhTile;
+    cd* s_ph = reinterpret_cast<cd*>(
+        reinterpret_cast<unsigned char*>(s_wacc + ((THREADS / 32) * nv + 1) / 2 * 2) +
+        pair_smem_bytes(L));
+    unsigned mask = 0u;
+    if (stage && tab_entries > 0 && phase_table_model(L))
+      mask = build_phase_table(om, d.n_w, grid_line(om, d.n_w), u0,
+                               (item.w0 + item.nw - 1) / kPhTile - u0 + 1, tab_entries, L,
+                               v.lay, s_ph, &s_bad);
     double* row = s_wacc + (threadIdx.x >> 5) * nv;
     const int seg = checkpoint_spacing(L - 2 > 0 ? L - 2 : 1);
     const bool fs = (d.flags & KR_FREE_SURFACE) != 0;
@@ -276,7 +288,10 @@ batch_gradient_kernel(unsigned char* plan, const double2* __restrict__ omega_all
       const size_t e = (size_t)pr.j * d.n_w + (valid ? iw : 0);
       sink.obs = obs_all + d.obs_off + e;
       sink.R_out = (d.flags & KR_BATCH_STORE_R) ? R_all + d.R_off + e : nullptr;
-      jacobian_pair(L, w, fs, seg, v.lay, v.dlay, v.coef, v.tan, sink);
+      const int iwt = valid ? iw : item.w0;
+      const PhaseAuto ph{((mask >> (iwt / kPhTile - u0)) & 1u) != 0,
+                         phase_at(s_ph, tab_entries, iwt, u0), PhaseDirect{w, v.lay}};
+      jacobian_pair(L, w, fs, seg, v.lay, v.dlay, v.coef, v.tan, ph, sink);
       double c2 = valid ? (sink.res.x * sink.res.x + sink.res.y * sink.res.y) : 0.0;
       for (int o = 16; o > 0; o >>= 1) c2 += __shfl_down_sync(0xffffffffu, c2, o);
       if ((threadIdx.x & 31) == 0) row[4 * L] += c2;
@@ -400,21 +415,35 @@ static int fwd_table_entries(int tile_w) {
   return tiles > kPhMaxTiles ? 0 : phase_entries(tiles);
 }
 
-// gradient kernel dynamic smem and whether the slowness data is staged
-static size_t grad_smem(int threads, int max_layers, int* stage) {
+// gradient kernel dynamic smem, whether the slowness data is staged, and the phase-table
+// entries (0: none).  The table of a model that tabulates (at most phase_table_max_layers()
+// layers) sits after that model's own staged data, inside the staging area sized for the
+// largest model where it fits.
+static size_t grad_smem(int threads, int max_layers, int tab_entries, int* stage, int* tab) {
   const size_t acc = sizeof(double) * (((size_t)(threads / 32) * (4 * max_layers + 1) + 1) / 2 * 2);
   const size_t pair = pair_smem_bytes(max_layers);
   *stage = (acc + pair <= kBatchStageMax) ? 1 : 0;
-  return acc + (*stage ? pair : 0);
+  *tab = 0;
+  if (!*stage) return acc;
+  size_t area = pair;
+  if (tab_entries > 0) {
+    const int lt = std::min(max_layers, phase_table_max_layers());
+    const size_t need = pair_smem_bytes(lt) + sizeof(cd) * (size_t)tab_entries * 2 * (lt - 1);
+    if (acc + std::max(area, need) <= kBatchStageMax) {
+      area = std::max(area, need);
+      *tab = tab_entries;
+    }
+  }
+  return acc + area;
 }
 
 template <int THREADS>
 static kr_status grids(PlanHeader& h, int max_layers, int tab_entries, size_t* fsm,
-                       size_t* gsm, int* stage) {
+                       size_t* gsm, int* stage, int* gtab) {
   const int lt = std::min(max_layers, phase_table_max_layers());
   *fsm = fwd_smem(max_layers) +
          (tab_entries ? sizeof(cd) * (size_t)tab_entries * 2 * (size_t)(lt - 1) : 0);
-  *gsm = grad_smem(THREADS, max_layers, stage);
+  *gsm = grad_smem(THREADS, max_layers, tab_entries, stage, gtab);
   if (*fsm > 48 * 1024 &&
       cudaFuncSetAttribute(batch_forward_kernel<THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)*fsm) != cudaSuccess)
@@ -519,8 +548,9 @@ extern "C" kr_status kr_batch_launch(void* plan, const kr_batch_config* cfg, int
   size_t fsm = 0, gsm = 0;
   int stage = 0;
   const int tab = fwd_table_entries(cfg->tile_w);
-  kr_status s = (cfg->threads == 64) ? grids<64>(h, max_layers, tab, &fsm, &gsm, &stage)
-                                     : grids<128>(h, max_layers, tab, &fsm, &gsm, &stage);
+  int gtab = 0;
+  kr_status s = (cfg->threads == 64) ? grids<64>(h, max_layers, tab, &fsm, &gsm, &stage, &gtab)
+                                     : grids<128>(h, max_layers, tab, &fsm, &gsm, &stage, &gtab);
   if (s != KR_OK) {
     set_last_error_msg("kr_batch_launch: shared-memory attribute");
     return s;
@@ -538,14 +568,14 @@ extern "C" kr_status kr_batch_launch(void* plan, const kr_batch_config* cfg, int
     if (s != KR_OK) return s;
     batch_gradient_kernel<64><<<h.grid_grad, 64, gsm, st>>>(
         pl, w, reinterpret_cast<const double2*>(R_obs), reinterpret_cast<double2*>(R), chi_grad,
-        stage);
+        stage, gtab);
   } else {
     batch_forward_kernel<128><<<h.grid_fwd, 128, fsm, st>>>(pl, w, reinterpret_cast<double2*>(R), tab);
     s = check_launch("kr_batch_launch: forward");
     if (s != KR_OK) return s;
     batch_gradient_kernel<128><<<h.grid_grad, 128, gsm, st>>>(
         pl, w, reinterpret_cast<const double2*>(R_obs), reinterpret_cast<double2*>(R), chi_grad,
-        stage);
+        stage, gtab);
   }
   return check_launch("kr_batch_launch: gradient");
 }

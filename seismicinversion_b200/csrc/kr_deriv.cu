@@ -21,6 +21,7 @@
 
 #include "kr_adjoint.cuh"
 #include "kr_internal.cuh"
+#include "kr_phase.cuh"
 
 namespace kr {
 
@@ -145,14 +146,16 @@ template <bool GRAD, int MINB>
 __global__ void __launch_bounds__(kDerThreads, MINB)
 deriv_sweep_kernel(int L, const double* __restrict__ p, int n_p,
                    const double2* __restrict__ omega, int n_w, int n_wtiles, int free_surface,
-                   int seg, int stage, const LayerP* __restrict__ lay_all,
+                   int seg, int stage, int table, const LayerP* __restrict__ lay_all,
                    const LayerD* __restrict__ dlay_all, const Iface* __restrict__ coef_all,
                    const ScatTan* __restrict__ tan_all, const double2* __restrict__ R_obs,
                    double2* __restrict__ R_out, double2* __restrict__ J,
                    double* __restrict__ partial) {
   // dynamic smem: [warps][4L + 1] per-warp accumulators (GRAD), then, if `stage`, this
-  // block's slowness data (tangents, coefficients, layer terms, layer derivatives)
+  // block's slowness data (tangents, coefficients, layer terms, layer derivatives), then, if
+  // `table`, the phase-factor table of this block's frequency tile (kr_phase.cuh)
   extern __shared__ __align__(16) double s_wacc[];
+  __shared__ unsigned s_bad;
   const int ip = blockIdx.x / n_wtiles;
   const int iw = (blockIdx.x % n_wtiles) * kDerThreads + threadIdx.x;
   const bool valid = iw < n_w;
@@ -189,6 +192,17 @@ deriv_sweep_kernel(int L, const double* __restrict__ p, int n_p,
     lay = sl;
     dlay = sd;
   }
+  const int tile = blockIdx.x % n_wtiles;
+  const size_t acc_bytes = GRAD ? sizeof(double) * (((kDerThreads / 32) * nv + 1) / 2 * 2) : 0;
+  cd* s_ph = reinterpret_cast<cd*>(reinterpret_cast<unsigned char*>(s_wacc) + acc_bytes +
+                                   pair_smem_bytes(L));
+  bool use_tab = false;
+  if (table)
+    use_tab = (build_phase_table(omega, n_w, grid_line(omega, n_w), tile, 1, kPhHead + 1, L, lay,
+                                 s_ph, &s_bad) &
+               1u) != 0;
+  const PhaseAuto ph{use_tab, phase_at(s_ph, kPhHead + 1, valid ? iw : tile * kDerThreads, tile),
+                     PhaseDirect{w, lay}};
   PairSink<GRAD> sink;
   sink.L = L;
   sink.ip = ip;
@@ -199,7 +213,7 @@ deriv_sweep_kernel(int L, const double* __restrict__ p, int n_p,
   sink.R_out = R_out;
   sink.J = J;
   sink.s_wacc = s_wacc;
-  jacobian_pair(L, w, free_surface != 0, seg, lay, dlay, coef, tan, sink);
+  jacobian_pair(L, w, free_surface != 0, seg, lay, dlay, coef, tan, ph, sink);
   if (GRAD) {
     const cd res = sink.res;
     double c2 = valid ? (res.x * res.x + res.y * res.y) : 0.0;
@@ -250,9 +264,10 @@ static int deriv_minb() {
 template <bool GRAD, int MINB>
 static kr_status launch_sweep_v(unsigned blocks, size_t smem, cudaStream_t st, int L,
                                 const double* p, int n_p, const double2* omega, int n_w,
-                                int n_wtiles, int fs, int seg, int stage, const LayerP* lay,
-                                const LayerD* dlay, const Iface* coef, const ScatTan* tan,
-                                const double2* R_obs, double2* R, double2* J, double* partial) {
+                                int n_wtiles, int fs, int seg, int stage, int table,
+                                const LayerP* lay, const LayerD* dlay, const Iface* coef,
+                                const ScatTan* tan, const double2* R_obs, double2* R, double2* J,
+                                double* partial) {
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(deriv_sweep_kernel<GRAD, MINB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -262,21 +277,23 @@ static kr_status launch_sweep_v(unsigned blocks, size_t smem, cudaStream_t st, i
     }
   }
   deriv_sweep_kernel<GRAD, MINB><<<blocks, kDerThreads, smem, st>>>(
-      L, p, n_p, omega, n_w, n_wtiles, fs, seg, stage, lay, dlay, coef, tan, R_obs, R, J, partial);
+      L, p, n_p, omega, n_w, n_wtiles, fs, seg, stage, table, lay, dlay, coef, tan, R_obs, R, J,
+      partial);
   return KR_OK;
 }
 
 template <bool GRAD>
 static kr_status launch_sweep(int minb, unsigned blocks, size_t smem, cudaStream_t st, int L,
                               const double* p, int n_p, const double2* omega, int n_w,
-                              int n_wtiles, int fs, int seg, int stage, const LayerP* lay,
-                              const LayerD* dlay, const Iface* coef, const ScatTan* tan,
-                              const double2* R_obs, double2* R, double2* J, double* partial) {
+                              int n_wtiles, int fs, int seg, int stage, int table,
+                              const LayerP* lay, const LayerD* dlay, const Iface* coef,
+                              const ScatTan* tan, const double2* R_obs, double2* R, double2* J,
+                              double* partial) {
   if (minb == 3)
     return launch_sweep_v<GRAD, 3>(blocks, smem, st, L, p, n_p, omega, n_w, n_wtiles, fs, seg,
-                                   stage, lay, dlay, coef, tan, R_obs, R, J, partial);
+                                   stage, table, lay, dlay, coef, tan, R_obs, R, J, partial);
   return launch_sweep_v<GRAD, 2>(blocks, smem, st, L, p, n_p, omega, n_w, n_wtiles, fs, seg,
-                                 stage, lay, dlay, coef, tan, R_obs, R, J, partial);
+                                 stage, table, lay, dlay, coef, tan, R_obs, R, J, partial);
 }
 
 template <bool GRAD>
@@ -303,10 +320,13 @@ static kr_status launch_deriv(const double* layers, int L, const double* p, int 
   const size_t acc = GRAD ? sizeof(double) * (((size_t)(kDerThreads / 32) * (4 * L + 1) + 1) / 2 * 2) : 0;
   const size_t pair = pair_smem_bytes(L);
   const int stage = (acc + pair <= kStageSmemMax) ? 1 : 0;
-  const size_t smem = acc + (stage ? pair : 0);
+  // phase table of the block's tile after the staged slowness data (models that tabulate in
+  // kr_reflectivity, so R here is bit-identical to the forward kernel's)
+  const int table = (stage && phase_table_model(L)) ? 1 : 0;
+  const size_t smem = acc + (stage ? pair : 0) + (table ? phase_table_bytes(L, 1) : 0);
   s = launch_sweep<GRAD>(deriv_minb(), (unsigned)n_blocks, smem, st, L, p, n_p,
                          reinterpret_cast<const double2*>(omega), n_w, n_wtiles,
-                         (flags & KR_FREE_SURFACE) ? 1 : 0, seg, stage, w.lay, w.dlay, w.coef,
+                         (flags & KR_FREE_SURFACE) ? 1 : 0, seg, stage, table, w.lay, w.dlay, w.coef,
                          w.tan, reinterpret_cast<const double2*>(R_obs),
                          reinterpret_cast<double2*>(R), reinterpret_cast<double2*>(J), w.partial);
   if (s != KR_OK) return s;

@@ -44,14 +44,6 @@ __device__ __forceinline__ void block_prologue(const double* __restrict__ tab, i
   __syncthreads();
 }
 
-// Phase factors exp(omega * i eta h) and exp(omega * i neta h) of layer l, evaluated directly.
-struct PhaseDirect {
-  cd w;
-  const LayerP* lay;
-  __device__ __forceinline__ cd a(int l) const { return cexp_(w * lay[l].ca); }
-  __device__ __forceinline__ cd b(int l) const { return cexp_(w * lay[l].cb); }
-};
-
 // The full upward sweep for one (omega, p) with coefficients in shared memory; `ph` supplies
 // the layer phase factors (PhaseDirect, or a tabulated source with the same a(l) / b(l)).
 // Returns RRd_PP below the ocean and the ocean phase factor e0.  The phase factors of the

@@ -109,6 +109,15 @@ struct LayerP {
   double pad;  // 96 bytes: arrays of LayerP are whole 16-byte units (vector copies)
 };
 
+// Phase factors exp(omega * i eta h) and exp(omega * i neta h) of layer l, evaluated directly
+// (kernels on uniform frequency grids use a tabulated source with the same a(l) / b(l)).
+struct PhaseDirect {
+  cd w;
+  const LayerP* lay;
+  KR_HD cd a(int l) const { return cexp_(w * lay[l].ca); }
+  KR_HD cd b(int l) const { return cexp_(w * lay[l].cb); }
+};
+
 // Layer table layout (device or host): 6 rows of n_layers doubles:
 // alpha, beta, rho, thickness, Q_alpha, Q_beta.
 KR_HD LayerP layer_terms(const double* tab, int n_layers, int l, double p) {

@@ -76,6 +76,15 @@ struct PhaseTable {
   __device__ __forceinline__ cd b(int l) const { return at(2 * l + 1); }
 };
 
+// Either source, chosen per block (a uniform branch), so that callers compile once.
+struct PhaseAuto {
+  bool tab;
+  PhaseTable t;
+  PhaseDirect d;
+  __device__ __forceinline__ cd a(int l) const { return tab ? t.a(l) : d.a(l); }
+  __device__ __forceinline__ cd b(int l) const { return tab ? t.b(l) : d.b(l); }
+};
+
 __device__ __forceinline__ PhaseTable phase_at(const cd* s_ph, int entries, int k, int u0) {
   const int t = k & (kPhTile - 1);
   return PhaseTable{s_ph, entries, t & (kPhLo - 1), kPhLo + (t >> 4), kPhHead + (k >> 7) - u0};

@@ -71,7 +71,8 @@ extern "C" void emu_jacobian(const double* tab, int L, const double* p, int n_p,
     const int seg = checkpoint_spacing(I - 1 > 0 ? I - 1 : 1);
     for (int k = 0; k < nw; ++k) {
       HostSink s{L, nw, k, R + 2 * (size_t)j * nw, J + 2 * (size_t)j * 4 * L * nw};
-      jacobian_pair(L, mk(w[2 * k], w[2 * k + 1]), fs != 0, seg, lay, dlay, f, t, s);
+      jacobian_pair(L, mk(w[2 * k], w[2 * k + 1]), fs != 0, seg, lay, dlay, f, t,
+                    PhaseDirect{mk(w[2 * k], w[2 * k + 1]), lay}, s);
     }
   }
 }
