@@ -23,9 +23,17 @@ namespace kr {
 
 // ---------------- 2x2 complex matrix helpers ([[a, b], [c, d]]) ----------------
 KR_HD M2 m2(cd a, cd b, cd c, cd d) { M2 r; r.a = a; r.b = b; r.c = c; r.d = d; return r; }
-KR_HD M2 mmul(const M2& x, const M2& y) {
-  return m2(x.a * y.a + x.b * y.c, x.a * y.b + x.b * y.d, x.c * y.a + x.d * y.c,
-            x.c * y.b + x.d * y.d);
+KR_HD M2 mmul(const M2& x, const M2& y) {  // x y, fused products (cdot2)
+  return m2(cdot2(x.a, y.a, x.b, y.c), cdot2(x.a, y.b, x.b, y.d), cdot2(x.c, y.a, x.d, y.c),
+            cdot2(x.c, y.b, x.d, y.d));
+}
+KR_HD M2 mmul_neg(const M2& x, const M2& y) {  // -(x y)
+  return m2(cdot2(-x.a, y.a, -x.b, y.c), cdot2(-x.a, y.b, -x.b, y.d),
+            cdot2(-x.c, y.a, -x.d, y.c), cdot2(-x.c, y.b, -x.d, y.d));
+}
+KR_HD M2 mmac(const M2& s, const M2& x, const M2& y) {  // s + x y
+  return m2(cmac2(s.a, x.a, y.a, x.b, y.c), cmac2(s.b, x.a, y.b, x.b, y.d),
+            cmac2(s.c, x.c, y.a, x.d, y.c), cmac2(s.d, x.c, y.b, x.d, y.d));
 }
 KR_HD M2 mT(const M2& x) { return m2(x.a, x.c, x.b, x.d); }
 KR_HD M2 madd(const M2& x, const M2& y) { return m2(x.a + y.a, x.b + y.b, x.c + y.c, x.d + y.d); }
@@ -110,13 +118,15 @@ KR_HD void interface_tangents(double p, int iface, const LayerP& up, const Layer
 // and the 10 coefficient adjoints cbar (same order as ScatTan).
 KR_HD void kennett_step_reverse(const M2& r, cd ea, cd eb, const Iface& f, const M2& ob,
                                 M2& rbar, cd& eabar, cd& ebbar, cd cbar[10]) {
+  // forward quantities, formed exactly as in kennett_step
   cd eaea = ea * ea, ebeb = eb * eb, eaeb = ea * eb;
   M2 m = m2(eaea * r.a, eaeb * r.b, eaeb * r.c, ebeb * r.d);
   M2 Ru = m2(f.ru11, f.ru12, f.ru12, f.ru22);
   M2 Td = m2(f.td11, f.td12, f.td21, f.td22);
-  M2 Rm = mmul(Ru, m);
-  M2 N = m2(1.0 - Rm.a, -Rm.b, -Rm.c, 1.0 - Rm.d);
-  cd idet = recip(N.a * N.d - N.b * N.c);
+  const cd one = mk(1.0, 0.0);
+  M2 N = m2(cmac2(one, -f.ru11, m.a, -f.ru12, m.c), cdot2(-f.ru11, m.b, -f.ru12, m.d),
+            cdot2(-f.ru12, m.a, -f.ru22, m.c), cmac2(one, -f.ru12, m.b, -f.ru22, m.d));
+  cd idet = recip(cdot2(N.a, N.d, -N.b, N.c));
   M2 U = m2(N.d * idet, -(N.b * idet), -(N.c * idet), N.a * idet);
   M2 X = mmul(m, U);
   M2 Z = mmul(mT(Td), X);
@@ -125,19 +135,19 @@ KR_HD void kennett_step_reverse(const M2& r, cd ea, cd eb, const Iface& f, const
   M2 Tdb = mmul(mT(Z), ob);
   // Z = Td^T X
   M2 Xb = mmul(Td, Zb);
-  Tdb = madd(Tdb, mmul(X, mT(Zb)));
+  Tdb = mmac(Tdb, X, mT(Zb));
   // X = m U: mb = Xb U^T, Ub = m^T Xb.  U = N^-1: Nb = -U^T Ub U^T = -(m U)^T (Xb U^T)
   // = -X^T mb (before mb's second term below), two 2x2 products fewer than the literal form.
   M2 mb = mmul(Xb, mT(U));
-  M2 Nb = mneg(mmul(mT(X), mb));
+  M2 Nb = mmul_neg(mT(X), mb);
   // N = I - Ru m
-  M2 Rub = mneg(mmul(Nb, mT(m)));
-  mb = madd(mb, mneg(mmul(Ru, Nb)));
+  M2 Rub = mmul_neg(Nb, mT(m));
+  mb = mmac(mb, mneg(Ru), Nb);
   // m = E r E
   rbar = m2(mb.a * eaea, mb.b * eaeb, mb.c * eaeb, mb.d * ebeb);
-  cd cross = r.b * mb.b + r.c * mb.c;
-  eabar = 2.0 * (ea * (r.a * mb.a)) + eb * cross;
-  ebbar = 2.0 * (eb * (r.d * mb.d)) + ea * cross;
+  cd cross = cdot2(r.b, mb.b, r.c, mb.c);
+  eabar = cmac(eb * cross, 2.0 * ea, r.a * mb.a);
+  ebbar = cmac(ea * cross, 2.0 * eb, r.d * mb.d);
   cbar[0] = ob.a;
   cbar[1] = ob.b + ob.c;
   cbar[2] = ob.d;

@@ -42,6 +42,17 @@ KR_HD cd operator+(double s, cd a) { return mk(a.x + s, a.y); }
 KR_HD cd operator-(double s, cd a) { return mk(s - a.x, -a.y); }
 KR_HD cd operator-(cd a, double s) { return mk(a.x - s, a.y); }
 KR_HD cd conj(cd a) { return mk(a.x, -a.y); }
+// Fused complex multiply-accumulate: s + a b with two FMAs per component (one rounding per
+// FMA, no separate product and sum), and a b + c d as one multiply and three FMAs per
+// component.  Operand negations are free in an FMA, so s - a b is cmac(s, -a, b).
+KR_HD cd cmac(cd s, cd a, cd b) {
+  return mk(fma(a.x, b.x, fma(-a.y, b.y, s.x)), fma(a.x, b.y, fma(a.y, b.x, s.y)));
+}
+KR_HD cd cdot2(cd a, cd b, cd c, cd d) {
+  return mk(fma(a.x, b.x, fma(-a.y, b.y, fma(c.x, d.x, -(c.y * d.y)))),
+            fma(a.x, b.y, fma(a.y, b.x, fma(c.x, d.y, c.y * d.x))));
+}
+KR_HD cd cmac2(cd s, cd a, cd b, cd c, cd d) { return cmac(cmac(s, c, d), a, b); }
 KR_HD double abs2(cd a) { return fma(a.x, a.x, a.y * a.y); }
 
 // 1/z via the conjugate over |z|^2, with a power-of-two prescale so that |z|^2 neither
@@ -274,22 +285,24 @@ struct M2 {
 KR_HD M2 kennett_step(const M2& r, cd ea, cd eb, const Iface& f) {
   cd eaea = ea * ea, ebeb = eb * eb, eaeb = ea * eb;
   cd m11 = eaea * r.a, m12 = eaeb * r.b, m21 = eaeb * r.c, m22 = ebeb * r.d;
-  cd n11 = 1.0 - (f.ru11 * m11 + f.ru12 * m21);
-  cd n12 = -(f.ru11 * m12 + f.ru12 * m22);
-  cd n21 = -(f.ru12 * m11 + f.ru22 * m21);
-  cd n22 = 1.0 - (f.ru12 * m12 + f.ru22 * m22);
-  cd idet = recip(n11 * n22 - n12 * n21);
+  // N = I - Ru MT
+  const cd one = mk(1.0, 0.0);
+  cd n11 = cmac2(one, -f.ru11, m11, -f.ru12, m21);
+  cd n12 = cdot2(-f.ru11, m12, -f.ru12, m22);
+  cd n21 = cdot2(-f.ru12, m11, -f.ru22, m21);
+  cd n22 = cmac2(one, -f.ru12, m12, -f.ru22, m22);
+  cd idet = recip(cdot2(n11, n22, -n12, n21));
   cd u11 = n22 * idet, u12 = -(n12 * idet), u21 = -(n21 * idet), u22 = n11 * idet;
-  cd x11 = m11 * u11 + m12 * u21, x12 = m11 * u12 + m12 * u22;
-  cd x21 = m21 * u11 + m22 * u21, x22 = m21 * u12 + m22 * u22;
+  cd x11 = cdot2(m11, u11, m12, u21), x12 = cdot2(m11, u12, m12, u22);
+  cd x21 = cdot2(m21, u11, m22, u21), x22 = cdot2(m21, u12, m22, u22);
   // Tu X with Tu = Td^T
-  cd z11 = f.td11 * x11 + f.td21 * x21, z12 = f.td11 * x12 + f.td21 * x22;
-  cd z21 = f.td12 * x11 + f.td22 * x21, z22 = f.td12 * x12 + f.td22 * x22;
+  cd z11 = cdot2(f.td11, x11, f.td21, x21), z12 = cdot2(f.td11, x12, f.td21, x22);
+  cd z21 = cdot2(f.td12, x11, f.td22, x21), z22 = cdot2(f.td12, x12, f.td22, x22);
   M2 o;
-  o.a = f.rd11 + (z11 * f.td11 + z12 * f.td21);
-  o.b = f.rd12 + (z11 * f.td12 + z12 * f.td22);
-  o.c = f.rd12 + (z21 * f.td11 + z22 * f.td21);
-  o.d = f.rd22 + (z21 * f.td12 + z22 * f.td22);
+  o.a = cmac2(f.rd11, z11, f.td11, z12, f.td21);
+  o.b = cmac2(f.rd12, z11, f.td12, z12, f.td22);
+  o.c = cmac2(f.rd12, z21, f.td11, z22, f.td21);
+  o.d = cmac2(f.rd22, z21, f.td12, z22, f.td22);
   return o;
 }
 
@@ -299,16 +312,17 @@ KR_HD M2 kennett_step(const M2& r, cd ea, cd eb, const Iface& f) {
 KR_HD cd kennett_last_step_pp(const M2& r, cd ea, cd eb, const Iface& f) {
   cd eaea = ea * ea, ebeb = eb * eb, eaeb = ea * eb;
   cd m11 = eaea * r.a, m12 = eaeb * r.b, m21 = eaeb * r.c, m22 = ebeb * r.d;
-  cd n11 = 1.0 - (f.ru11 * m11 + f.ru12 * m21);
-  cd n12 = -(f.ru11 * m12 + f.ru12 * m22);
-  cd n21 = -(f.ru12 * m11 + f.ru22 * m21);
-  cd n22 = 1.0 - (f.ru12 * m12 + f.ru22 * m22);
-  cd idet = recip(n11 * n22 - n12 * n21);
+  const cd one = mk(1.0, 0.0);
+  cd n11 = cmac2(one, -f.ru11, m11, -f.ru12, m21);
+  cd n12 = cdot2(-f.ru11, m12, -f.ru12, m22);
+  cd n21 = cdot2(-f.ru12, m11, -f.ru22, m21);
+  cd n22 = cmac2(one, -f.ru12, m12, -f.ru22, m22);
+  cd idet = recip(cdot2(n11, n22, -n12, n21));
   cd u11 = n22 * idet, u12 = -(n12 * idet), u21 = -(n21 * idet), u22 = n11 * idet;
-  cd x11 = m11 * u11 + m12 * u21, x12 = m11 * u12 + m12 * u22;
-  cd x21 = m21 * u11 + m22 * u21, x22 = m21 * u12 + m22 * u22;
-  cd z11 = f.td11 * x11 + f.td21 * x21, z12 = f.td11 * x12 + f.td21 * x22;
-  return f.rd11 + (z11 * f.td11 + z12 * f.td21);
+  cd x11 = cdot2(m11, u11, m12, u21), x12 = cdot2(m11, u12, m12, u22);
+  cd x21 = cdot2(m21, u11, m22, u21), x22 = cdot2(m21, u12, m22, u22);
+  cd z11 = cdot2(f.td11, x11, f.td21, x21), z12 = cdot2(f.td11, x12, f.td21, x22);
+  return cmac2(f.rd11, z11, f.td11, z12, f.td21);
 }
 
 // PP reflectivity at the surface from RRd_PP below the ocean and the ocean phase e0.
