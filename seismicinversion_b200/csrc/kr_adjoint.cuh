@@ -207,27 +207,32 @@ KR_HD void contract(const ScatTan& t, const cd cbar[10], AccT& up, AccT& lo) {
   lo.r = lo.r + s[5];
 }
 
-constexpr int kSegMax = 24;  // steps kept per segment (inputs + phase factors)
-constexpr int kCpMax = 16;   // checkpoints: (I - 1) <= 16 * 16 covers 256 layers
+// Tape of one (omega, p) pair, in local memory: up to kSegMax steps of inputs and phase
+// factors (96 B per step) plus kCpMax checkpoints.  64 steps hold every model of up to 66
+// layers outright, so those run without any recomputation; measured on an uneven batch of
+// 3-64-layer models, the larger per-thread stack (~7 KB) costs far less than recomputing
+// segments did (24 steps: 1080 ms, 40: 1049 ms, 64: 963 ms per batch).
+constexpr int kSegMax = 64;
+constexpr int kCpMax = 4;  // segments of the deepest model (kr_deriv.cu checks the bound)
 
 // Steps per segment: one segment (a full tape, no recomputation) when the pair's steps fit
-// the segment buffer, else ~sqrt(steps) (checkpoints every `seg` steps).
+// the buffer, else the fewest segments of at most kSegMax steps, of balanced length.
 KR_HD int checkpoint_spacing(int nsteps) {
   if (nsteps <= kSegMax) return nsteps > 0 ? nsteps : 1;
-  int s = 1;
-  while (s * s < nsteps) ++s;
-  return s;
+  const int nseg = (nsteps + kSegMax - 1) / kSegMax;
+  return (nsteps + nseg - 1) / nseg;
 }
 
 // R and dR/dtheta for one (omega, p) pair; `ph` supplies the layer phase factors at omega
-// (PhaseDirect or a tabulated source), `w` itself enters the phase derivatives.  The sink's reflectivity(R) returns the seed of
-// the reverse sweep (1 for dR/dtheta itself, 2 conj(R - R_obs) for the misfit gradient) and
-// its AccT picks complex or real accumulation.  Forward sweep storing the state every `seg`
-// steps (and recording the top segment's step inputs and phases outright), then the reverse
-// sweep top-down, every other segment recomputed from its checkpoint (memory
-// O(sqrt(I)) states instead of I; no recomputation at all when the steps fit one segment).  sink.reflectivity(R) is called once before
-// the reverse pass, sink.layer(l, acc) once per layer l (in order 0, 1, ..., L-1) with
-// the finished dR/d(alpha_l, beta_l, rho_l, h_l).
+// (PhaseDirect or a tabulated source), `w` itself enters the phase derivatives.  The sink's
+// reflectivity(R) returns the seed of the reverse sweep (1 for dR/dtheta itself,
+// 2 conj(R - R_obs) for the misfit gradient) and its AccT picks complex or real
+// accumulation.  Forward sweep storing the state every `seg` steps (and recording the top
+// segment's step inputs and phases outright), then the reverse sweep top-down, every other
+// segment recomputed from its checkpoint (no recomputation at all when the steps fit one
+// segment).  sink.reflectivity(R) is called once before the reverse pass, sink.layer(l, acc)
+// once per layer l (in order 0, 1, ..., L-1) with the finished dR/d(alpha_l, beta_l, rho_l,
+// h_l).
 #ifdef __CUDACC__
 #pragma nv_exec_check_disable
 #endif

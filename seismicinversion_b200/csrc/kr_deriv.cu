@@ -4,7 +4,7 @@
 // Three kernels:
 //   deriv_layer_kernel : per (p, layer)      layer terms + derivative factors  -> workspace
 //   deriv_iface_kernel : per (p, interface)  coefficients + 10x6 tangents      -> workspace
-//   deriv_sweep_kernel : per (omega, p)      forward sweep with sqrt(I) checkpoints, then the
+//   deriv_sweep_kernel : per (omega, p)      forward sweep with checkpoints every <= 64 steps, then the
 //                        reverse sweep segment by segment (each segment recomputed from its
 //                        checkpoint: per-layer recomputation instead of a full tape), giving
 //                        dR/d(theta) for all 4L parameters.  JAC mode writes them
@@ -26,6 +26,8 @@
 namespace kr {
 
 constexpr int kDerThreads = 128;
+static_assert((kMaxLayers - 2 + kSegMax - 1) / kSegMax <= kCpMax,
+              "checkpoints must cover the deepest model");
 
 static size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
 

@@ -127,6 +127,44 @@ def test_misfit_gradient_vs_jacobian_and_fd():
             assert abs(out[k * L + l] - fd) / (np.max(np.abs(out[:4 * L])) + 1e-300) < 1e-6, (k, l)
 
 
+@pytest.mark.parametrize("n_sub", [100, 199])
+def test_deep_models_recomputed_segments(n_sub):
+    """Models deeper than one 64-step tape (101 and 200 layers): the reverse sweep recomputes
+    checkpointed segments.  Jacobian columns against central differences of the oracle, and
+    the misfit gradient against the Jacobian contracted with the residual."""
+    from seismicinversion_b200 import device as D
+    from seismicinversion_b200.earth_models import random_layered_model
+
+    m = random_layered_model(n_sub, seed=40 + n_sub)
+    L = m.n_layers
+    tab = D.layer_table(m)
+    p = np.array([0.08, 0.4])
+    w = np.arange(1, 48) * (2 * np.pi / 64) + 1j * (np.pi / 64)
+    Rg, J = D.jacobian(tab, p, w, True)
+    J = J.cpu().numpy()
+    Ro = O.reflectivity(m.alpha, m.beta, m.rho, m.thickness, m.Q_alpha, m.Q_beta, p, w, True)
+    assert rel_err(Rg.cpu().numpy(), Ro) < 1e-10
+    base = [m.alpha, m.beta, m.rho, m.thickness]
+    for k, l in [(0, 1), (1, L // 3), (2, L // 2), (3, L - 2), (0, L - 1), (2, L - 1)]:
+        arrs = [b.copy() for b in base]
+        d = 1e-4 * arrs[k][l]  # deep columns are small: a larger step keeps rounding noise down
+        arrs[k][l] += d
+        Rp = O.reflectivity(*arrs, m.Q_alpha, m.Q_beta, p, w, True)
+        arrs[k][l] -= 2 * d
+        Rm = O.reflectivity(*arrs, m.Q_alpha, m.Q_beta, p, w, True)
+        fd = (Rp - Rm) / (2 * d)
+        # deep layers barely move R (their column is ~1e-6 of the largest): judge each column
+        # against the Jacobian's overall scale where the finite difference is only noise
+        scale = max(np.max(np.abs(fd)), 1e-4 * np.max(np.abs(J)))
+        err = np.max(np.abs(J[:, k * L + l] - fd)) / scale
+        assert err < 1e-6, (k, l, err)
+    R_obs = Ro * (1 + 0.02 * np.sin(np.arange(w.size)))[None, :]
+    out, _ = D.misfit_gradient(tab, p, w, R_obs, True)
+    r = Rg.cpu().numpy() - R_obs
+    g_ref = 2 * (r.conj()[:, None, :] * J).real.sum(axis=(0, 2))
+    assert rel_err(out.cpu().numpy()[:4 * L], g_ref) < 1e-12
+
+
 def test_gradient_inversion_size_64p_1024w():
     """21-layer inversion model, 64 slownesses x 1024 frequencies in one launch: gradient
     entries vs central differences of the oracle misfit (subset of 8 slownesses for the

@@ -130,6 +130,31 @@ def test_adjoint_vs_reference_jacrev_21_layers(emu_jac, golden):
         assert rel_err(packed(J, m.n_layers)[0], g[f"J_p{p}"]) < 1e-10
 
 
+def test_adjoint_deep_model_recomputed_segments(emu_jac):
+    """101 layers: 99 steps do not fit one 64-step tape, so the reverse sweep runs over two
+    checkpointed segments, the second recomputed; columns checked against central
+    differences of the oracle."""
+    from seismicinversion_b200.earth_models import random_layered_model
+
+    m = random_layered_model(100, seed=31)
+    L = m.n_layers
+    w = np.arange(1, 17) * 0.25 + 0.04j
+    p = np.array([0.1, 0.45])
+    R, J = emu_jac(m, p, w, 1)
+    Ro = O.reflectivity(m.alpha, m.beta, m.rho, m.thickness, m.Q_alpha, m.Q_beta, p, w, True)
+    assert rel_err(R, Ro) < 1e-10
+    base = [m.alpha, m.beta, m.rho, m.thickness]
+    for k, l in [(0, 1), (1, 20), (2, 50), (3, 60), (0, 97), (1, 99), (2, 100), (3, 99)]:
+        arrs = [b.copy() for b in base]
+        d = 1e-6 * arrs[k][l]
+        arrs[k][l] += d
+        Rp = O.reflectivity(*arrs, m.Q_alpha, m.Q_beta, p, w, True)
+        arrs[k][l] -= 2 * d
+        Rm = O.reflectivity(*arrs, m.Q_alpha, m.Q_beta, p, w, True)
+        fd = (Rp - Rm) / (2 * d)
+        assert rel_err(J[:, k * L + l], fd) < 1e-6, (k, l, rel_err(J[:, k * L + l], fd))
+
+
 def test_adjoint_vs_fd_all_parameters(emu_jac):
     """Every layer parameter incl. the ocean's alpha, rho, h, damped frequencies, free surface."""
     from seismicinversion_b200.earth_models import random_layered_model
