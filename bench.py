@@ -315,6 +315,7 @@ def bench_serving(torch, dev, rates=(100, 1000, 3000, 10000, 20000), duration=1.
             t_start = time.perf_counter()
             t_next = t_start
             reqs = []
+            consumed = 0  # the client consumes results in arrival order, releasing them
             for k in range(n):
                 t_next += gaps[k]
                 dt = t_next - time.perf_counter()
@@ -322,8 +323,12 @@ def bench_serving(torch, dev, rates=(100, 1000, 3000, 10000, 20000), duration=1.
                     time.sleep(dt)  # releases the GIL to the scheduler thread
                 m, p_t, w_t, g, obs = pool[k % len(pool)]
                 reqs.append(srv.submit(m, p_t, w_t, gradient=g, R_obs=obs))
+                while consumed < len(reqs) and reqs[consumed].done.is_set():
+                    reqs[consumed].result = None
+                    consumed += 1
             for r in reqs:
                 r.wait(120)
+                r.result = None
             stats = srv.stats(since=t_start)
         out[f"rate_{lam}"] = {k: stats[k] for k in ("completed", "throughput_rps", "p50_ms",
                                                      "p99_ms", "batches", "mean_queue_ms",

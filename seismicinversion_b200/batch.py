@@ -58,14 +58,27 @@ def _flat(x, dtype) -> torch.Tensor:
     return torch.as_tensor(np.ascontiguousarray(x)).to(dtype).reshape(-1)
 
 
-def _cat(parts, dtype, dev) -> torch.Tensor:
-    """Concatenate on the device (host parts are copied once, device parts stay put)."""
+def _cat_into(out: torch.Tensor, parts):
+    """Concatenate 1-D parts into the device view ``out`` (one kernel for device parts).
+    Returns the pinned host staging tensor when some part lives on the host (the caller
+    keeps it until the stream-ordered copy has run), else None."""
     if not parts:
-        return torch.zeros(1, dtype=dtype, device=dev)
-    host = [t for t in parts if not t.is_cuda]
-    if len(host) == len(parts):
-        return torch.cat(parts).to(dev, non_blocking=False)
-    return torch.cat([t.to(dev) for t in parts])
+        return None
+    n = sum(t.numel() for t in parts)
+    if all(t.is_cuda for t in parts):
+        torch.cat([t.to(out.dtype) for t in parts], out=out[:n])
+        return None
+    host = torch.cat([t.cpu().to(out.dtype) for t in parts]).pin_memory()
+    out[:n].copy_(host, non_blocking=True)
+    return host
+
+
+def _size_class(nbytes: int) -> int:
+    """Allocation size for a batch block: eight classes per power of two (<= 12.5 % slack),
+    at least 1 MiB, so that batches of similar size reuse the same cached blocks."""
+    nbytes = max(int(nbytes), 1 << 20)
+    step = 1 << max(0, (nbytes - 1).bit_length() - 3)
+    return (nbytes + step - 1) // step * step
 
 
 class ModelBatch:
@@ -131,17 +144,37 @@ class ModelBatch:
                 go += 4 * L + 1
             self.max_layers = max(self.max_layers, L)
         self.desc = desc
-        dev = self.dev
-        self.layers = torch.as_tensor(np.concatenate(tabs) if tabs else np.zeros(1), device=dev)
-        self.p = _cat(ps, torch.float64, dev)
-        self.omega = _cat(ws, torch.complex128, dev)
-        self.R_obs = _cat(obs, torch.complex128, dev) if obs else None
-        self.R = torch.empty(max(ro, 1), dtype=torch.complex128, device=dev)
-        self.chi_grad = torch.zeros(max(go, 1), dtype=torch.float64, device=dev)
         self.graph = None
         self.schedule = None
         self.plan = None
-        self.set_schedule(schedule or (128, 256))
+        schedule = tuple(schedule or (128, 256))
+        plan_bytes = self._plan_bytes(schedule)
+        # One device block per batch holds every buffer (layers, grids, R_obs, R, chi_grad,
+        # plan), its size rounded up to a size class: a stream of batches of varying shape
+        # then reuses cached blocks of a few classes instead of calling cudaMalloc (slow, and
+        # able to stall the host for tens of ms) for each of several buffers per batch.
+        sizes = [8 * max(lo, 1), 8 * max(po, 1), 16 * max(wo, 1), 16 * max(oo, 1),
+                 16 * max(ro, 1), 8 * max(go, 1), plan_bytes]
+        offs, total = [], 0
+        for n_b in sizes:
+            offs.append(total)
+            total += (n_b + 255) // 256 * 256
+        block = torch.empty(_size_class(total), dtype=torch.uint8, device=self.dev)
+        view = [block[o:o + n_b] for o, n_b in zip(offs, sizes)]
+        self.layers = view[0].view(torch.float64)
+        staged = torch.from_numpy(np.concatenate(tabs) if tabs else np.zeros(1)).pin_memory()
+        self.layers.copy_(staged, non_blocking=True)
+        self.p = view[1].view(torch.float64)
+        self.omega = view[2].view(torch.complex128)
+        self.R_obs = view[3].view(torch.complex128) if obs else None
+        # pinned sources stay referenced until their stream-ordered copies have run
+        self._staged = [staged, _cat_into(self.p, ps), _cat_into(self.omega, ws),
+                        _cat_into(self.R_obs, obs) if obs else None]
+        self.R = view[4].view(torch.complex128)
+        self.chi_grad = view[5].view(torch.float64)
+        self.chi_grad.zero_()
+        self._block = block
+        self.set_schedule(schedule, plan=view[6])
 
     @classmethod
     def from_tables(cls, tables: np.ndarray, p, omega, free_surface: bool = False,
@@ -183,20 +216,27 @@ class ModelBatch:
     def _cfg(self, schedule):
         return _lib.BatchConfig(int(schedule[0]), int(schedule[1]), 0, 0)
 
-    def set_schedule(self, schedule: tuple[int, int]) -> None:
+    def _plan_bytes(self, schedule) -> int:
+        h = _lib.lib()
+        cfg = self._cfg(schedule)
+        nbytes = h.kr_batch_plan_bytes(self.desc.ctypes.data, len(self.desc), ctypes.byref(cfg))
+        if nbytes == 0:
+            raise ValueError(f"invalid batch or schedule {schedule}")
+        return int(nbytes)
+
+    def set_schedule(self, schedule: tuple[int, int], plan: torch.Tensor | None = None) -> None:
         """(Re)plan the batch for a schedule (threads, frequencies per item)."""
         h = _lib.lib()
         cfg = self._cfg(schedule)
         n = len(self.desc)
-        nbytes = h.kr_batch_plan_bytes(self.desc.ctypes.data, n, ctypes.byref(cfg))
-        if nbytes == 0:
-            raise ValueError(f"invalid batch or schedule {schedule}")
+        nbytes = self._plan_bytes(schedule)
         meta = h.kr_batch_plan_meta_bytes(self.desc.ctypes.data, n, ctypes.byref(cfg))
         image = torch.empty(meta, dtype=torch.uint8, pin_memory=True)
         st = h.kr_batch_plan_host(self.desc.ctypes.data, n, ctypes.byref(cfg), image.data_ptr(),
                                   meta)
         _lib.check(st, "kr_batch_plan_host")
-        plan = torch.empty(nbytes, dtype=torch.uint8, device=self.dev)
+        if plan is None or plan.numel() < nbytes:
+            plan = torch.empty(nbytes, dtype=torch.uint8, device=self.dev)
         plan[:meta].copy_(image, non_blocking=True)  # stream-ordered before any launch
         self._plan_image = image  # keep the pinned source alive until the copy has run
         self.plan, self.schedule, self._cfg_obj, self.graph = plan, tuple(schedule), cfg, None
