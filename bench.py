@@ -28,6 +28,7 @@ import statistics
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 from pathlib import Path
 
@@ -120,6 +121,63 @@ class Clocks:
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
                 "samples": len(sm)}
+
+
+class NvmlClocks:
+    """NVML sampler (every 5 ms, read-only queries) running during the timed region; the
+    timed region of a step is tens of ms, too short for nvidia-smi's 200 ms interval."""
+
+    NAMES = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+             "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+             "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+             "sw_power_cap": "nvmlClocksEventReasonSwPowerCap"}
+
+    def __init__(self, handle, nvml):
+        self.h, self.nvml = handle, nvml
+        self.samples, self.stop_flag, self.thread = [], threading.Event(), None
+
+    @classmethod
+    def open(cls, torch, dev):
+        import pynvml
+
+        pynvml.nvmlInit()
+        props = torch.cuda.get_device_properties(dev)
+        bus = f"{props.pci_domain_id:08X}:{props.pci_bus_id:02X}:{props.pci_device_id:02X}.0"
+        return cls(pynvml.nvmlDeviceGetHandleByPciBusId(bus), pynvml)
+
+    def _run(self):
+        n = self.nvml
+        while not self.stop_flag.is_set():
+            try:
+                sm = n.nvmlDeviceGetClockInfo(self.h, n.NVML_CLOCK_SM)
+                mx = n.nvmlDeviceGetMaxClockInfo(self.h, n.NVML_CLOCK_SM)
+                rs = n.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.samples.append((sm, mx, rs))
+            except Exception:
+                pass
+            self.stop_flag.wait(0.005)
+
+    def start(self):
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
+
+    def stop(self):
+        self.stop_flag.set()
+        self.thread.join(5)
+        sm = [x[0] for x in self.samples]
+        reasons = sorted(k for k, attr in self.NAMES.items()
+                         if any(x[2] & getattr(self.nvml, attr) for x in self.samples))
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(x[1] for x in self.samples) if sm else None,
+                "reasons": reasons, "samples": len(sm), "sampler": "nvml 5 ms"}
+
+
+def clock_sampler(torch, dev, index):
+    """NVML sampler when pynvml can open the device, else nvidia-smi."""
+    try:
+        return NvmlClocks.open(torch, dev)
+    except Exception:
+        return Clocks(index)
 
 
 def fp64_peak(torch, dev):
@@ -297,15 +355,27 @@ def bench_serving(torch, dev, rates=(100, 1000, 3000, 10000, 20000), duration=1.
         pool.append((m, p_t, w_t, b % 2 == 1, obs))
     torch.cuda.synchronize()
     rng = np.random.default_rng(7)
+    rng_w = np.random.default_rng(8)
     out = {"workload": "Poisson stream, uneven models as the batching workload, 50/50 fwd/grad"}
-    # warm-up: kernel modules, streams, allocator segments, pinned staging buffers
+    # warm-up (untimed): kernel modules, streams, allocator blocks of the batch size classes,
+    # pinned staging buffers: the whole pool at once, then a short stream at a high rate
     with KennettServer(hbm_budget_bytes=120 * 10**9, max_batch_requests=64, max_inflight=2,
                        prewarm_bytes=4 << 30) as srv:
-        for k in range(len(pool)):
-            m, p_t, w_t, g, obs = pool[k]
-            srv.submit(m, p_t, w_t, gradient=g, R_obs=obs)
-        for r in list(srv.completed):
-            pass
+        warm = [srv.submit(m, p_t, w_t, gradient=g, R_obs=obs) for m, p_t, w_t, g, obs in pool]
+        for r in warm:
+            r.wait(120)
+        warm = []
+        t_next = time.perf_counter()
+        for k in range(1500):
+            t_next += rng_w.exponential(1.0 / 5000)
+            dt = t_next - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            m, p_t, w_t, g, obs = pool[k % len(pool)]
+            warm.append(srv.submit(m, p_t, w_t, gradient=g, R_obs=obs))
+        for r in warm:
+            r.wait(120)
+        del warm
     torch.cuda.synchronize()
     for lam in rates:
         n = int(min(max_requests, lam * duration))
@@ -411,7 +481,7 @@ def run_sharded(args, rank, world, local):
     torch.cuda.synchronize()
     dist.barrier()
     torch.cuda.synchronize()
-    clk = Clocks(local)
+    clk = clock_sampler(torch, dev, local)
     clk.start()
     evs = []
     for _ in range(args.steps):
@@ -532,7 +602,7 @@ def run_ours(args, rank, world, local):
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    clk = Clocks(local)
+    clk = clock_sampler(torch, dev, local)
     clk.start()
     evs = []
     for _ in range(args.steps):
