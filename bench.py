@@ -210,6 +210,31 @@ def _events(torch, st, fn, reps):
     return a.elapsed_time(b) / reps
 
 
+def bench_gmm(torch, D, tab, p_t, w_t, R_kennett, reps):
+    """Global Matrix Method forward (kr_gmm_reflectivity) on the gather's R grid: time per
+    launch and agreement with the Kennett grid of the timed step (slownesses <= 1.0 s/km)."""
+    n_p, n_w = R_kennett.shape
+    Rg = torch.empty_like(R_kennett)
+    D.gmm_reflectivity(tab, p_t, w_t, True, out=Rg)
+    torch.cuda.synchronize()
+    evs = []
+    for _ in range(reps):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        e[0].record()
+        D.gmm_reflectivity(tab, p_t, w_t, True, out=Rg)
+        e[1].record()
+        evs.append(e)
+    torch.cuda.synchronize()
+    ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+    sel = p_t <= 1.0
+    diff = float(((Rg[sel] - R_kennett[sel]).abs().amax(1) / R_kennett[sel].abs().amax(1)).max())
+    L = tab.shape[1]
+    upd = n_p * n_w * (L - 2)
+    return {"workload": "21-layer gather grid, 8192 p x 2047 damped omega, free surface",
+            "ms": ms, "interface_updates_per_s": upd / (ms * 1e-3),
+            "max_rel_diff_vs_kennett_p_le_1": diff}
+
+
 def bench_inversion(torch, dev, reps):
     """tau-p inversion workload: 21-layer model (79 packed parameters), 64 slownesses on
     [0.05, 0.6], omega_k = k 2pi/64 (k = 1..1024), start = true * exp(0.1 N(0,1)) (seed 2)."""
@@ -695,6 +720,7 @@ def run_ours(args, rank, world, local):
 
     extra = {}
     if world == 1 and not args.no_extra:
+        extra["gmm"] = bench_gmm(torch, D, tab, p_t, w_t, R, max(args.steps, 3))
         extra["inversion"] = bench_inversion(torch, dev, max(args.steps, 3))
         extra["batched"] = bench_batched(torch, dev, max(args.steps, 2))
         extra["serving"] = bench_serving(torch, dev)

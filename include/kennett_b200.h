@@ -72,6 +72,18 @@ kr_status kr_reflectivity(const double* layers, int32_t n_layers, const double* 
                           const double* omega, int32_t n_w, uint32_t flags, double* R,
                           void* stream);
 
+/*
+ * The same R(p, omega) by the Global Matrix Method with the block-Riccati sweep, an
+ * independent FP64 evaluation of the reflectivity.  Replaces gmm_reflectivity
+ * (GlobalMatrix/global_matrix.py:297-348) and the forward of gmm_reflectivity_torch
+ * (GlobalMatrix/gmm_torch.py:229-305, riccati_solver.py:200-330).  Arguments and errors as
+ * kr_reflectivity; with KR_FREE_SURFACE the result is R / (1 + R).  One thread per
+ * (omega, p); per interface a 4x4 complex solve with partial pivoting.
+ */
+kr_status kr_gmm_reflectivity(const double* layers, int32_t n_layers, const double* p,
+                              int32_t n_p, const double* omega, int32_t n_w, uint32_t flags,
+                              double* R, void* stream);
+
 /* Bytes of device workspace kr_jacobian needs. */
 size_t kr_jacobian_workspace_bytes(int32_t n_layers, int32_t n_p, int32_t n_w);
 
@@ -79,9 +91,9 @@ size_t kr_jacobian_workspace_bytes(int32_t n_layers, int32_t n_p, int32_t n_w);
  * Reflectivity and its Jacobian with respect to every layer's alpha, beta, rho, h.
  * Replaces the autograd graph of kennett_reflectivity_torch
  * (Kennett_Reflectivity/kennett_torch.py:312-480) and jacobian (kennett_torch.py:611-641,
- * jacrev of Re and Im).  Hand-written adjoint: one reverse sweep per (omega, p), states
- * recomputed from sqrt(I) checkpoints; interface-coefficient tangents by forward-mode dual
- * numbers once per (p, interface).
+ * jacrev of Re and Im).  Hand-written adjoint: one reverse sweep per (omega, p) over a
+ * tape of up to 64 steps (deeper models checkpoint and recompute segments); interface-
+ * coefficient tangents by forward-mode dual numbers once per (p, interface).
  *   layers, p, omega, flags : as kr_reflectivity
  *   R : device complex [n_p][n_w] output, or NULL
  *   J : device complex [n_p][4*n_layers][n_w] output, J[j][k*L + l][w] = dR(p_j, w)/d theta,

@@ -32,6 +32,10 @@ _LAZY = {
     "compute_taup_traces": ".taup_inversion",
     "invert_taup": ".taup_inversion",
     "taup_misfit_grad_hessian": ".taup_inversion",
+    "gmm_reflectivity": ".global_matrix",
+    "gmm_reflectivity_torch": ".gmm_torch",
+    "gmm_jacobian": ".gmm_torch",
+    "gmm_hessian": ".gmm_torch",
 }
 
 __all__ = ["LayerModel", "complex_slowness", "vertical_slowness", "ricker_spectrum",

@@ -52,6 +52,7 @@ _SIGNATURES = {
     "kr_version": (_i32, []),
     "kr_validate_layers": (_i32, [_vp, _i32]),
     "kr_reflectivity": (_i32, [_vp, _i32, _vp, _i32, _vp, _i32, _u32, _vp, _vp]),
+    "kr_gmm_reflectivity": (_i32, [_vp, _i32, _vp, _i32, _vp, _i32, _u32, _vp, _vp]),
     "kr_jacobian_workspace_bytes": (_size_t, [_i32, _i32, _i32]),
     "kr_jacobian": (_i32, [_vp, _i32, _vp, _i32, _vp, _i32, _u32, _vp, _vp, _vp, _size_t, _vp]),
     "kr_misfit_gradient_workspace_bytes": (_size_t, [_i32, _i32, _i32]),

@@ -55,7 +55,7 @@ KR_HD cd cdot2(cd a, cd b, cd c, cd d) {
 KR_HD cd cmac2(cd s, cd a, cd b, cd c, cd d) { return cmac(cmac(s, c, d), a, b); }
 KR_HD double abs2(cd a) { return fma(a.x, a.x, a.y * a.y); }
 
-// 1/z via the conjugate over |z|^2, with a power-of-two prescale so that |z|^2 neither
+// 1/z via the conjugate over |z|^2, with a prescale by 1e-150 or 1e150 so that |z|^2 neither
 // overflows nor underflows for the magnitudes met here (down to ~1e-150).
 KR_HD cd recip(cd z) {
   double m = fmax(fabs(z.x), fabs(z.y));

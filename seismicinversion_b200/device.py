@@ -92,6 +92,25 @@ def reflectivity(layers: torch.Tensor, p, omega, free_surface: bool = False,
     return out
 
 
+def gmm_reflectivity(layers: torch.Tensor, p, omega, free_surface: bool = False,
+                     out: torch.Tensor | None = None) -> torch.Tensor:
+    """R[p, omega] by the Global Matrix Method (block-Riccati sweep): ``kr_gmm_reflectivity``."""
+    dev = layers.device
+    p_t = _dev_f64(p, dev).reshape(-1)
+    w_t = _dev_c128(omega, dev).reshape(-1)
+    n_p, n_w = p_t.numel(), w_t.numel()
+    if out is None:
+        out = torch.empty((n_p, n_w), dtype=torch.complex128, device=dev)
+    elif out.shape != (n_p, n_w) or out.dtype != torch.complex128 or not out.is_contiguous():
+        raise ValueError("out must be a contiguous complex128 tensor of shape (n_p, n_w)")
+    flags = _lib.KR_FREE_SURFACE if free_surface else 0
+    st = _lib.lib().kr_gmm_reflectivity(layers.data_ptr(), layers.shape[1], p_t.data_ptr(), n_p,
+                                        w_t.data_ptr(), n_w, flags, out.data_ptr(),
+                                        stream_handle(dev))
+    _lib.check(st, "kr_gmm_reflectivity")
+    return out
+
+
 def bessel_sum(R: torch.Tensor, p, pw, dp: float, omega_real, offsets,
                out: torch.Tensor | None = None) -> torch.Tensor:
     """U[r, w] = sum_j R[j, w] ((pw_j w) dp) J0((w p_j) r): ``kr_bessel_sum``."""

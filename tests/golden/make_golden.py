@@ -7,7 +7,7 @@ Run from the repository root with the reference checked out read-only::
 It imports ``Kennett_Reflectivity`` from that checkout and stores its outputs (NumPy
 reflectivity, batched reflectivity, seismogram, CPU gather, scattering matrices, torch
 forward, ``jacobian`` (jacrev), ``frechet_kennett``, ``hessian`` and a small ``invert_taup``
-run) as ``.npz`` files.  The fixtures are committed; tests and the GPU box never need the
+run, and the GlobalMatrix forward) as ``.npz`` files.  The fixtures are committed; tests and the GPU box never need the
 reference itself.  Models come from ``seismicinversion_b200.earth_models`` with fixed seeds.
 """
 
@@ -48,6 +48,43 @@ def training_data_golden(ref_root: str) -> None:
             out[f"{split}_log_params"] = data["log_params"].numpy()
             out[f"{split}_reflectivity"] = data["reflectivity"].numpy()
     np.savez_compressed(HERE / "training_data_small.npz", **out)
+
+
+def gmm_golden(ref_root: str) -> None:
+    """Reference GlobalMatrix forward (NumPy riccati and dense solvers, torch riccati)."""
+    sys.path.insert(0, ref_root)
+    import torch
+    from GlobalMatrix.global_matrix import gmm_reflectivity
+    from GlobalMatrix.gmm_torch import gmm_reflectivity_torch
+    from Kennett_Reflectivity.kennett_torch import model_to_tensors
+    from Kennett_Reflectivity.layer_model import LayerModel
+
+    from seismicinversion_b200.earth_models import default_ocean_crust_model, random_layered_model
+
+    def ref_model(m):
+        return LayerModel.from_arrays(m.alpha, m.beta, m.rho, m.thickness, m.Q_alpha, m.Q_beta)
+
+    out = {}
+    w255 = np.arange(1, 256, dtype=np.float64) * (2 * np.pi / 64.0)
+    cases = [("default", default_ocean_crust_model(), np.array([0.1, 0.3, 0.6, 1.0]), w255),
+             ("two", random_layered_model(1, seed=3), np.array([0.1, 0.5]), w255),
+             ("three", random_layered_model(2, seed=4), np.array([0.2, 0.7]), w255),
+             ("c1", random_layered_model(20, seed=1), np.array([0.05, 0.3, 0.7, 1.1]),
+              np.arange(1, 2048, dtype=np.float64) * (2 * np.pi / 64.0) + 1j * np.pi / 64.0)]
+    for tag, m, ps, w in cases:
+        out.update({f"{tag}_{k}": v for k, v in _model_arrays(m).items()})
+        out[f"{tag}_p"], out[f"{tag}_omega"] = ps, w
+        for fs in (False, True):
+            out[f"{tag}_R_fs{int(fs)}"] = np.stack(
+                [gmm_reflectivity(ref_model(m), p, w, free_surface=fs) for p in ps])
+        out[f"{tag}_Rdense_fs0"] = np.stack(
+            [gmm_reflectivity(ref_model(m), p, w, solver="dense") for p in ps[:2]])
+    m2 = random_layered_model(20, seed=2)
+    t2 = model_to_tensors(m2)
+    om64 = torch.arange(1, 65, dtype=torch.float64) * (2 * np.pi / 64.0)
+    out["c2_torch_R_p0.3"] = gmm_reflectivity_torch(**t2, p=0.3, omega=om64).detach().numpy()
+    out["c2_torch_omega"] = om64.numpy()
+    np.savez_compressed(HERE / "gmm_reflectivity.npz", **out)
 
 
 def main(ref_root: str) -> None:
@@ -205,6 +242,9 @@ if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     if "--training-data-only" in sys.argv:
         training_data_golden(root)
+    elif "--gmm-only" in sys.argv:
+        gmm_golden(root)
     else:
         main(root)
         training_data_golden(root)
+        gmm_golden(root)

@@ -102,3 +102,20 @@ def test_oracle_fd_vs_jacrev(golden):
             J = O.fd_jacobian(m.alpha, m.beta, m.rho, th, m.Q_alpha, m.Q_beta, p, g["omega"],
                               free_surface=bool(fs))[0]
             assert rel_err(J, g[f"J_p{p}_fs{fs}"]) < 1e-5
+
+
+@pytest.mark.parametrize("tag", ["default", "two", "three", "c1"])
+def test_gmm_oracle_vs_reference(golden, tag):
+    """GMM oracle (block-Riccati restatement) against the reference's gmm_reflectivity, and
+    the reference's dense and Riccati solvers against each other."""
+    from oracle import gmm_oracle
+
+    g = golden("gmm_reflectivity.npz")
+    m = [g[f"{tag}_{k}"] for k in ("alpha", "beta", "rho", "thickness", "Q_alpha", "Q_beta")]
+    for fs in (0, 1):
+        R = gmm_oracle.gmm_reflectivity(*m, g[f"{tag}_p"], g[f"{tag}_omega"], bool(fs))
+        assert rel_err(R, g[f"{tag}_R_fs{fs}"]) < 1e-10, (tag, fs)
+    assert rel_err(g[f"{tag}_Rdense_fs0"], g[f"{tag}_R_fs0"][:2]) < 1e-10
+    # the two methods compute one reflectivity
+    Rk = O.reflectivity(*m, g[f"{tag}_p"], g[f"{tag}_omega"], False)
+    assert rel_err(g[f"{tag}_R_fs0"], Rk) < 1e-9
