@@ -280,6 +280,35 @@ def bench_inversion(torch, dev, reps):
                              "s_per_iteration": dt / max(res.n_iterations, 1),
                              "param_err_first_last": [res.param_error_history[0],
                                                       res.param_error_history[-1]]}
+    # K concurrent inversions (true models seeds 2..2+K-1, lognormal starts), LM state on
+    # the device: one batched gradient (+ exact-Hessian) launch and one batched trial launch
+    # per round for all K
+    from seismicinversion_b200.taup_batch import invert_taup_batch
+
+    K = 16
+    trues, inits = [], []
+    for k in range(K):
+        tm = random_layered_model(20, seed=2 + k)
+        r = np.random.default_rng(2 + k)
+        x0 = np.concatenate([tm.alpha[1:], tm.beta[1:], tm.rho[1:], tm.thickness[1:-1]])
+        x0 = x0 * np.exp(0.1 * r.standard_normal(len(x0)))
+        trues.append(tm)
+        inits.append(x0)
+    for hess in ("gauss-newton", "exact"):
+        its = 5 if hess == "gauss-newton" else 2
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = invert_taup_batch(trues, list(p), nfreq=1024, max_iter=its, hessian=hess,
+                                initial_params=inits, tol=0.0)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        n_it = sum(x.n_iterations for x in res)
+        seq = out[f"lm_{hess}"]["s_per_iteration"]
+        out[f"lm_batch16_{hess}"] = {
+            "inversions": K, "iterations_each": its, "seconds": dt,
+            "s_per_round_all_inversions": dt / its,
+            "inversion_iterations_per_s": n_it / dt,
+            "speedup_vs_sequential_invert_taup": (n_it * seq) / dt}
     return out
 
 

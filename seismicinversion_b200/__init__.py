@@ -32,6 +32,7 @@ _LAZY = {
     "compute_taup_traces": ".taup_inversion",
     "invert_taup": ".taup_inversion",
     "taup_misfit_grad_hessian": ".taup_inversion",
+    "invert_taup_batch": ".taup_batch",
     "gmm_reflectivity": ".global_matrix",
     "gmm_reflectivity_torch": ".gmm_torch",
     "gmm_jacobian": ".gmm_torch",

@@ -279,3 +279,35 @@ def test_invert_taup_gauss_newton_converges():
     res = invert_taup(default_ocean_crust_model(), [0.1, 0.2, 0.3, 0.4], nfreq=32,
                       perturbation=0.02, max_iter=20, hessian="gauss-newton")
     assert res.converged and res.param_error_history[-1] < 1e-6
+
+
+@pytest.mark.parametrize("hessian", ["gauss-newton", "exact"])
+def test_invert_taup_batch_matches_sequential(hessian):
+    """K concurrent inversions with the LM state on the device follow the sequential
+    invert_taup trajectories (same starts, same rules; gradients agree to ~1e-12, so the
+    histories agree closely) and converge alike."""
+    from seismicinversion_b200.earth_models import default_ocean_crust_model, random_layered_model
+    from seismicinversion_b200.taup_batch import invert_taup_batch
+    from seismicinversion_b200.taup_inversion import invert_taup
+
+    models = [default_ocean_crust_model(), random_layered_model(4, seed=12),
+              random_layered_model(4, seed=13)]
+    ps = [0.1, 0.2, 0.3, 0.4]
+    seeds = [42, 7, 8]
+    res = invert_taup_batch(models, ps, nfreq=32, perturbation=0.03, max_iter=25, seeds=seeds,
+                            hessian=hessian)
+    for k, m in enumerate(models):
+        ref = invert_taup(m, ps, nfreq=32, perturbation=0.03, max_iter=25, seed=seeds[k],
+                          hessian=hessian)
+        r = res[k]
+        assert np.allclose(r.initial_model.alpha, ref.initial_model.alpha, rtol=1e-15)
+        n = min(4, r.n_iterations, ref.n_iterations)
+        for i in range(n):
+            assert abs(r.misfit_history[i] - ref.misfit_history[i]) <= \
+                1e-6 * ref.misfit_history[0], (k, i)
+        # same outcome: converged alike, final errors alike, the same recovered model
+        assert r.converged == ref.converged
+        assert abs(r.param_error_history[-1] - ref.param_error_history[-1]) <= \
+            0.05 * ref.param_error_history[0] + 1e-6, (k, r.param_error_history[-1],
+                                                        ref.param_error_history[-1])
+        assert np.allclose(r.recovered_model.alpha, ref.recovered_model.alpha, rtol=1e-3)
