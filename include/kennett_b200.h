@@ -218,7 +218,8 @@ typedef struct {
   int64_t grad_off;
 } kr_model_desc;
 
-/* Schedule of a batch: threads per block (64 or 128) and frequencies per work item. */
+/* Schedule of a batch: threads per block (32: one warp per work item; 64 or 128) and
+ * frequencies per work item. */
 typedef struct {
   int32_t threads;
   int32_t tile_w;

@@ -317,7 +317,8 @@ static int occupancy_grid(const void* fn, int threads, size_t smem) {
 }
 
 static bool valid_config(const kr_batch_config* c) {
-  return c && (c->threads == 64 || c->threads == 128) && c->tile_w >= 32 && c->tile_w <= 8192;
+  return c && (c->threads == 32 || c->threads == 64 || c->threads == 128) && c->tile_w >= 32 &&
+         c->tile_w <= 8192;
 }
 
 struct PlanLayout {
@@ -535,22 +536,22 @@ extern "C" kr_status kr_batch_plan(const kr_model_desc* descs, int32_t n_models,
   return KR_OK;
 }
 
-extern "C" kr_status kr_batch_launch(void* plan, const kr_batch_config* cfg, int32_t max_layers,
-                                     const double* layers, const double* p, const double* omega,
-                                     const double* R_obs, double* R, double* chi_grad,
-                                     void* stream) {
-  if (!plan || !valid_config(cfg) || !layers || !p || !omega) return KR_ERR_INVALID_ARGUMENT;
-  if (max_layers < 2 || max_layers > kMaxLayers) return KR_ERR_INVALID_ARGUMENT;
-  cudaStream_t st = (cudaStream_t)stream;
-  unsigned char* pl = static_cast<unsigned char*>(plan);
+namespace kr {
+
+// One batch launch for a block size of THREADS (32: one warp per work item, i.e. per
+// (model, slowness) pair and frequency range; 64 / 128: two / four warps per item).
+template <int THREADS>
+static kr_status launch_batch(unsigned char* pl, const kr_batch_config* cfg, int max_layers,
+                              const double* layers, const double* p, const double* omega,
+                              const double* R_obs, double* R, double* chi_grad,
+                              cudaStream_t st) {
   // Grid sizes from an occupancy query (host-side, capture-safe).
   PlanHeader h{};
   size_t fsm = 0, gsm = 0;
   int stage = 0;
   const int tab = fwd_table_entries(cfg->tile_w);
   int gtab = 0;
-  kr_status s = (cfg->threads == 64) ? grids<64>(h, max_layers, tab, &fsm, &gsm, &stage, &gtab)
-                                     : grids<128>(h, max_layers, tab, &fsm, &gsm, &stage, &gtab);
+  kr_status s = grids<THREADS>(h, max_layers, tab, &fsm, &gsm, &stage, &gtab);
   if (s != KR_OK) {
     set_last_error_msg("kr_batch_launch: shared-memory attribute");
     return s;
@@ -562,20 +563,32 @@ extern "C" kr_status kr_batch_launch(void* plan, const kr_batch_config* cfg, int
   s = check_launch("kr_batch_launch: prep");
   if (s != KR_OK) return s;
   const double2* w = reinterpret_cast<const double2*>(omega);
-  if (cfg->threads == 64) {
-    batch_forward_kernel<64><<<h.grid_fwd, 64, fsm, st>>>(pl, w, reinterpret_cast<double2*>(R), tab);
-    s = check_launch("kr_batch_launch: forward");
-    if (s != KR_OK) return s;
-    batch_gradient_kernel<64><<<h.grid_grad, 64, gsm, st>>>(
-        pl, w, reinterpret_cast<const double2*>(R_obs), reinterpret_cast<double2*>(R), chi_grad,
-        stage, gtab);
-  } else {
-    batch_forward_kernel<128><<<h.grid_fwd, 128, fsm, st>>>(pl, w, reinterpret_cast<double2*>(R), tab);
-    s = check_launch("kr_batch_launch: forward");
-    if (s != KR_OK) return s;
-    batch_gradient_kernel<128><<<h.grid_grad, 128, gsm, st>>>(
-        pl, w, reinterpret_cast<const double2*>(R_obs), reinterpret_cast<double2*>(R), chi_grad,
-        stage, gtab);
-  }
+  batch_forward_kernel<THREADS><<<h.grid_fwd, THREADS, fsm, st>>>(
+      pl, w, reinterpret_cast<double2*>(R), tab);
+  s = check_launch("kr_batch_launch: forward");
+  if (s != KR_OK) return s;
+  batch_gradient_kernel<THREADS><<<h.grid_grad, THREADS, gsm, st>>>(
+      pl, w, reinterpret_cast<const double2*>(R_obs), reinterpret_cast<double2*>(R), chi_grad,
+      stage, gtab);
   return check_launch("kr_batch_launch: gradient");
+}
+
+}  // namespace kr
+
+extern "C" kr_status kr_batch_launch(void* plan, const kr_batch_config* cfg, int32_t max_layers,
+                                     const double* layers, const double* p, const double* omega,
+                                     const double* R_obs, double* R, double* chi_grad,
+                                     void* stream) {
+  if (!plan || !valid_config(cfg) || !layers || !p || !omega) return KR_ERR_INVALID_ARGUMENT;
+  if (max_layers < 2 || max_layers > kMaxLayers) return KR_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  unsigned char* pl = static_cast<unsigned char*>(plan);
+  switch (cfg->threads) {
+    case 32:
+      return launch_batch<32>(pl, cfg, max_layers, layers, p, omega, R_obs, R, chi_grad, st);
+    case 64:
+      return launch_batch<64>(pl, cfg, max_layers, layers, p, omega, R_obs, R, chi_grad, st);
+    default:
+      return launch_batch<128>(pl, cfg, max_layers, layers, p, omega, R_obs, R, chi_grad, st);
+  }
 }

@@ -59,7 +59,7 @@ def _check(batch, items):
             assert rel_err(g.cpu().numpy(), out[:4 * L].cpu().numpy()) < 1e-12, b
 
 
-@pytest.mark.parametrize("schedule", [(64, 64), (128, 256), (128, 512)])
+@pytest.mark.parametrize("schedule", [(32, 64), (32, 100), (64, 64), (128, 256), (128, 512)])
 def test_batch_matches_single_calls(schedule):
     from seismicinversion_b200.batch import ModelBatch
 
