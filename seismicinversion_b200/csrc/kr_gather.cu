@@ -101,43 +101,66 @@ constexpr int kRotSteps = 32;
 // Slownesses staged per shared-memory chunk: (p_j, pw_j dp) and (1 / p_j, pw_j dp / sqrt p_j).
 constexpr int kChunk = 256;
 
-// Terms of one fast chunk for one thread: exact cos / sin anchor every kRotSteps, rotation
-// of (u, v) = (cos + sin, cos - sin) in between.  The amplitude 1 / sqrt(pi omega r) is
-// common to the thread and applied to (ax, ay) by the caller; 1 / sqrt(p_j) is staged.
+// R rows are staged through shared memory in tiles of kSub slownesses x 32 frequencies
+// (16 KB), double-buffered with cp.async: the 8 offset warps of a block read each R element
+// from shared memory instead of each loading it from L1 / L2, and the next tile is in flight
+// while the current one is summed.  kSub equals the rotation anchor spacing.
+constexpr int kSub = kRotSteps;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(gmem),
+               "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+
+// Block-cooperative: R rows [j0, j0 + ns) x frequencies [iw0, iw0 + 32) into `tile`,
+// zero-filled (no global read) outside the grid.
+__device__ __forceinline__ void stage_R(double2 (*tile)[kBsW], const double2* __restrict__ R,
+                                        int j0, int ns, int iw0, int n_w, int tid) {
+  for (int e = tid; e < kSub * kBsW; e += kBsW * kBsR) {
+    const int row = e / kBsW, col = e - row * kBsW;
+    const bool ok = row < ns && iw0 + col < n_w;
+    const double2* src = ok ? R + (size_t)(j0 + row) * n_w + iw0 + col : R;
+    cp_async16(&tile[row][col], src, ok ? 16 : 0);
+  }
+}
+
+// Terms of one staged tile for one thread on the fast path: exact cos / sin anchor at the
+// tile's first slowness, rotation of (u, v) = (cos + sin, cos - sin) in between.  The
+// amplitude 1 / sqrt(pi omega r) is common to the thread and applied to (ax, ay) by the
+// caller; 1 / sqrt(p_j) is staged.
 template <int NT>
-__device__ __forceinline__ void fast_chunk(const double2* s_pf, const double2* s_ig, int n,
-                                           double om, double r, double inv_omr, double cdl,
-                                           double sd, int n_w, const double2*& Rp, double& ax,
-                                           double& ay) {
-  double u, v;
-  for (int g = 0; g < n; g += kRotSteps) {
-    const int m = min(kRotSteps, n - g);
-    double s, c;
-    sincos((om * s_pf[g].x) * r, &s, &c);
-    u = c + s;
-    v = c - s;
+__device__ __forceinline__ void fast_tile(const double2* s_pf, const double2* s_ig,
+                                          const double2 (*tile)[kBsW], int k0, int m, int lane,
+                                          double om, double r, double inv_omr, double cdl,
+                                          double sd, double& ax, double& ay) {
+  double s, c;
+  sincos((om * s_pf[k0].x) * r, &s, &c);
+  double u = c + s, v = c - s;
 #pragma unroll 8
-    for (int k = g; k < g + m; ++k) {
-      const double2 ig = s_ig[k];
-      const double2 rv = __ldg(Rp);
-      Rp += n_w;
-      const double t = j0_asym_scaled<NT>(ig.x * inv_omr, u, v) * ig.y;
-      const double u2 = fma(u, cdl, v * sd);
-      v = fma(v, cdl, -u * sd);
-      u = u2;
-      ax = fma(t, rv.x, ax);
-      ay = fma(t, rv.y, ay);
-    }
+  for (int k = 0; k < m; ++k) {
+    const double2 ig = s_ig[k0 + k];
+    const double2 rv = tile[k][lane];
+    const double t = j0_asym_scaled<NT>(ig.x * inv_omr, u, v) * ig.y;
+    const double u2 = fma(u, cdl, v * sd);
+    v = fma(v, cdl, -u * sd);
+    u = u2;
+    ax = fma(t, rv.x, ax);
+    ay = fma(t, rv.y, ay);
   }
 }
 
 // One thread per (omega, offset) and slowness slice.  Grid: x = slowness slice, y = offset
 // group, z = frequency tile, so the hardware starts the low-frequency tiles (small J0
-// arguments, the slowest blocks) first and the cheap high-frequency tiles fill the tail.  Per chunk of the slice, the block
-// stages (p_j, pw_j dp) in shared memory and checks once whether the chunk continues the
-// slice's arithmetic progression (to 4.5 ulp); inside such a chunk cos / sin of
-// x_j = (omega p_j) r advance by one rotation per slowness, with an exact sincos anchor every
-// kRotSteps.  omega is factored out of the weight: U = omega * sum_j J0(x_j) (pw_j dp) R_j.
+// arguments, the slowest blocks) first and the cheap high-frequency tiles fill the tail.
+// Per chunk of the slice the block stages (p_j, pw_j dp) and (1 / p_j, pw_j dp / sqrt p_j)
+// in shared memory and checks once whether the chunk continues the slice's arithmetic
+// progression (to 4.5 ulp); inside such a chunk cos / sin of x_j = (omega p_j) r advance by
+// one rotation per slowness, with an exact sincos anchor every kRotSteps.  R arrives in
+// double-buffered tiles (stage_R).  omega is factored out of the weight:
+// U = omega * sum_j J0(x_j) (pw_j dp) R_j.
 __global__ void __launch_bounds__(kBsW * kBsR, 2)
 bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ p,
                       const double* __restrict__ pw, int n_p, double dp,
@@ -147,12 +170,15 @@ bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ 
   __shared__ double2 s_pf[kChunk];  // (p_j, pw_j dp)
   __shared__ double2 s_ig[kChunk];  // (1 / p_j, pw_j dp / sqrt(p_j))
   __shared__ double s_j0[kJ0TabIntervals * kJ0Row];
+  __shared__ __align__(16) double2 s_R[2][kSub][kBsW];
   const int tid = threadIdx.y * kBsW + threadIdx.x;
   for (int e = tid; e < kJ0TabIntervals * kJ0Row; e += kBsW * kBsR) {
     const int k = e / kJ0Row, n = e - k * kJ0Row;
     s_j0[e] = n <= kJ0TabDegree ? kJ0Taylor[k][n] : 0.0;  // made visible by the chunk barrier
   }
-  const int iw = blockIdx.z * kBsW + threadIdx.x;
+  const int lane = threadIdx.x;
+  const int iw0 = blockIdx.z * kBsW;
+  const int iw = iw0 + lane;
   const int ir = blockIdx.y * kBsR + threadIdx.y;
   const int j_begin = blockIdx.x * p_per_slice;
   const int j_end = min(n_p, j_begin + p_per_slice);
@@ -171,12 +197,11 @@ bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ 
   sincos(omr * step, &sd, &cdl);
   double c = 0.0, s = 0.0;
   int since = kRotSteps;  // steps since the last exact anchor (kRotSteps: none valid)
-  double ax = 0.0, ay = 0.0;  // fast-chunk terms, without the factor 1 / sqrt(pi omega r)
+  double ax = 0.0, ay = 0.0;  // fast-path terms, without the factor 1 / sqrt(pi omega r)
   double bx = 0.0, by = 0.0;  // other terms, complete
-  const double2* Rp = R + (size_t)j_begin * n_w + (active ? iw : 0);
   for (int jc = j_begin; jc < j_end; jc += kChunk) {
     const int n = min(kChunk, j_end - jc);
-    __syncthreads();
+    __syncthreads();  // the previous chunk's readers of s_pf, s_ig, s_R are done
     bool ok = true;
     if (tid < n) {
       const int j = jc + tid;
@@ -187,53 +212,65 @@ bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ 
       const double lin = fma((double)(j - j_begin), step, p0);
       ok = fabs(pj - lin) <= 1e-15 * fabs(pj);
     }
+    stage_R(s_R[0], R, jc, min(kSub, n), iw0, n_w, tid);
+    cp_async_commit();
     const bool uniform = __syncthreads_and(ok) != 0;
     if (!uniform) since = kRotSteps;
-    if (!active) continue;
     // Fast chunk: slownesses in arithmetic progression with x increasing from >= 25, so every
-    // term takes the asymptotic branch; anchor cos / sin exactly every kRotSteps terms and
-    // rotate in between (no data-dependent branches in the inner loop).  The number of
-    // expansion terms follows from the chunk's smallest argument.
+    // term takes the asymptotic branch with the anchor / rotation scheme (no data-dependent
+    // branches in the inner loop).  The number of expansion terms follows from the chunk's
+    // smallest argument.
     const double x_first = (om * s_pf[0].x) * r;
-    if (uniform && step > 0.0 && omr > 0.0 && x_first >= kJ0X0) {
-      if (x_first >= 3000.0)
-        fast_chunk<2>(s_pf, s_ig, n, om, r, inv_omr, cdl, sd, n_w, Rp, ax, ay);
-      else if (x_first >= 300.0)
-        fast_chunk<3>(s_pf, s_ig, n, om, r, inv_omr, cdl, sd, n_w, Rp, ax, ay);
-      else if (x_first >= 100.0)
-        fast_chunk<4>(s_pf, s_ig, n, om, r, inv_omr, cdl, sd, n_w, Rp, ax, ay);
-      else if (x_first >= 60.0)
-        fast_chunk<5>(s_pf, s_ig, n, om, r, inv_omr, cdl, sd, n_w, Rp, ax, ay);
-      else
-        fast_chunk<7>(s_pf, s_ig, n, om, r, inv_omr, cdl, sd, n_w, Rp, ax, ay);
-      since = kRotSteps;
-      continue;
-    }
-#pragma unroll 4
-    for (int k = 0; k < n; ++k) {
-      const double2 pf = s_pf[k];
-      const double2 rv = __ldg(Rp);
-      Rp += n_w;
-      const double x = (om * pf.x) * r;
-      double jv;
-      if (x < kJ0X0) {
-        jv = x > -kJ0X0 ? j0_table(s_j0, fabs(x)) : j0(x);
-        since = kRotSteps;
-      } else {
-        if (since < kRotSteps) {
-          const double c2 = fma(c, cdl, -s * sd);
-          s = fma(s, cdl, c * sd);
-          c = c2;
-          ++since;
-        } else {
-          sincos(x, &s, &c);
-          since = uniform ? 1 : kRotSteps;
+    const bool fast = active && uniform && step > 0.0 && omr > 0.0 && x_first >= kJ0X0;
+    const int nt = x_first >= 3000.0 ? 2 : x_first >= 300.0 ? 3 : x_first >= 100.0 ? 4
+                 : x_first >= 60.0 ? 5 : 7;
+    if (fast) since = kRotSteps;
+    const int nsub = (n + kSub - 1) / kSub;
+    for (int sb = 0; sb < nsub; ++sb) {
+      if (sb + 1 < nsub)
+        stage_R(s_R[(sb + 1) & 1], R, jc + (sb + 1) * kSub, min(kSub, n - (sb + 1) * kSub), iw0,
+                n_w, tid);
+      cp_async_commit();
+      cp_async_wait_1();  // this thread's copies of tile sb have landed
+      __syncthreads();    // ... and every thread's
+      const double2(*tile)[kBsW] = s_R[sb & 1];
+      const int k0 = sb * kSub, m = min(kSub, n - k0);
+      if (fast) {
+        switch (nt) {
+          case 2: fast_tile<2>(s_pf, s_ig, tile, k0, m, lane, om, r, inv_omr, cdl, sd, ax, ay); break;
+          case 3: fast_tile<3>(s_pf, s_ig, tile, k0, m, lane, om, r, inv_omr, cdl, sd, ax, ay); break;
+          case 4: fast_tile<4>(s_pf, s_ig, tile, k0, m, lane, om, r, inv_omr, cdl, sd, ax, ay); break;
+          case 5: fast_tile<5>(s_pf, s_ig, tile, k0, m, lane, om, r, inv_omr, cdl, sd, ax, ay); break;
+          default: fast_tile<7>(s_pf, s_ig, tile, k0, m, lane, om, r, inv_omr, cdl, sd, ax, ay); break;
         }
-        jv = j0_asymptotic(x, c, s);
+      } else if (active) {
+#pragma unroll 4
+        for (int k = 0; k < m; ++k) {
+          const double2 pf = s_pf[k0 + k];
+          const double2 rv = tile[k][lane];
+          const double x = (om * pf.x) * r;
+          double jv;
+          if (x < kJ0X0) {
+            jv = x > -kJ0X0 ? j0_table(s_j0, fabs(x)) : j0(x);
+            since = kRotSteps;
+          } else {
+            if (since < kRotSteps) {
+              const double c2 = fma(c, cdl, -s * sd);
+              s = fma(s, cdl, c * sd);
+              c = c2;
+              ++since;
+            } else {
+              sincos(x, &s, &c);
+              since = uniform ? 1 : kRotSteps;
+            }
+            jv = j0_asymptotic(x, c, s);
+          }
+          const double t = jv * pf.y;
+          bx = fma(t, rv.x, bx);
+          by = fma(t, rv.y, by);
+        }
       }
-      const double t = jv * pf.y;
-      bx = fma(t, rv.x, bx);
-      by = fma(t, rv.y, by);
+      __syncthreads();  // tile sb is read before iteration sb + 1 refills its buffer
     }
   }
   if (active)
