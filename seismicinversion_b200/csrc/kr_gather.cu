@@ -116,14 +116,19 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::); }
 
 // Block-cooperative: R rows [j0, j0 + ns) x frequencies [iw0, iw0 + 32) into `tile`,
-// zero-filled (no global read) outside the grid.
+// zero-filled (no global read) outside the grid.  Warp ty copies rows ty, ty + 8, ...;
+// lane copies frequency iw0 + lane (one coalesced 512-byte row per warp and copy).
 __device__ __forceinline__ void stage_R(double2 (*tile)[kBsW], const double2* __restrict__ R,
-                                        int j0, int ns, int iw0, int n_w, int tid) {
-  for (int e = tid; e < kSub * kBsW; e += kBsW * kBsR) {
-    const int row = e / kBsW, col = e - row * kBsW;
-    const bool ok = row < ns && iw0 + col < n_w;
-    const double2* src = ok ? R + (size_t)(j0 + row) * n_w + iw0 + col : R;
-    cp_async16(&tile[row][col], src, ok ? 16 : 0);
+                                        int j0, int ns, int iw0, int n_w) {
+  const int ty = threadIdx.y, lane = threadIdx.x;
+  const bool col_ok = iw0 + lane < n_w;
+  const double2* src = R + (size_t)(j0 + ty) * n_w + iw0 + lane;
+  const size_t stride = (size_t)kBsR * n_w;
+#pragma unroll
+  for (int i = 0; i < kSub / kBsR; ++i) {
+    const int row = ty + i * kBsR;
+    const bool ok = col_ok && row < ns;
+    cp_async16(&tile[row][lane], ok ? src + i * stride : R, ok ? 16 : 0);
   }
 }
 
@@ -131,6 +136,24 @@ __device__ __forceinline__ void stage_R(double2 (*tile)[kBsW], const double2* __
 // tile's first slowness, rotation of (u, v) = (cos + sin, cos - sin) in between.  The
 // amplitude 1 / sqrt(pi omega r) is common to the thread and applied to (ax, ay) by the
 // caller; 1 / sqrt(p_j) is staged.
+template <int NT, int M>
+__device__ __forceinline__ void fast_terms(const double2* __restrict__ ig_p,
+                                           const double2* __restrict__ r_p, int m, double inv_omr,
+                                           double cdl, double sd, double& u, double& v,
+                                           double& ax, double& ay) {
+#pragma unroll 8
+  for (int k = 0; k < (M > 0 ? M : m); ++k) {
+    const double2 ig = ig_p[k];
+    const double2 rv = r_p[k * kBsW];
+    const double t = j0_asym_scaled<NT>(ig.x * inv_omr, u, v) * ig.y;
+    const double u2 = fma(u, cdl, v * sd);
+    v = fma(v, cdl, -u * sd);
+    u = u2;
+    ax = fma(t, rv.x, ax);
+    ay = fma(t, rv.y, ay);
+  }
+}
+
 template <int NT>
 __device__ __forceinline__ void fast_tile(const double2* s_pf, const double2* s_ig,
                                           const double2 (*tile)[kBsW], int k0, int m, int lane,
@@ -139,17 +162,11 @@ __device__ __forceinline__ void fast_tile(const double2* s_pf, const double2* s_
   double s, c;
   sincos((om * s_pf[k0].x) * r, &s, &c);
   double u = c + s, v = c - s;
-#pragma unroll 8
-  for (int k = 0; k < m; ++k) {
-    const double2 ig = s_ig[k0 + k];
-    const double2 rv = tile[k][lane];
-    const double t = j0_asym_scaled<NT>(ig.x * inv_omr, u, v) * ig.y;
-    const double u2 = fma(u, cdl, v * sd);
-    v = fma(v, cdl, -u * sd);
-    u = u2;
-    ax = fma(t, rv.x, ax);
-    ay = fma(t, rv.y, ay);
-  }
+  // full tiles run a loop of compile-time length (no remainder handling)
+  if (m == kSub)
+    fast_terms<NT, kSub>(s_ig + k0, &tile[0][lane], kSub, inv_omr, cdl, sd, u, v, ax, ay);
+  else
+    fast_terms<NT, 0>(s_ig + k0, &tile[0][lane], m, inv_omr, cdl, sd, u, v, ax, ay);
 }
 
 // One thread per (omega, offset) and slowness slice.  Grid: x = slowness slice, y = offset
@@ -212,7 +229,7 @@ bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ 
       const double lin = fma((double)(j - j_begin), step, p0);
       ok = fabs(pj - lin) <= 1e-15 * fabs(pj);
     }
-    stage_R(s_R[0], R, jc, min(kSub, n), iw0, n_w, tid);
+    stage_R(s_R[0], R, jc, min(kSub, n), iw0, n_w);
     cp_async_commit();
     const bool uniform = __syncthreads_and(ok) != 0;
     if (!uniform) since = kRotSteps;
@@ -229,7 +246,7 @@ bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ 
     for (int sb = 0; sb < nsub; ++sb) {
       if (sb + 1 < nsub)
         stage_R(s_R[(sb + 1) & 1], R, jc + (sb + 1) * kSub, min(kSub, n - (sb + 1) * kSub), iw0,
-                n_w, tid);
+                n_w);
       cp_async_commit();
       cp_async_wait_1();  // this thread's copies of tile sb have landed
       __syncthreads();    // ... and every thread's
