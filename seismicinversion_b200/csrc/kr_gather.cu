@@ -233,15 +233,7 @@ bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ 
     cp_async_commit();
     const bool uniform = __syncthreads_and(ok) != 0;
     if (!uniform) since = kRotSteps;
-    // Fast chunk: slownesses in arithmetic progression with x increasing from >= 25, so every
-    // term takes the asymptotic branch with the anchor / rotation scheme (no data-dependent
-    // branches in the inner loop).  The number of expansion terms follows from the chunk's
-    // smallest argument.
-    const double x_first = (om * s_pf[0].x) * r;
-    const bool fast = active && uniform && step > 0.0 && omr > 0.0 && x_first >= kJ0X0;
-    const int nt = x_first >= 3000.0 ? 2 : x_first >= 300.0 ? 3 : x_first >= 100.0 ? 4
-                 : x_first >= 60.0 ? 5 : 7;
-    if (fast) since = kRotSteps;
+    const bool rising = active && uniform && step > 0.0 && omr > 0.0;
     const int nsub = (n + kSub - 1) / kSub;
     for (int sb = 0; sb < nsub; ++sb) {
       if (sb + 1 < nsub)
@@ -252,7 +244,16 @@ bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ 
       __syncthreads();    // ... and every thread's
       const double2(*tile)[kBsW] = s_R[sb & 1];
       const int k0 = sb * kSub, m = min(kSub, n - k0);
+      // Fast tile: slownesses in arithmetic progression with x increasing from >= 25, so
+      // every term takes the asymptotic branch with the anchor / rotation scheme (no
+      // data-dependent branches in the inner loop).  The number of expansion terms follows
+      // from the tile's smallest argument.
+      const double x_first = (om * s_pf[k0].x) * r;
+      const bool fast = rising && x_first >= kJ0X0;
+      const int nt = x_first >= 3000.0 ? 2 : x_first >= 300.0 ? 3 : x_first >= 100.0 ? 4
+                   : x_first >= 60.0 ? 5 : 7;
       if (fast) {
+        since = kRotSteps;
         switch (nt) {
           case 2: fast_tile<2>(s_pf, s_ig, tile, k0, m, lane, om, r, inv_omr, cdl, sd, ax, ay); break;
           case 3: fast_tile<3>(s_pf, s_ig, tile, k0, m, lane, om, r, inv_omr, cdl, sd, ax, ay); break;
