@@ -87,10 +87,12 @@ class ModelBatch:
     """Device-resident packed batch with its plan; see the module docstring.
 
     ``p``, ``omega`` and ``R_obs`` of the items may be NumPy arrays or (CUDA) tensors; device
-    tensors are concatenated on the device without a host round trip."""
+    tensors are concatenated on the device without a host round trip.  ``alloc_stream``: take
+    the batch's device block from that stream's allocator pool (a server running batches on
+    several streams then keeps one pool of cached blocks instead of one per stream)."""
 
     def __init__(self, items: list[BatchItem], schedule: tuple[int, int] | None = None,
-                 device=None):
+                 device=None, alloc_stream: torch.cuda.Stream | None = None):
         self.dev = D.require_cuda(device)
         self.items = items
         n = len(items)
@@ -161,7 +163,14 @@ class ModelBatch:
         for n_b in sizes:
             offs.append(total)
             total += (n_b + 255) // 256 * 256
-        block = torch.empty(_size_class(total), dtype=torch.uint8, device=self.dev)
+        if alloc_stream is None:
+            block = torch.empty(_size_class(total), dtype=torch.uint8, device=self.dev)
+        else:
+            # allocated from one stream's pool (shared by every batch of a server, whatever
+            # stream runs it) and marked as used by the stream that runs this batch
+            with torch.cuda.stream(alloc_stream):
+                block = torch.empty(_size_class(total), dtype=torch.uint8, device=self.dev)
+            block.record_stream(torch.cuda.current_stream(self.dev))
         view = [block[o:o + n_b] for o, n_b in zip(offs, sizes)]
         self.layers = view[0].view(torch.float64)
         staged = torch.from_numpy(np.concatenate(tabs) if tabs else np.zeros(1)).pin_memory()

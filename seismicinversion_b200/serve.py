@@ -94,18 +94,21 @@ class GpuBatchExecutor:
         self.torch = torch
         self.dev = D.require_cuda(device)
         self.streams = [torch.cuda.Stream(self.dev) for _ in range(n_streams)]
+        # every batch's device block comes from this stream's allocator pool, so cached
+        # blocks serve all execution streams (a pool per stream would keep calling cudaMalloc
+        # for sizes that another stream has cached)
+        self.alloc_stream = torch.cuda.Stream(self.dev)
         self.schedule = schedule
         self._k = 0
 
     def prewarm(self, device_bytes: int, host_bytes: int = 16 << 20) -> None:
-        """Reserve caching-allocator segments on every stream (and pinned host blocks) so
+        """Reserve a caching-allocator segment on the allocation stream (and pinned host blocks) so
         that steady-state batches reuse cached memory instead of calling cudaMalloc /
         cudaHostAlloc, which are slow and (cudaMalloc) synchronise the device."""
         torch = self.torch
-        for s in self.streams:
-            with torch.cuda.stream(s):
-                x = torch.empty(int(device_bytes), dtype=torch.uint8, device=self.dev)
-                del x
+        with torch.cuda.stream(self.alloc_stream):
+            x = torch.empty(int(device_bytes), dtype=torch.uint8, device=self.dev)
+            del x
         # one pinned block per power-of-two size class from 1 KB up (the host caching
         # allocator serves plan images and staging copies from these)
         sizes, b = [], 1024
@@ -125,7 +128,8 @@ class GpuBatchExecutor:
         with torch.cuda.stream(s):
             items = [BatchItem(r.model, r.p, r.omega, gradient=r.gradient, R_obs=r.R_obs,
                                free_surface=r.free_surface, store_R=r.gradient) for r in reqs]
-            batch = ModelBatch(items, schedule=self.schedule, device=self.dev)
+            batch = ModelBatch(items, schedule=self.schedule, device=self.dev,
+                               alloc_stream=self.alloc_stream)
             batch.launch()
             ev = torch.cuda.Event()
             ev.record(s)
