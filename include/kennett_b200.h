@@ -5,7 +5,9 @@
  * pointer owned by the caller; the library never allocates or frees caller memory, and
  * every call is enqueued on the caller's CUDA stream (`stream`, a cudaStream_t passed as
  * void*, NULL = legacy default stream).  Calls return a kr_status; no C++ exception
- * crosses this boundary.  Complex numbers are interleaved (re, im) float64 pairs.
+ * crosses this boundary.  Complex numbers are interleaved (re, im) float64 pairs, and every
+ * complex array must start on a 16-byte boundary (the kernels move complex values as
+ * 16-byte units); a misaligned complex pointer is rejected with KR_ERR_INVALID_ARGUMENT.
  *
  * Layer table: float64 [6][n_layers], rows alpha (P velocity), beta (S velocity, 0 in the
  * acoustic ocean = layer 0), rho, thickness (+inf or >= 1e30 marks the half-space), Q_alpha,
@@ -26,7 +28,7 @@ extern "C" {
 typedef int32_t kr_status;
 
 #define KR_OK 0
-#define KR_ERR_INVALID_ARGUMENT 1   /* null pointer, negative size, unknown flag bits      */
+#define KR_ERR_INVALID_ARGUMENT 1   /* null or misaligned pointer, negative size, bad flags */
 #define KR_ERR_INVALID_MODEL 2      /* layer table violates the model rules                 */
 #define KR_ERR_CUDA 3               /* a CUDA runtime call or kernel launch failed          */
 #define KR_ERR_CUFFT 4              /* a cuFFT call failed                                  */

@@ -36,7 +36,6 @@ KR_HD M2 mmac(const M2& s, const M2& x, const M2& y) {  // s + x y
             cmac2(s.c, x.c, y.a, x.d, y.c), cmac2(s.d, x.c, y.b, x.d, y.d));
 }
 KR_HD M2 mT(const M2& x) { return m2(x.a, x.c, x.b, x.d); }
-KR_HD M2 madd(const M2& x, const M2& y) { return m2(x.a + y.a, x.b + y.b, x.c + y.c, x.d + y.d); }
 KR_HD M2 mneg(const M2& x) { return m2(-x.a, -x.b, -x.c, -x.d); }
 
 // Per-layer derivative factors for one slowness.

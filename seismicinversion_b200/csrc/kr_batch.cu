@@ -580,6 +580,8 @@ extern "C" kr_status kr_batch_launch(void* plan, const kr_batch_config* cfg, int
                                      const double* R_obs, double* R, double* chi_grad,
                                      void* stream) {
   if (!plan || !valid_config(cfg) || !layers || !p || !omega) return KR_ERR_INVALID_ARGUMENT;
+  if (!aligned16(omega) || (R && !aligned16(R)) || (R_obs && !aligned16(R_obs)))
+    return KR_ERR_INVALID_ARGUMENT;
   if (max_layers < 2 || max_layers > kMaxLayers) return KR_ERR_INVALID_ARGUMENT;
   cudaStream_t st = (cudaStream_t)stream;
   unsigned char* pl = static_cast<unsigned char*>(plan);

@@ -345,6 +345,7 @@ static kr_status deriv_args(const double* layers, int L, const double* p, int n_
   if (L < 2) return KR_ERR_INVALID_MODEL;
   if (L > kMaxLayers) return KR_ERR_TOO_LARGE;
   if (n_p > 0 && n_w > 0 && (!layers || !p || !omega)) return KR_ERR_INVALID_ARGUMENT;
+  if (!aligned16(omega)) return KR_ERR_INVALID_ARGUMENT;
   return KR_OK;
 }
 
@@ -369,7 +370,7 @@ extern "C" kr_status kr_jacobian(const double* layers, int32_t n_layers, const d
   kr_status s = deriv_args(layers, n_layers, p, n_p, omega, n_w, flags);
   if (s != KR_OK) return s;
   if (n_p == 0 || n_w == 0) return KR_OK;
-  if (!J) return KR_ERR_INVALID_ARGUMENT;
+  if (!J || !aligned16(J) || (R && !aligned16(R))) return KR_ERR_INVALID_ARGUMENT;
   return launch_deriv<false>(layers, n_layers, p, n_p, omega, n_w, flags, nullptr, R, J, nullptr,
                              workspace, workspace_bytes, (cudaStream_t)stream);
 }
@@ -394,7 +395,7 @@ extern "C" kr_status kr_misfit_gradient(const double* layers, int32_t n_layers, 
     if (e != cudaSuccess) set_last_error("kr_misfit_gradient: memset", e);
     return cuda_status(e);
   }
-  if (!R_obs) return KR_ERR_INVALID_ARGUMENT;
+  if (!R_obs || !aligned16(R_obs) || (R && !aligned16(R))) return KR_ERR_INVALID_ARGUMENT;
   return launch_deriv<true>(layers, n_layers, p, n_p, omega, n_w, flags, R_obs, R, nullptr,
                             chi_grad, workspace, workspace_bytes, st);
 }

@@ -125,6 +125,7 @@ extern "C" kr_status kr_reflectivity(const double* layers, int32_t n_layers, con
   if (n_layers > kMaxLayers) return KR_ERR_TOO_LARGE;
   if (n_p == 0 || n_w == 0) return KR_OK;
   if (!layers || !p || !omega || !R) return KR_ERR_INVALID_ARGUMENT;
+  if (!aligned16(omega) || !aligned16(R)) return KR_ERR_INVALID_ARGUMENT;
   const int n_wtiles = (n_w + kFwdThreads - 1) / kFwdThreads;
   cudaStream_t st = (cudaStream_t)stream;
   switch (forward_minb()) {

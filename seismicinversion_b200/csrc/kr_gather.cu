@@ -1,13 +1,13 @@
 // Discrete-wavenumber gather: Bessel-weighted slowness sum and the omega -> t step.
 //
 // kr_bessel_sum: one thread per (offset, omega) and slowness slice.  Blocks are
-// 32 frequencies x 8 offsets; the slowness range is split over grid.z so the grid fills
-// the 148 SMs several times over; each slice writes its partial U to the workspace and a
-// second kernel adds the slices in a fixed order (bit-reproducible).  J0 is evaluated on
+// 32 frequencies x 8 offsets; the slowness range is split into slices (grid.x) so the grid
+// fills the 148 SMs several times over; each slice writes its partial U to the workspace and
+// a second kernel adds the slices in a fixed order (bit-reproducible).  J0 is evaluated on
 // the fly in registers (FP64): Hankel's asymptotic expansion above x = 25 with cos/sin
-// carried along the slowness loop by rotation (exact anchors every 32 steps), CUDA's j0
-// below; R[p][omega] loads are coalesced along omega and shared by the block's 8 offsets
-// through L1.
+// carried along the slowness loop by rotation (exact anchors every 32 steps), a piecewise
+// Taylor table below; R[p][omega] arrives through shared memory in tiles of 32 slownesses
+// x 32 frequencies (cp.async, double-buffered) shared by the block's 8 offsets.
 //
 // kr_traces: builds the half spectrum conj(U S) (DC and Nyquist zero) and runs a batched
 // cuFFT Z2D: for a Hermitian spectrum H, the forward DFT the reference applies
@@ -33,8 +33,8 @@ constexpr int kBsR = 8;   // offsets per block
 //   J0(x) = sqrt(2 / (pi x)) [P(x) cos(x - pi/4) - Q(x) sin(x - pi/4)]
 //         = sqrt(1 / (pi x)) [(P + Q) cos x + (P - Q) sin x],
 //   P = sum_m (-1)^m a_{2m} x^{-2m},  Q = sum_m (-1)^m a_{2m+1} x^{-2m-1}.
-// With 7 terms each the truncation error is below 4e-16 absolute for x >= 25 (checked
-// against SciPy's j0); below 25 the kernel calls CUDA's j0.
+// With 7 terms each the truncation error is below 7e-16 absolute for x >= 25 (checked
+// against SciPy's j0); below 25 the kernel uses the Taylor table of kr_j0_table.h.
 // ---------------------------------------------------------------------------------------
 constexpr double kJ0X0 = 25.0;
 constexpr int kJ0Terms = 7;
@@ -437,6 +437,7 @@ extern "C" kr_status kr_bessel_sum(const double* R, const double* p, const doubl
     return cuda_status(e);
   }
   if (!R || !p || !pw) return KR_ERR_INVALID_ARGUMENT;
+  if (!aligned16(R) || !aligned16(U)) return KR_ERR_INVALID_ARGUMENT;
   if ((n_r + kBsR - 1) / kBsR > 65535 || (n_w + kBsW - 1) / kBsW > 65535)
     return KR_ERR_TOO_LARGE;
   BesselPlan b = bessel_plan(n_p, n_w, n_r);
@@ -471,6 +472,7 @@ extern "C" kr_status kr_traces(const double* U, const double* S, int32_t n_r, in
   if (n_r == 0) return KR_OK;
   if (nw < 2) return KR_ERR_INVALID_ARGUMENT;
   if (!U || !traces) return KR_ERR_INVALID_ARGUMENT;
+  if (!aligned16(U) || (S && !aligned16(S))) return KR_ERR_INVALID_ARGUMENT;
   cudaStream_t st = (cudaStream_t)stream;
   std::lock_guard<std::mutex> lk(g_fft_mu);
   FftEntry* e = nullptr;
@@ -581,6 +583,7 @@ extern "C" kr_status kr_bessel_sum_noalloc(const double* R, const double* p, con
     return cuda_status(e);
   }
   if (!R || !p || !pw) return KR_ERR_INVALID_ARGUMENT;
+  if (!aligned16(R) || !aligned16(U)) return KR_ERR_INVALID_ARGUMENT;
   void* scratch = nullptr;
   kr_status s = scratch_address(&scratch);
   if (s != KR_OK) return s;

@@ -67,7 +67,6 @@ __device__ __forceinline__ void e_up(const LayerG& g, double p, cd E[4][2]) {
 
 KR_HD double cabs1(cd z) { return fabs(z.x) + fabs(z.y); }
 
-template <int N>
 __device__ __forceinline__ void swap_rows(cd (&A)[4][4], cd (&B)[4][2], int c, int piv) {
   // rows c and piv (piv >= c); compile-time indices only
 #pragma unroll
@@ -104,7 +103,7 @@ __device__ __forceinline__ void solve4x2(cd (&A)[4][4], cd (&B)[4][2]) {
         piv = r;
       }
     }
-    swap_rows<4>(A, B, c, piv);
+    swap_rows(A, B, c, piv);
     inv[c] = recip(A[c][c]);
 #pragma unroll
     for (int r = c + 1; r < 4; ++r) {
@@ -270,6 +269,7 @@ extern "C" kr_status kr_gmm_reflectivity(const double* layers, int32_t n_layers,
   if (n_layers > kMaxLayers) return KR_ERR_TOO_LARGE;
   if (n_p == 0 || n_w == 0) return KR_OK;
   if (!layers || !p || !omega || !R) return KR_ERR_INVALID_ARGUMENT;
+  if (!aligned16(omega) || !aligned16(R)) return KR_ERR_INVALID_ARGUMENT;
   const int n_wtiles = (n_w + kGmmThreads - 1) / kGmmThreads;
   // tiles per block: enough slownesses x tile groups for ~8 waves, at most kGmmTabTiles
   long long tpb = ((long long)n_p * n_wtiles) / (148LL * 4 * 8);

@@ -19,6 +19,10 @@ __host__ __device__ inline size_t prologue_smem_bytes(int n_layers) {
 
 inline kr_status cuda_status(cudaError_t e) { return e == cudaSuccess ? KR_OK : KR_ERR_CUDA; }
 
+// Complex arrays are read and written as 16-byte units (vector loads, cp.async): every
+// complex pointer of the C ABI must be 16-byte aligned.  Null passes (checked separately).
+inline bool aligned16(const void* ptr) { return ((uintptr_t)ptr & 15u) == 0; }
+
 // Remembers the last CUDA error string for kr_last_error().
 void set_last_error(const char* where, cudaError_t e);
 void set_last_error_msg(const char* msg);

@@ -100,3 +100,19 @@ def test_no_cpu_fallback_without_gpu():
 
     with pytest.raises(RuntimeError, match="CUDA"):
         kennett_reflectivity(default_ocean_crust_model(), 0.2, np.array([1.0, 2.0]))
+
+
+def test_misaligned_complex_pointers_rejected(so):
+    """Every complex array must start on a 16-byte boundary; the checks run on the host
+    before anything is enqueued (fake addresses are never dereferenced)."""
+    i32, u32 = ctypes.c_int32, ctypes.c_uint32
+    vp = ctypes.c_void_p
+    tab, pp = vp(0x1000), vp(0x2000)
+    for fn in (so.kr_reflectivity, so.kr_gmm_reflectivity):
+        # omega misaligned by 8 bytes, then R misaligned
+        assert fn(tab, i32(3), pp, i32(2), vp(0x3008), i32(4), u32(0), vp(0x4000), None) == 1
+        assert fn(tab, i32(3), pp, i32(2), vp(0x3000), i32(4), u32(0), vp(0x4008), None) == 1
+    ws = vp(0x8000)
+    assert so.kr_bessel_sum(vp(0x3008), pp, pp, i32(2), ctypes.c_double(0.1), vp(0x5000),
+                            i32(4), vp(0x6000), i32(2), vp(0x7000), ws, ctypes.c_size_t(1 << 20),
+                            None) == 1
