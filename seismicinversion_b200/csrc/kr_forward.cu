@@ -19,17 +19,25 @@ constexpr int kFwdThreads = 128;
 constexpr int kTabTiles = kFwdTabTiles;  // frequency tiles per block on the table path
 static_assert(kFwdThreads == kPhTile, "one forward tile is one phase-table tile");
 
+// Bytes of the double-buffered per-tile products hi * mid (PhaseTableHM).
+inline size_t phase_hm_bytes(int n_layers) {
+  return 2 * sizeof(cd) * (size_t)kPhMid * 2 * (size_t)(n_layers - 1);
+}
+
 template <int MINB>
 __global__ void __launch_bounds__(kFwdThreads, MINB)
 reflectivity_kernel(const double* __restrict__ tab, int n_layers, const double* __restrict__ p,
                     int n_p, const double2* __restrict__ omega, int n_w, int n_wtiles,
-                    int tiles_per_block, int free_surface, int use_table,
+                    int tiles_per_block, int free_surface, int use_table, int use_hm,
                     double2* __restrict__ R) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ unsigned s_bad;
   LayerP* s_layer = reinterpret_cast<LayerP*>(smem);
   Iface* s_iface = reinterpret_cast<Iface*>(smem + sizeof(LayerP) * n_layers);
   cd* s_ph = reinterpret_cast<cd*>(smem + prologue_smem_bytes(n_layers));
+  const int n_phase = 2 * (n_layers - 1);
+  cd* s_hm = reinterpret_cast<cd*>(smem + prologue_smem_bytes(n_layers) +
+                                   phase_table_bytes(n_layers, kTabTiles));
   const int groups = (n_wtiles + tiles_per_block - 1) / tiles_per_block;
   const int ip = blockIdx.x / groups;
   const int t0 = (blockIdx.x % groups) * tiles_per_block;
@@ -42,6 +50,33 @@ reflectivity_kernel(const double* __restrict__ tab, int n_layers, const double* 
                              n_layers, s_layer, s_ph, &s_bad);
   const bool fs = free_surface != 0;
   double2* Rp = R + (size_t)ip * n_w;
+  if (use_table && use_hm) {
+    // per-tile products hi * mid, double-buffered: tile t + 1's are formed while tile t is
+    // swept, one barrier per tile
+    const int lo = threadIdx.x & (kPhLo - 1), m = threadIdx.x >> 4;
+    phase_hm(s_ph, entries, n_phase, kPhHead, s_hm);
+    __syncthreads();
+    for (int t = t0; t < t1; ++t) {
+      const int b = (t - t0) & 1;
+      if (t + 1 < t1)
+        phase_hm(s_ph, entries, n_phase, kPhHead + t + 1 - t0, s_hm + (b ^ 1) * n_phase * kPhMid);
+      const int iw = t * kFwdThreads + threadIdx.x;
+      if (iw < n_w) {
+        cd e0, rpp;
+        if ((mask >> (t - t0)) & 1u) {
+          rpp = sweep_ph(n_layers, s_iface,
+                         PhaseTableHM{s_ph, s_hm + b * n_phase * kPhMid, entries, lo, m}, &e0);
+        } else {
+          const double2 wv = omega[iw];
+          rpp = sweep(mk(wv.x, wv.y), n_layers, s_layer, s_iface, &e0);
+        }
+        const cd out = pp_surface(rpp, e0, fs);
+        Rp[iw] = make_double2(out.x, out.y);
+      }
+      __syncthreads();
+    }
+    return;
+  }
   for (int t = t0; t < t1; ++t) {
     const int iw = t * kFwdThreads + threadIdx.x;
     if (iw >= n_w) break;
@@ -89,9 +124,13 @@ static kr_status launch_forward(const double* layers, int n_layers, const double
   size_t smem = prologue_smem_bytes(n_layers);
   int tpb = tiles_per_block(n_p, n_wtiles);
   const bool table = phase_table_model(n_layers);  // <= 50 KB: 4 blocks of 128 per SM
+  bool hm = false;
   if (table) {
     smem += phase_table_bytes(n_layers, kTabTiles);
     tpb = tpb < kTabTiles ? tpb : kTabTiles;
+    // the per-tile products only where they keep the block within the same budget
+    hm = smem + phase_hm_bytes(n_layers) <= kFwdTabSmemMax;
+    if (hm) smem += phase_hm_bytes(n_layers);
   }
   const long long blocks = (long long)n_p * ((n_wtiles + tpb - 1) / tpb);
   if (blocks > 0x7fffffffLL) return KR_ERR_TOO_LARGE;
@@ -105,7 +144,8 @@ static kr_status launch_forward(const double* layers, int n_layers, const double
   }
   reflectivity_kernel<MINB><<<(unsigned)blocks, kFwdThreads, smem, st>>>(
       layers, n_layers, p, n_p, reinterpret_cast<const double2*>(omega), n_w, n_wtiles, tpb,
-      (flags & KR_FREE_SURFACE) ? 1 : 0, table ? 1 : 0, reinterpret_cast<double2*>(R));
+      (flags & KR_FREE_SURFACE) ? 1 : 0, table ? 1 : 0, hm ? 1 : 0,
+      reinterpret_cast<double2*>(R));
   return check_launch("kr_reflectivity");
 }
 

@@ -85,6 +85,30 @@ struct PhaseAuto {
   __device__ __forceinline__ cd b(int l) const { return tab ? t.b(l) : d.b(l); }
 };
 
+// The same factors with the per-tile products hi[u] * mid[m] formed once per block and tile
+// (phase_hm): one complex product per lookup instead of two, the same roundings in the same
+// order, so the values are bit-identical to PhaseTable's.
+struct PhaseTableHM {
+  const cd* tab;
+  const cd* hm;  // [2 (L - 1)][kPhMid] products of the current tile
+  int entries, lo, m;
+  __device__ __forceinline__ cd at(int id) const {
+    return hm[id * kPhMid + m] * tab[id * entries + lo];
+  }
+  __device__ __forceinline__ cd a(int l) const { return at(2 * l); }
+  __device__ __forceinline__ cd b(int l) const { return at(2 * l + 1); }
+};
+
+// Block-cooperative: s_hm[id * kPhMid + m] = hi[hi_entry] * mid[m] for the n_phase phases.
+__device__ __forceinline__ void phase_hm(const cd* s_ph, int entries, int n_phase, int hi_entry,
+                                         cd* s_hm) {
+  for (int e = threadIdx.x; e < n_phase * kPhMid; e += blockDim.x) {
+    const int id = e / kPhMid, m = e - id * kPhMid;
+    const cd* q = s_ph + id * entries;
+    s_hm[e] = q[hi_entry] * q[kPhLo + m];
+  }
+}
+
 __device__ __forceinline__ PhaseTable phase_at(const cd* s_ph, int entries, int k, int u0) {
   const int t = k & (kPhTile - 1);
   return PhaseTable{s_ph, entries, t & (kPhLo - 1), kPhLo + (t >> 4), kPhHead + (k >> 7) - u0};
