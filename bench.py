@@ -738,8 +738,13 @@ def run_ours(args, rank, world, local):
         t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t[0])
-    h2d = tab.numel() * 8 + p.nbytes + (om.nbytes * 2) + offsets.nbytes + S.nbytes + decay.nbytes
-    h2d += (taper * p).nbytes + om.nbytes
+    # compute_gather_gpu uploads one pinned staging buffer per call (layer-table slot, grid
+    # arrays, offsets, source spectrum, decay): its size is the host-to-device traffic
+    from seismicinversion_b200.kennett_gather_gpu import _grid_inputs
+
+    h2d = 8 * int(_grid_inputs(float(T), int(nw), int(npp), float(pmax), float(np.pi / T),
+                               ricker_10hz, np.ascontiguousarray(offsets, dtype=np.float64)
+                               .tobytes())[2][-1])
     d2h = R.numel() * 16 + G.numel() * 8
 
     peak = fp64_peak(torch, dev)
