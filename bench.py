@@ -131,6 +131,10 @@ def _nvml_sample_loop(bus_id, conn, interval):
     pynvml.nvmlInit()
     h = pynvml.nvmlDeviceGetHandleByPciBusId(bus_id)
     smax = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+    # the first queries of a process are slow (tens to hundreds of ms): make them before
+    # the timed region starts
+    pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+    pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
     samples = []
     conn.send("ready")
     t0 = _t.perf_counter()

@@ -115,7 +115,7 @@ class GpuBatchExecutor:
         while b <= int(host_bytes):
             sizes.append(b)
             b *= 2
-        blocks = [torch.empty(n, dtype=torch.uint8, pin_memory=True) for n in sizes for _ in range(4)]
+        blocks = [torch.empty(n, dtype=torch.uint8, pin_memory=True) for n in sizes for _ in range(8)]
         del blocks
         torch.cuda.synchronize(self.dev)
 
