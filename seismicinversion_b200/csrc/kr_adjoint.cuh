@@ -117,7 +117,10 @@ KR_HD void interface_tangents(double p, int iface, const LayerP& up, const Layer
 // and the 10 coefficient adjoints cbar (same order as ScatTan).
 KR_HD void kennett_step_reverse(const M2& r, cd ea, cd eb, const Iface& f, const M2& ob,
                                 M2& rbar, cd& eabar, cd& ebbar, cd cbar[10]) {
-  // forward quantities, formed exactly as in kennett_step
+  // Forward quantities of the full-matrix form of the step (the reference's).  On the
+  // symmetric states kennett_step produces, both forms are the same function of the
+  // coefficients and phase factors at every step, so the chained derivatives below are
+  // those of kennett_step.
   cd eaea = ea * ea, ebeb = eb * eb, eaeb = ea * eb;
   M2 m = m2(eaea * r.a, eaeb * r.b, eaeb * r.c, ebeb * r.d);
   M2 Ru = m2(f.ru11, f.ru12, f.ru12, f.ru22);

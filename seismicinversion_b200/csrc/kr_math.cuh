@@ -10,8 +10,9 @@
 //   PP + free surface     kennett_reflectivity.py:264-326
 //
 // Storage choices (ours): Rd and Ru are symmetric and Tu = Td^T (reciprocity,
-// scattering_matrices.py:150), so an interface is 10 complex numbers.  The 2x2 inverse is
-// one reciprocal of the determinant times the adjugate.
+// scattering_matrices.py:150), so an interface is 10 complex coefficients, stored with 11
+// derived constants of the Kennett step, which runs in a symmetric adjugate form (one
+// reciprocal per step; see kennett_step).
 #pragma once
 
 #include <math.h>
@@ -165,7 +166,14 @@ struct IfaceT {
   T ru11, ru12, ru22;
   T td11, td12, td21, td22;
 };
-typedef IfaceT<cd> Iface;
+
+// The coefficients plus the per-interface constants of kennett_step: 2 ru12, det Ru, and the
+// quadratic forms of Td that give the entries (11, 12, 22) of Td^T X Td for a symmetric X
+// from (x11, x12, x22): q[3 i + k] multiplies the k-th entry in output row i.
+struct Iface : IfaceT<cd> {
+  cd ru12x2, dru;
+  cd q[9];
+};
 
 // Scalar-generic so that the same code yields values (T = cd) and forward-mode tangents
 // (T = a dual number).  rho enters as T so its tangent can be seeded.
@@ -264,65 +272,75 @@ KR_HD Iface interface_coeffs(double p, int iface, const LayerP& up, const LayerP
   else
     solid_solid<cd>(p, up.eta, up.neta, to_c(up.rho), up.betac, lo.eta, lo.neta, to_c(lo.rho),
                     lo.betac, o);
+  const cd t11 = o.td11, t12 = o.td12, t21 = o.td21, t22 = o.td22;
+  o.ru12x2 = 2.0 * o.ru12;
+  o.dru = cdot2(o.ru11, o.ru22, -o.ru12, o.ru12);
+  o.q[0] = t11 * t11;
+  o.q[1] = 2.0 * (t11 * t21);
+  o.q[2] = t21 * t21;
+  o.q[3] = t11 * t12;
+  o.q[4] = cdot2(t11, t22, t21, t12);
+  o.q[5] = t21 * t22;
+  o.q[6] = t12 * t12;
+  o.q[7] = 2.0 * (t12 * t22);
+  o.q[8] = t22 * t22;
   return o;
 }
 
 // ---------------------------------------------------------------------------------------
 // One Kennett addition step: RRd <- Rd + Tu MT (I - Ru MT)^-1 Td with MT = E RRd E,
-// E = diag(ea, eb) of the layer below the interface.  RRd = [[a, b], [c, d]].
+// E = diag(ea, eb) of the layer below the interface (kennett_reflectivity.py:235-256).
 //
-// RRd is symmetric in exact arithmetic, but the two off-diagonal entries carry different
-// rounding, and at large slowness (evanescent layers, near-cancelling interface
-// determinants) the recursion amplifies rounding by ~1e6-1e8: carrying one off-diagonal
-// for both positions loses 1e-8 relative accuracy against an extended-precision
-// evaluation, the full matrix keeps the reference's ~1e-10.  So the step carries all four
-// entries, in the reference's product order (kennett_reflectivity.py:235-256).
+// Evaluated in a symmetric form (ours).  Rd, Ru and MT are symmetric and Tu = Td^T, so
+// X = MT N^-1 (N = I - Ru MT) and RRd are symmetric, and for 2x2 matrices the adjugate is
+// linear, adj(I - Ru MT) = I - adj(MT) adj(Ru), which gives
+//     X = (MT - det(MT) adj(Ru)) / det N,   det N = 1 - tr(Ru MT) + det(Ru) det(MT),
+//     RRd = Rd + Td^T X Td   (three entries, from per-interface quadratic forms of Td).
+// The linearised step maps a perturbation dRRd to Td^T N^-T E dRRd E N^-1 Td, a congruence,
+// so an antisymmetric part of the rounding never reaches R; the reference's full-matrix
+// evaluation carries such a part, and carrying one of its off-diagonals for both positions
+// turns it into error (1e-8 at large slowness).  The symmetric form has none by
+// construction and avoids forming N's entries, whose products cancel when the interface
+// determinants do: on the reference's 5-layer default model, over the 8192-slowness gather
+// grid, its worst relative error against an 80-bit evaluation of the reference's form is
+// 1.7e-10 (no free surface) and 8.1e-11 (free surface), against 8.9e-10 and 2.4e-10 for the
+// full-matrix form in double; on 21-layer models both stay near 1e-12.  ~120 FP64 operations
+// per step instead of ~190.  RRd = [[a, b], [c, d]] with c = b.
 // ---------------------------------------------------------------------------------------
 struct M2 {
   cd a, b, c, d;
 };
 
-KR_HD M2 kennett_step(const M2& r, cd ea, cd eb, const Iface& f) {
+// X = MT (I - Ru MT)^-1 of the step (entries 11, 12, 22).
+KR_HD void step_x(const M2& r, cd ea, cd eb, const Iface& f, cd& x11, cd& x12, cd& x22) {
   cd eaea = ea * ea, ebeb = eb * eb, eaeb = ea * eb;
-  cd m11 = eaea * r.a, m12 = eaeb * r.b, m21 = eaeb * r.c, m22 = ebeb * r.d;
-  // N = I - Ru MT
+  cd m11 = eaea * r.a, m12 = eaeb * r.b, m22 = ebeb * r.d;
+  cd dm = cdot2(m11, m22, -m12, m12);
   const cd one = mk(1.0, 0.0);
-  cd n11 = cmac2(one, -f.ru11, m11, -f.ru12, m21);
-  cd n12 = cdot2(-f.ru11, m12, -f.ru12, m22);
-  cd n21 = cdot2(-f.ru12, m11, -f.ru22, m21);
-  cd n22 = cmac2(one, -f.ru12, m12, -f.ru22, m22);
-  cd idet = recip(cdot2(n11, n22, -n12, n21));
-  cd u11 = n22 * idet, u12 = -(n12 * idet), u21 = -(n21 * idet), u22 = n11 * idet;
-  cd x11 = cdot2(m11, u11, m12, u21), x12 = cdot2(m11, u12, m12, u22);
-  cd x21 = cdot2(m21, u11, m22, u21), x22 = cdot2(m21, u12, m22, u22);
-  // Tu X with Tu = Td^T
-  cd z11 = cdot2(f.td11, x11, f.td21, x21), z12 = cdot2(f.td11, x12, f.td21, x22);
-  cd z21 = cdot2(f.td12, x11, f.td22, x21), z22 = cdot2(f.td12, x12, f.td22, x22);
+  cd idet = recip(cmac(cmac(cmac(cmac(one, -f.ru11, m11), -f.ru12x2, m12), -f.ru22, m22),
+                       f.dru, dm));
+  x11 = cmac(m11, -f.ru22, dm) * idet;
+  x12 = cmac(m12, f.ru12, dm) * idet;
+  x22 = cmac(m22, -f.ru11, dm) * idet;
+}
+
+KR_HD M2 kennett_step(const M2& r, cd ea, cd eb, const Iface& f) {
+  cd x11, x12, x22;
+  step_x(r, ea, eb, f, x11, x12, x22);
   M2 o;
-  o.a = cmac2(f.rd11, z11, f.td11, z12, f.td21);
-  o.b = cmac2(f.rd12, z11, f.td12, z12, f.td22);
-  o.c = cmac2(f.rd12, z21, f.td11, z22, f.td21);
-  o.d = cmac2(f.rd22, z21, f.td12, z22, f.td22);
+  o.a = cmac(cmac(cmac(f.rd11, f.q[0], x11), f.q[1], x12), f.q[2], x22);
+  o.b = cmac(cmac(cmac(f.rd12, f.q[3], x11), f.q[4], x12), f.q[5], x22);
+  o.d = cmac(cmac(cmac(f.rd22, f.q[6], x11), f.q[7], x12), f.q[8], x22);
+  o.c = o.b;
   return o;
 }
 
-// The last (ocean-bottom) step, returning only RRd_00: that interface's Rd has one entry and
-// Td one column (Td = [[t11, 0], [t21, 0]]), so RRd_00 = rd11 + t11 (x11 t11 + x12 t21)
-// + t21 (x21 t11 + x22 t21) with X = MT (I - Ru MT)^-1 (same products as kennett_step).
+// The last (ocean-bottom) step, returning only RRd_00 (the same arithmetic as kennett_step's
+// first entry; that interface's Td has one column, so only q[0..2] are non-zero).
 KR_HD cd kennett_last_step_pp(const M2& r, cd ea, cd eb, const Iface& f) {
-  cd eaea = ea * ea, ebeb = eb * eb, eaeb = ea * eb;
-  cd m11 = eaea * r.a, m12 = eaeb * r.b, m21 = eaeb * r.c, m22 = ebeb * r.d;
-  const cd one = mk(1.0, 0.0);
-  cd n11 = cmac2(one, -f.ru11, m11, -f.ru12, m21);
-  cd n12 = cdot2(-f.ru11, m12, -f.ru12, m22);
-  cd n21 = cdot2(-f.ru12, m11, -f.ru22, m21);
-  cd n22 = cmac2(one, -f.ru12, m12, -f.ru22, m22);
-  cd idet = recip(cdot2(n11, n22, -n12, n21));
-  cd u11 = n22 * idet, u12 = -(n12 * idet), u21 = -(n21 * idet), u22 = n11 * idet;
-  cd x11 = cdot2(m11, u11, m12, u21), x12 = cdot2(m11, u12, m12, u22);
-  cd x21 = cdot2(m21, u11, m22, u21), x22 = cdot2(m21, u12, m22, u22);
-  cd z11 = cdot2(f.td11, x11, f.td21, x21), z12 = cdot2(f.td11, x12, f.td21, x22);
-  return cmac2(f.rd11, z11, f.td11, z12, f.td21);
+  cd x11, x12, x22;
+  step_x(r, ea, eb, f, x11, x12, x22);
+  return cmac(cmac(cmac(f.rd11, f.q[0], x11), f.q[1], x12), f.q[2], x22);
 }
 
 // PP reflectivity at the surface from RRd_PP below the ocean and the ocean phase e0.

@@ -76,7 +76,7 @@ def request_bytes(model: LayerModel, n_p: int, n_w: int, gradient: bool) -> int:
     L = model.n_layers
     I = L - 1
     b = 48 * L + 8 * n_p + 16 * n_w + 16 * n_p * n_w  # layers, p, omega, R
-    coef = 88 * L + 160 * I + 512
+    coef = 96 * L + 336 * I + 512
     if gradient:
         b += 16 * n_p * n_w + 8 * (4 * L + 1)  # R_obs, chi_grad
         coef += 112 * L + 960 * I + 256
