@@ -23,20 +23,6 @@ namespace kr {
 
 // ---------------- 2x2 complex matrix helpers ([[a, b], [c, d]]) ----------------
 KR_HD M2 m2(cd a, cd b, cd c, cd d) { M2 r; r.a = a; r.b = b; r.c = c; r.d = d; return r; }
-KR_HD M2 mmul(const M2& x, const M2& y) {  // x y, fused products (cdot2)
-  return m2(cdot2(x.a, y.a, x.b, y.c), cdot2(x.a, y.b, x.b, y.d), cdot2(x.c, y.a, x.d, y.c),
-            cdot2(x.c, y.b, x.d, y.d));
-}
-KR_HD M2 mmul_neg(const M2& x, const M2& y) {  // -(x y)
-  return m2(cdot2(-x.a, y.a, -x.b, y.c), cdot2(-x.a, y.b, -x.b, y.d),
-            cdot2(-x.c, y.a, -x.d, y.c), cdot2(-x.c, y.b, -x.d, y.d));
-}
-KR_HD M2 mmac(const M2& s, const M2& x, const M2& y) {  // s + x y
-  return m2(cmac2(s.a, x.a, y.a, x.b, y.c), cmac2(s.b, x.a, y.b, x.b, y.d),
-            cmac2(s.c, x.c, y.a, x.d, y.c), cmac2(s.d, x.c, y.b, x.d, y.d));
-}
-KR_HD M2 mT(const M2& x) { return m2(x.a, x.c, x.b, x.d); }
-KR_HD M2 mneg(const M2& x) { return m2(-x.a, -x.b, -x.c, -x.d); }
 
 // Per-layer derivative factors for one slowness.
 struct LayerD {
@@ -112,54 +98,60 @@ KR_HD void interface_tangents(double p, int iface, const LayerP& up, const Layer
     for (int j = 0; j < 6; ++j) out.t[k][j] = c[k]->d[j];
 }
 
-// Reverse of kennett_step.  Inputs: the step's input state r, the phase factors, the
-// interface, and ob = dR/d(step output).  Outputs: rbar = dR/d(step input), dR/dea, dR/deb
-// and the 10 coefficient adjoints cbar (same order as ScatTan).
+// Reverse of kennett_step, differentiating its symmetric adjugate form.  States and their
+// adjoints are symmetric: the adjoint of an off-diagonal entry is that of the one value both
+// positions share (ob.b; ob.c is not read and rbar.c is 0).  Inputs: the step's input state
+// r, the phase factors, the interface, and ob = dR/d(step output).  Outputs:
+// rbar = dR/d(step input), dR/dea, dR/deb and the 10 coefficient adjoints cbar (same order
+// as ScatTan).  Forward, with P = ea^2, Q = eb^2, S = ea eb:
+//   m = (P r11, S r12, Q r22),  dm = m11 m22 - m12^2,  dru = ru11 ru22 - ru12^2,
+//   D = 1 - ru11 m11 - 2 ru12 m12 - ru22 m22 + dru dm,
+//   A = (m11 - ru22 dm, m12 + ru12 dm, m22 - ru11 dm),  X = A / D,
+//   out = Rd + Td^T X Td = Rd + q(Td) . X.
 KR_HD void kennett_step_reverse(const M2& r, cd ea, cd eb, const Iface& f, const M2& ob,
                                 M2& rbar, cd& eabar, cd& ebbar, cd cbar[10]) {
-  // Forward quantities of the full-matrix form of the step (the reference's).  On the
-  // symmetric states kennett_step produces, both forms are the same function of the
-  // coefficients and phase factors at every step, so the chained derivatives below are
-  // those of kennett_step.
-  cd eaea = ea * ea, ebeb = eb * eb, eaeb = ea * eb;
-  M2 m = m2(eaea * r.a, eaeb * r.b, eaeb * r.c, ebeb * r.d);
-  M2 Ru = m2(f.ru11, f.ru12, f.ru12, f.ru22);
-  M2 Td = m2(f.td11, f.td12, f.td21, f.td22);
+  // forward quantities, formed exactly as in kennett_step
+  const cd P = ea * ea, Q = eb * eb, S = ea * eb;
+  const cd m11 = P * r.a, m12 = S * r.b, m22 = Q * r.d;
+  const cd dm = cdot2(m11, m22, -m12, m12);
   const cd one = mk(1.0, 0.0);
-  M2 N = m2(cmac2(one, -f.ru11, m.a, -f.ru12, m.c), cdot2(-f.ru11, m.b, -f.ru12, m.d),
-            cdot2(-f.ru12, m.a, -f.ru22, m.c), cmac2(one, -f.ru12, m.b, -f.ru22, m.d));
-  cd idet = recip(cdot2(N.a, N.d, -N.b, N.c));
-  M2 U = m2(N.d * idet, -(N.b * idet), -(N.c * idet), N.a * idet);
-  M2 X = mmul(m, U);
-  M2 Z = mmul(mT(Td), X);
-  // out = Rd + Z Td
-  M2 Zb = mmul(ob, mT(Td));
-  M2 Tdb = mmul(mT(Z), ob);
-  // Z = Td^T X
-  M2 Xb = mmul(Td, Zb);
-  Tdb = mmac(Tdb, X, mT(Zb));
-  // X = m U: mb = Xb U^T, Ub = m^T Xb.  U = N^-1: Nb = -U^T Ub U^T = -(m U)^T (Xb U^T)
-  // = -X^T mb (before mb's second term below), two 2x2 products fewer than the literal form.
-  M2 mb = mmul(Xb, mT(U));
-  M2 Nb = mmul_neg(mT(X), mb);
-  // N = I - Ru m
-  M2 Rub = mmul_neg(Nb, mT(m));
-  mb = mmac(mb, mneg(Ru), Nb);
-  // m = E r E
-  rbar = m2(mb.a * eaea, mb.b * eaeb, mb.c * eaeb, mb.d * ebeb);
-  cd cross = cdot2(r.b, mb.b, r.c, mb.c);
-  eabar = cmac(eb * cross, 2.0 * ea, r.a * mb.a);
-  ebbar = cmac(ea * cross, 2.0 * eb, r.d * mb.d);
-  cbar[0] = ob.a;
-  cbar[1] = ob.b + ob.c;
-  cbar[2] = ob.d;
-  cbar[3] = Rub.a;
-  cbar[4] = Rub.b + Rub.c;
-  cbar[5] = Rub.d;
-  cbar[6] = Tdb.a;
-  cbar[7] = Tdb.b;
-  cbar[8] = Tdb.c;
-  cbar[9] = Tdb.d;
+  const cd idet = recip(cmac(cmac(cmac(cmac(one, -f.ru11, m11), -f.ru12x2, m12), -f.ru22, m22),
+                             f.dru, dm));
+  const cd a11 = cmac(m11, -f.ru22, dm), a12 = cmac(m12, f.ru12, dm),
+           a22 = cmac(m22, -f.ru11, dm);
+  const cd x11 = a11 * idet, x12 = a12 * idet, x22 = a22 * idet;
+  const cd o11 = ob.a, o12 = ob.b, o22 = ob.d;
+  // out = Rd + q . X: adjoints of X, and of Td through the quadratic forms (W = X Td)
+  const cd xb11 = cmac(cmac(f.q[0] * o11, f.q[3], o12), f.q[6], o22);
+  const cd xb12 = cmac(cmac(f.q[1] * o11, f.q[4], o12), f.q[7], o22);
+  const cd xb22 = cmac(cmac(f.q[2] * o11, f.q[5], o12), f.q[8], o22);
+  const cd w1 = cdot2(f.td11, x11, f.td21, x12), w2 = cdot2(f.td11, x12, f.td21, x22);
+  const cd w3 = cdot2(f.td12, x11, f.td22, x12), w4 = cdot2(f.td12, x12, f.td22, x22);
+  const cd o11x2 = 2.0 * o11, o22x2 = 2.0 * o22;
+  cbar[0] = o11;
+  cbar[1] = o12;
+  cbar[2] = o22;
+  cbar[6] = cdot2(o11x2, w1, o12, w3);  // td11
+  cbar[7] = cdot2(o12, w1, o22x2, w3);  // td12
+  cbar[8] = cdot2(o11x2, w2, o12, w4);  // td21
+  cbar[9] = cdot2(o12, w2, o22x2, w4);  // td22
+  // X = A / D
+  const cd ab11 = xb11 * idet, ab12 = xb12 * idet, ab22 = xb22 * idet;
+  const cd Db = -(cmac(cdot2(xb11, a11, xb12, a12), xb22, a22) * (idet * idet));
+  // A and D from m, dm and Ru
+  const cd dmb = cmac(cmac(cmac(f.dru * Db, -f.ru22, ab11), f.ru12, ab12), -f.ru11, ab22);
+  const cd mb11 = cmac(cmac(ab11, -f.ru11, Db), m22, dmb);
+  const cd mb22 = cmac(cmac(ab22, -f.ru22, Db), m11, dmb);
+  const cd mb12 = cmac(cmac(ab12, -f.ru12x2, Db), -2.0 * m12, dmb);
+  const cd dDb = Db * dm;  // adjoint of dru
+  cbar[3] = cmac(cmac(-(m11 * Db), f.ru22, dDb), -ab22, dm);                 // ru11
+  cbar[4] = cmac(cmac(-2.0 * (m12 * Db), -f.ru12x2, dDb), ab12, dm);         // ru12
+  cbar[5] = cmac(cmac(-(m22 * Db), f.ru11, dDb), -ab11, dm);                 // ru22
+  // m = (P r11, S r12, Q r22)
+  rbar = m2(mb11 * P, mb12 * S, mk(0.0, 0.0), mb22 * Q);
+  const cd Sb = r.b * mb12;
+  eabar = cmac(eb * Sb, 2.0 * ea, r.a * mb11);
+  ebbar = cmac(ea * Sb, 2.0 * eb, r.d * mb22);
 }
 
 // Bytes of one slowness's derivative data in shared memory (layer terms, layer derivative
@@ -316,10 +308,10 @@ KR_HD void jacobian_pair(int L, cd w, bool free_surface, int seg, const LayerP* 
       ob = rb;
     }
   }
-  // bottom interface I-1 initialises RRd = Rd
+  // bottom interface I-1 initialises RRd = Rd (ob.b: the symmetric off-diagonal's adjoint)
   cd cbar[10];
   cbar[0] = ob.a;
-  cbar[1] = ob.b + ob.c;
+  cbar[1] = ob.b;
   cbar[2] = ob.d;
   for (int k = 3; k < 10; ++k) cbar[k] = mk(0.0, 0.0);
   contract(tan[I - 1], cbar, cur, nxt);
