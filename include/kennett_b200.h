@@ -269,8 +269,9 @@ kr_status kr_batch_launch(void* plan, const kr_batch_config* cfg, int32_t max_la
 /*
  * Tuning knob (no counterpart in the reference): register budget of the kr_reflectivity
  * kernel as the number of 128-thread blocks each SM must fit (4 -> 128 registers per thread,
- * 5 -> 96, 6 -> 80; other values select 4).  Process-wide; results are identical for every
- * setting, only speed changes.
+ * 5 -> 96, 6 -> 80; other values restore the automatic choice: 5 for models whose phases
+ * come from the frequency-grid table, 4 otherwise).  Process-wide; results are identical for
+ * every setting, only speed changes.
  */
 void kr_set_forward_variant(int32_t min_blocks_per_sm);
 

@@ -19,9 +19,10 @@ constexpr int kFwdThreads = 128;
 constexpr int kTabTiles = kFwdTabTiles;  // frequency tiles per block on the table path
 static_assert(kFwdThreads == kPhTile, "one forward tile is one phase-table tile");
 
-// Bytes of the double-buffered per-tile products hi * mid (PhaseTableHM).
+// Bytes of the per-warp products hi * mid of the current tile (PhaseTableHM).
+constexpr int kFwdWarps = kFwdThreads / 32;
 inline size_t phase_hm_bytes(int n_layers) {
-  return 2 * sizeof(cd) * (size_t)kPhMid * 2 * (size_t)(n_layers - 1);
+  return sizeof(cd) * (size_t)kFwdWarps * 2 * 2 * (size_t)(n_layers - 1);
 }
 
 template <int MINB>
@@ -51,21 +52,19 @@ reflectivity_kernel(const double* __restrict__ tab, int n_layers, const double* 
   const bool fs = free_surface != 0;
   double2* Rp = R + (size_t)ip * n_w;
   if (use_table && use_hm) {
-    // per-tile products hi * mid, double-buffered: tile t + 1's are formed while tile t is
-    // swept, one barrier per tile
-    const int lo = threadIdx.x & (kPhLo - 1), m = threadIdx.x >> 4;
-    phase_hm(s_ph, entries, n_phase, kPhHead, s_hm);
-    __syncthreads();
+    // per-tile products hi * mid, formed by each warp for its own two mid entries: the tile
+    // loop has no block barrier, so the warps drift apart and hide each other's latencies
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int lo = lane & (kPhLo - 1), m = lane >> 4;
+    cd* hmw = s_hm + warp * 2 * n_phase;
     for (int t = t0; t < t1; ++t) {
-      const int b = (t - t0) & 1;
-      if (t + 1 < t1)
-        phase_hm(s_ph, entries, n_phase, kPhHead + t + 1 - t0, s_hm + (b ^ 1) * n_phase * kPhMid);
       const int iw = t * kFwdThreads + threadIdx.x;
+      const bool tab_tile = (mask >> (t - t0)) & 1u;
+      if (tab_tile) phase_hm_warp(s_ph, entries, n_phase, kPhHead + t - t0, 2 * warp, hmw);
       if (iw < n_w) {
         cd e0, rpp;
-        if ((mask >> (t - t0)) & 1u) {
-          rpp = sweep_ph(n_layers, s_iface,
-                         PhaseTableHM{s_ph, s_hm + b * n_phase * kPhMid, entries, lo, m}, &e0);
+        if (tab_tile) {
+          rpp = sweep_ph(n_layers, s_iface, PhaseTableHM{s_ph, hmw, entries, lo, m}, &e0);
         } else {
           const double2 wv = omega[iw];
           rpp = sweep(mk(wv.x, wv.y), n_layers, s_layer, s_iface, &e0);
@@ -73,7 +72,7 @@ reflectivity_kernel(const double* __restrict__ tab, int n_layers, const double* 
         const cd out = pp_surface(rpp, e0, fs);
         Rp[iw] = make_double2(out.x, out.y);
       }
-      __syncthreads();
+      __syncwarp();  // the warp's products are read before the next tile's overwrite them
     }
     return;
   }
@@ -104,17 +103,20 @@ static int tiles_per_block(long long n_p, int n_wtiles) {
 }
 
 // Register budget of the forward kernel: blocks of 128 threads resident per SM the compiler
-// must allow (4 -> 128 registers, 5 -> 102, 6 -> 85).  Chosen by kr_set_forward_variant (the
-// autotuner) or the KR_FWD_MINB environment variable; default 4.
-static int g_fwd_minb = 0;
+// must allow (4 -> 128 registers, 5 -> 96, 6 -> 80).  Set by kr_set_forward_variant or the
+// KR_FWD_MINB environment variable; otherwise 5 for models on the phase-table path (21-layer
+// gather grid: 3.34 ms at 5, 3.45 ms at 4, 3.37 ms at 6) and 4 for direct phases, whose
+// exponentials need the registers.
+static int g_fwd_minb = -1;  // -1: not read yet, 0: automatic
 
-static int forward_minb() {
-  if (g_fwd_minb == 0) {
+static int forward_minb(bool table) {
+  if (g_fwd_minb < 0) {
     const char* e = getenv("KR_FWD_MINB");
-    int v = e ? atoi(e) : 4;
-    g_fwd_minb = (v == 5 || v == 6) ? v : 4;
+    const int v = e ? atoi(e) : 0;
+    g_fwd_minb = (v >= 4 && v <= 6) ? v : 0;
   }
-  return g_fwd_minb;
+  if (g_fwd_minb > 0) return g_fwd_minb;
+  return table ? 5 : 4;
 }
 
 template <int MINB>
@@ -154,7 +156,7 @@ static kr_status launch_forward(const double* layers, int n_layers, const double
 using namespace kr;
 
 extern "C" void kr_set_forward_variant(int32_t min_blocks_per_sm) {
-  g_fwd_minb = (min_blocks_per_sm == 5 || min_blocks_per_sm == 6) ? min_blocks_per_sm : 4;
+  g_fwd_minb = (min_blocks_per_sm >= 4 && min_blocks_per_sm <= 6) ? min_blocks_per_sm : 0;
 }
 
 extern "C" kr_status kr_reflectivity(const double* layers, int32_t n_layers, const double* p,
@@ -168,7 +170,7 @@ extern "C" kr_status kr_reflectivity(const double* layers, int32_t n_layers, con
   if (!aligned16(omega) || !aligned16(R)) return KR_ERR_INVALID_ARGUMENT;
   const int n_wtiles = (n_w + kFwdThreads - 1) / kFwdThreads;
   cudaStream_t st = (cudaStream_t)stream;
-  switch (forward_minb()) {
+  switch (forward_minb(phase_table_model(n_layers))) {
     case 6:
       return launch_forward<6>(layers, n_layers, p, n_p, omega, n_w, n_wtiles, flags, R, st);
     case 5:

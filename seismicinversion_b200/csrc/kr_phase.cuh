@@ -85,28 +85,30 @@ struct PhaseAuto {
   __device__ __forceinline__ cd b(int l) const { return tab ? t.b(l) : d.b(l); }
 };
 
-// The same factors with the per-tile products hi[u] * mid[m] formed once per block and tile
-// (phase_hm): one complex product per lookup instead of two, the same roundings in the same
-// order, so the values are bit-identical to PhaseTable's.
+// The same factors with the per-tile products hi[u] * mid[m] formed once per tile
+// (phase_hm_warp): one complex product per lookup instead of two, the same roundings in the
+// same order, so the values are bit-identical to PhaseTable's.  A warp's 32 consecutive
+// frequencies use two mid entries, so each warp forms its own products (no block barrier).
 struct PhaseTableHM {
   const cd* tab;
-  const cd* hm;  // [2 (L - 1)][kPhMid] products of the current tile
-  int entries, lo, m;
+  const cd* hm;  // [2 (L - 1)][2] products of the warp's current tile
+  int entries, lo, m;  // m: which of the warp's two mid entries
   __device__ __forceinline__ cd at(int id) const {
-    return hm[id * kPhMid + m] * tab[id * entries + lo];
+    return hm[2 * id + m] * tab[id * entries + lo];
   }
   __device__ __forceinline__ cd a(int l) const { return at(2 * l); }
   __device__ __forceinline__ cd b(int l) const { return at(2 * l + 1); }
 };
 
-// Block-cooperative: s_hm[id * kPhMid + m] = hi[hi_entry] * mid[m] for the n_phase phases.
-__device__ __forceinline__ void phase_hm(const cd* s_ph, int entries, int n_phase, int hi_entry,
-                                         cd* s_hm) {
-  for (int e = threadIdx.x; e < n_phase * kPhMid; e += blockDim.x) {
-    const int id = e / kPhMid, m = e - id * kPhMid;
-    const cd* q = s_ph + id * entries;
-    s_hm[e] = q[hi_entry] * q[kPhLo + m];
+// Warp-cooperative: s_hm[2 id + k] = hi[hi_entry] * mid[m0 + k] (k = 0, 1) for the n_phase
+// phases, followed by __syncwarp.
+__device__ __forceinline__ void phase_hm_warp(const cd* s_ph, int entries, int n_phase,
+                                              int hi_entry, int m0, cd* s_hm) {
+  for (int e = threadIdx.x & 31; e < 2 * n_phase; e += 32) {
+    const cd* q = s_ph + (e >> 1) * entries;
+    s_hm[e] = q[hi_entry] * q[kPhLo + m0 + (e & 1)];
   }
+  __syncwarp();
 }
 
 __device__ __forceinline__ PhaseTable phase_at(const cd* s_ph, int entries, int k, int u0) {

@@ -168,3 +168,28 @@ def test_device_tensors_stay_on_device():
     R = kennett_reflectivity_batch(m, torch.tensor([0.1, 0.2], device="cuda", dtype=torch.float64), w)
     assert R.is_cuda and R.dtype == torch.complex128
     assert rel_err(R.cpu().numpy(), _oracle(m, [0.1, 0.2], w.cpu().numpy(), False)) < TOL
+
+
+@pytest.mark.parametrize("n_sub", [20, 40])
+def test_register_budget_variants_are_bit_identical(n_sub):
+    """kr_set_forward_variant only changes the kernel's register budget: every setting gives
+    the same bits (21 layers on the phase-table path, 41 layers on direct phases)."""
+    from seismicinversion_b200 import _lib
+    from seismicinversion_b200 import device as D
+    from seismicinversion_b200.earth_models import random_layered_model
+
+    m = random_layered_model(n_sub, seed=11)
+    p = np.linspace(0.01, 1.1, 37)
+    w = np.arange(1, 700) * (2 * np.pi / 64) + 1j * (np.pi / 64)
+    tab = D.layer_table(m)
+    h = _lib.lib()
+    outs = []
+    try:
+        for v in (4, 5, 6, 0):
+            h.kr_set_forward_variant(v)
+            outs.append(D.reflectivity(tab, p, w, True).cpu().numpy())
+    finally:
+        h.kr_set_forward_variant(0)
+    for o in outs[1:]:
+        assert np.array_equal(o, outs[0])
+    assert rel_err(outs[0], _oracle(m, p, w, True)) < TOL
