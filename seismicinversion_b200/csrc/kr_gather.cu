@@ -7,7 +7,7 @@
 // the fly in registers (FP64): Hankel's asymptotic expansion above x = 25 with cos/sin
 // carried along the slowness loop by rotation (exact anchors every 32 steps), a piecewise
 // Taylor table below; R[p][omega] arrives through shared memory in tiles of 32 slownesses
-// x 32 frequencies (cp.async, double-buffered) shared by the block's 8 offsets.
+// x 32 frequencies (cp.async, a ring of three) shared by the block's 8 offsets.
 //
 // kr_traces: builds the half spectrum conj(U S) (DC and Nyquist zero) and runs a batched
 // cuFFT Z2D: for a Hermitian spectrum H, the forward DFT the reference applies
@@ -102,10 +102,14 @@ constexpr int kRotSteps = 32;
 constexpr int kChunk = 256;
 
 // R rows are staged through shared memory in tiles of kSub slownesses x 32 frequencies
-// (16 KB), double-buffered with cp.async: the 8 offset warps of a block read each R element
-// from shared memory instead of each loading it from L1 / L2, and the next tile is in flight
-// while the current one is summed.  kSub equals the rotation anchor spacing.
+// (16 KB) in a ring of three with cp.async: the 8 offset warps of a block read each R
+// element from shared memory instead of each loading it from L1 / L2, two tiles are in
+// flight while one is summed, and one block barrier per tile suffices (the barrier that
+// publishes tile t also shows every warp done with tile t - 1, whose buffer then takes
+// tile t + 2).  kSub equals the rotation anchor spacing.
 constexpr int kSub = kRotSteps;
+constexpr int kRing = 3;
+constexpr size_t kRingBytes = sizeof(double2) * kRing * kSub * kBsW;  // dynamic shared memory
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
@@ -176,7 +180,7 @@ __device__ __forceinline__ void fast_tile(const double2* s_pf, const double2* s_
 // in shared memory and checks once whether the chunk continues the slice's arithmetic
 // progression (to 4.5 ulp); inside such a chunk cos / sin of x_j = (omega p_j) r advance by
 // one rotation per slowness, with an exact sincos anchor every kRotSteps.  R arrives in
-// double-buffered tiles (stage_R).  omega is factored out of the weight:
+// tiles through a ring of three buffers (stage_R).  omega is factored out of the weight:
 // U = omega * sum_j J0(x_j) (pw_j dp) R_j.
 __global__ void __launch_bounds__(kBsW * kBsR, 2)
 bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ p,
@@ -187,7 +191,8 @@ bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ 
   __shared__ double2 s_pf[kChunk];  // (p_j, pw_j dp)
   __shared__ double2 s_ig[kChunk];  // (1 / p_j, pw_j dp / sqrt(p_j))
   __shared__ double s_j0[kJ0TabIntervals * kJ0Row];
-  __shared__ __align__(16) double2 s_R[2][kSub][kBsW];
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  double2(*s_R)[kSub][kBsW] = reinterpret_cast<double2(*)[kSub][kBsW]>(s_dyn);  // [kRing]
   const int tid = threadIdx.y * kBsW + threadIdx.x;
   for (int e = tid; e < kJ0TabIntervals * kJ0Row; e += kBsW * kBsR) {
     const int k = e / kJ0Row, n = e - k * kJ0Row;
@@ -229,20 +234,24 @@ bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ 
       const double lin = fma((double)(j - j_begin), step, p0);
       ok = fabs(pj - lin) <= 1e-15 * fabs(pj);
     }
+    const int nsub = (n + kSub - 1) / kSub;
+    // tiles 0 and 1 now, tile sb + 2 in iteration sb; every thread commits one group per
+    // step (empty ones included), so wait_group 1 at iteration sb means tile sb has landed
     stage_R(s_R[0], R, jc, min(kSub, n), iw0, n_w);
+    cp_async_commit();
+    if (nsub > 1) stage_R(s_R[1], R, jc + kSub, min(kSub, n - kSub), iw0, n_w);
     cp_async_commit();
     const bool uniform = __syncthreads_and(ok) != 0;
     if (!uniform) since = kRotSteps;
     const bool rising = active && uniform && step > 0.0 && omr > 0.0;
-    const int nsub = (n + kSub - 1) / kSub;
     for (int sb = 0; sb < nsub; ++sb) {
-      if (sb + 1 < nsub)
-        stage_R(s_R[(sb + 1) & 1], R, jc + (sb + 1) * kSub, min(kSub, n - (sb + 1) * kSub), iw0,
-                n_w);
-      cp_async_commit();
       cp_async_wait_1();  // this thread's copies of tile sb have landed
-      __syncthreads();    // ... and every thread's
-      const double2(*tile)[kBsW] = s_R[sb & 1];
+      __syncthreads();    // ... and every thread's; every thread is done with tile sb - 1
+      if (sb + 2 < nsub)
+        stage_R(s_R[(sb + 2) % kRing], R, jc + (sb + 2) * kSub,
+                min(kSub, n - (sb + 2) * kSub), iw0, n_w);
+      cp_async_commit();
+      const double2(*tile)[kBsW] = s_R[sb % kRing];
       const int k0 = sb * kSub, m = min(kSub, n - k0);
       // Fast tile: slownesses in arithmetic progression with x increasing from >= 25, so
       // every term takes the asymptotic branch with the anchor / rotation scheme (no
@@ -288,7 +297,6 @@ bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ 
           by = fma(t, rv.y, by);
         }
       }
-      __syncthreads();  // tile sb is read before iteration sb + 1 refills its buffer
     }
   }
   if (active)
@@ -308,6 +316,19 @@ __global__ void reduce_slices_kernel(const double2* __restrict__ partial, int n_
     }
     U[i] = make_double2(x, y);
   }
+}
+
+// The R ring lives in dynamic shared memory above the 48 KB default (with the static arrays
+// ~59 KB per block, two blocks per SM); the limit is raised on the current device per call.
+static kr_status bessel_ring_attribute(const char* where) {
+  cudaError_t e = cudaFuncSetAttribute(bessel_partial_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kRingBytes);
+  if (e != cudaSuccess) {
+    set_last_error(where, e);
+    return KR_ERR_CUDA;
+  }
+  return KR_OK;
 }
 
 struct BesselPlan {
@@ -444,7 +465,9 @@ extern "C" kr_status kr_bessel_sum(const double* R, const double* p, const doubl
   if (!workspace || workspace_bytes < b.partial_bytes) return KR_ERR_WORKSPACE;
   double2* partial = reinterpret_cast<double2*>(workspace);
   dim3 grid(b.n_slices, (n_r + kBsR - 1) / kBsR, (n_w + kBsW - 1) / kBsW);
-  bessel_partial_kernel<<<grid, dim3(kBsW, kBsR), 0, st>>>(
+  kr_status a = bessel_ring_attribute("kr_bessel_sum");
+  if (a != KR_OK) return a;
+  bessel_partial_kernel<<<grid, dim3(kBsW, kBsR), kRingBytes, st>>>(
       reinterpret_cast<const double2*>(R), p, pw, n_p, dp, omega, n_w, offsets, n_r,
       b.p_per_slice, partial);
   kr_status s = check_launch("kr_bessel_sum: partial");
@@ -597,7 +620,9 @@ extern "C" kr_status kr_bessel_sum_noalloc(const double* R, const double* p, con
   n_slices = (n_p + p_per_slice - 1) / p_per_slice;
   double2* partial = reinterpret_cast<double2*>(scratch);
   dim3 grid(n_slices, (n_r + kBsR - 1) / kBsR, (n_w + kBsW - 1) / kBsW);
-  bessel_partial_kernel<<<grid, dim3(kBsW, kBsR), 0, st>>>(
+  s = bessel_ring_attribute("kr_bessel_sum_noalloc");
+  if (s != KR_OK) return s;
+  bessel_partial_kernel<<<grid, dim3(kBsW, kBsR), kRingBytes, st>>>(
       reinterpret_cast<const double2*>(R), p, pw, n_p, dp, omega, n_w, offsets, n_r,
       p_per_slice, partial);
   s = check_launch("kr_bessel_sum_noalloc: partial");
