@@ -105,36 +105,13 @@ def _grid_inputs(T, nw, np_slow, p_max, gamma, source_func, offsets_bytes):
     return _GRID_CACHE[key]
 
 
-def compute_gather_gpu(model: LayerModel, offsets, T: float = 64.0, nw: int = 2048,
-                       np_slow: int = 4096, p_max: float = 1.2, gamma=None, source_func=None,
-                       free_surface: bool = False, device=None,
-                       return_reflectivity: bool = False, copy_chunks: int = 2):
-    """``(time, offsets, gather)`` exactly as ``compute_gather_gpu`` (``kennett_gather_gpu.py:169-284``).
-
-    With ``return_reflectivity=True`` the full R(p, omega + i gamma) grid is returned as a
-    fourth element.  The grid is computed in ``copy_chunks`` slowness blocks and each block is
-    copied to a pinned host buffer on a second stream while the later blocks and the Bessel
-    sum run, so the host copy overlaps the compute (two blocks hide the 268 MB copy of the
-    8192 x 2047 grid at ~57 GB/s; more blocks shorten the launches below full waves).
-    Returned arrays may share that pinned buffer with the next call; copy them to keep them.
-    """
-    dev = _dev.require_cuda(device)
-    if gamma is None:
-        gamma = np.pi / T
-    tab_h = pack_layers(model)
-    _dev.validate_table(tab_h)
-    offsets_h = np.ascontiguousarray(offsets, dtype=np.float64).reshape(-1)
-    nwm, L = nw - 1, tab_h.shape[1]
-    time, dp, off, sizes, static = _grid_inputs(float(T), int(nw), int(np_slow), float(p_max),
-                                                float(gamma), source_func, offsets_h.tobytes())
+def _enqueue_gather(dev, stage, off, sizes, L, nwm, nw, np_slow, dp, free_surface,
+                    return_reflectivity, copy_chunks):
+    """Enqueues one gather on the current stream (and the copy stream): upload of the pinned
+    staging buffer, the reflectivity grid in slowness blocks with each block's host copy,
+    the Bessel sum, the traces and their host copy.  No synchronisation; returns the pinned
+    host outputs (gather, R or None) and the device R."""
     main = torch.cuda.current_stream(dev)
-    # every input in one pinned staging buffer and one upload ahead of the first kernel, so
-    # that the kernels run back to back without host round trips between them; on a grid
-    # seen before only the layer table is packed
-    stage = _pinned((int(off[-1]),), torch.float64)
-    sn = stage.numpy()
-    sn[off[1]:] = static
-    sn[:tab_h.size] = tab_h.ravel()
     dbuf = torch.empty(stage.shape, dtype=torch.float64, device=dev)
     dbuf.copy_(stage, non_blocking=True)
     seg = [dbuf[a:a + n] for a, n in zip(off[:-1], sizes)]
@@ -161,8 +138,87 @@ def compute_gather_gpu(model: LayerModel, offsets, T: float = 64.0, nw: int = 20
     g = _dev.traces(U, nw, S=S_t, decay=dec_t)
     gh = _pinned(tuple(g.shape), g.dtype)
     gh.copy_(g, non_blocking=True)
+    return gh, Rh, R
+
+
+# Gathers replayed from CUDA graphs, keyed by grid, layer count and options: a repeated call
+# packs its layer table into the pinned staging buffer and replays one graph, instead of
+# ~15 launches and their host-side preparation.  A key is captured on its second call (the
+# first one runs eagerly and creates the cuFFT plan and kernel attributes the capture needs).
+_GRAPHS: dict = {}
+_GRAPH_SEEN: dict = {}
+_GRAPH_MAX = 2  # each graph holds its own R grid and workspaces on the device
+
+
+def _gather_graph(key, dev, enqueue_args, copy):
+    hit = _GRAPHS.get(key)
+    if hit is not None:
+        return hit
+    if key not in _GRAPH_SEEN:
+        if len(_GRAPH_SEEN) >= 64:
+            _GRAPH_SEEN.clear()
+        _GRAPH_SEEN[key] = True
+        return None
+    while len(_GRAPHS) >= _GRAPH_MAX:
+        _GRAPHS.pop(next(iter(_GRAPHS)))
+    torch.cuda.current_stream(dev).synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, capture_error_mode="relaxed"):
+        outs = _enqueue_gather(dev, *enqueue_args)
+        if copy is not None:
+            torch.cuda.current_stream(dev).wait_stream(copy)
+    _GRAPHS[key] = (graph, outs)
+    return _GRAPHS[key]
+
+
+def compute_gather_gpu(model: LayerModel, offsets, T: float = 64.0, nw: int = 2048,
+                       np_slow: int = 4096, p_max: float = 1.2, gamma=None, source_func=None,
+                       free_surface: bool = False, device=None,
+                       return_reflectivity: bool = False, copy_chunks: int = 2,
+                       use_graph: bool = True):
+    """``(time, offsets, gather)`` exactly as ``compute_gather_gpu`` (``kennett_gather_gpu.py:169-284``).
+
+    With ``return_reflectivity=True`` the full R(p, omega + i gamma) grid is returned as a
+    fourth element.  The grid is computed in ``copy_chunks`` slowness blocks and each block is
+    copied to a pinned host buffer on a second stream while the later blocks and the Bessel
+    sum run, so the host copy overlaps the compute (two blocks hide the 268 MB copy of the
+    8192 x 2047 grid at ~57 GB/s; more blocks shorten the launches below full waves).
+    With ``use_graph`` a grid seen before (same sizes, offsets, source, layer count and
+    options) replays a captured CUDA graph.  Returned arrays may share their pinned buffers
+    with the next call; copy them to keep them.
+    """
+    dev = _dev.require_cuda(device)
+    if gamma is None:
+        gamma = np.pi / T
+    tab_h = pack_layers(model)
+    _dev.validate_table(tab_h)
+    offsets_h = np.ascontiguousarray(offsets, dtype=np.float64).reshape(-1)
+    nwm, L = nw - 1, tab_h.shape[1]
+    grid_key = (float(T), int(nw), int(np_slow), float(p_max), float(gamma), source_func,
+                offsets_h.tobytes())
+    time, dp, off, sizes, static = _grid_inputs(*grid_key)
+    main = torch.cuda.current_stream(dev)
+    # every input in one pinned staging buffer and one upload ahead of the first kernel, so
+    # that the kernels run back to back without host round trips between them; on a grid
+    # seen before only the layer table is packed
+    stage = _pinned((int(off[-1]),), torch.float64)
+    sn = stage.numpy()
+    sn[off[1]:] = static
+    sn[:tab_h.size] = tab_h.ravel()
+    args = (stage, off, sizes, L, nwm, nw, int(np_slow), dp, bool(free_surface),
+            bool(return_reflectivity), int(copy_chunks))
+    copy = _copy_stream(dev) if return_reflectivity else None
+    entry = None
+    if use_graph:
+        entry = _gather_graph((dev, grid_key) + args[3:], dev, args, copy)
+    if entry is not None:
+        graph, (gh, Rh, _) = entry
+        graph.replay()
+    else:
+        gh, Rh, R = _enqueue_gather(dev, *args)
+        if return_reflectivity:
+            R.record_stream(copy)
     if return_reflectivity:
-        R.record_stream(copy)
         copy.synchronize()
     main.synchronize()
     if return_reflectivity:
