@@ -23,6 +23,12 @@ namespace kr {
 
 // ---------------- 2x2 complex matrix helpers ([[a, b], [c, d]]) ----------------
 KR_HD M2 m2(cd a, cd b, cd c, cd d) { M2 r; r.a = a; r.b = b; r.c = c; r.d = d; return r; }
+// A symmetric state as its three entries (the tape's storage) and back.
+struct S3 {
+  cd a, b, d;
+};
+KR_HD S3 s3(const M2& x) { S3 r; r.a = x.a; r.b = x.b; r.d = x.d; return r; }
+KR_HD M2 m2(const S3& x) { return m2(x.a, x.b, x.b, x.d); }
 
 // Per-layer derivative factors for one slowness.
 struct LayerD {
@@ -201,8 +207,9 @@ KR_HD void contract(const ScatTan& t, const cd cbar[10], AccT& up, AccT& lo) {
   lo.r = lo.r + s[5];
 }
 
-// Tape of one (omega, p) pair, in local memory: up to kSegMax steps of inputs and phase
-// factors (96 B per step) plus kCpMax checkpoints.  64 steps hold every model of up to 66
+// Tape of one (omega, p) pair, in local memory: up to kSegMax steps of inputs (the three
+// entries of the symmetric state) and phase factors (80 B per step) plus kCpMax
+// checkpoints.  64 steps hold every model of up to 66
 // layers outright, so those run without any recomputation; measured on an uneven batch of
 // 3-64-layer models, the larger per-thread stack (~7 KB) costs far less than recomputing
 // segments did (24 steps: 1080 ms, 40: 1049 ms, 64: 963 ms per batch).
@@ -238,16 +245,16 @@ KR_HD void jacobian_pair(int L, cd w, bool free_surface, int seg, const LayerP* 
   const int nsteps = I - 1;  // step s applies interface i = I - 2 - s
   const int ncp = nsteps > 0 ? (nsteps + seg - 1) / seg : 0;
   const int top0 = (ncp - 1) * seg;  // first step of the top segment (reversed first)
-  M2 cp[kCpMax];
-  M2 sg[kSegMax];
+  S3 cp[kCpMax];
+  S3 sg[kSegMax];
   cd sea[kSegMax], seb[kSegMax];
   M2 r = m2(coef[I - 1].rd11, coef[I - 1].rd12, coef[I - 1].rd12, coef[I - 1].rd22);
   for (int s = 0; s < nsteps; ++s) {
-    if (s % seg == 0) cp[s / seg] = r;
+    if (s % seg == 0) cp[s / seg] = s3(r);
     const int i = I - 2 - s;
     const cd ea = ph.a(i + 1), eb = ph.b(i + 1);
     if (s >= top0) {  // the top segment is recorded now and never recomputed
-      sg[s - top0] = r;
+      sg[s - top0] = s3(r);
       sea[s - top0] = ea;
       seb[s - top0] = eb;
     }
@@ -279,11 +286,11 @@ KR_HD void jacobian_pair(int L, cd w, bool free_surface, int seg, const LayerP* 
     const int s1 = s0 + seg < nsteps ? s0 + seg : nsteps;
     if (q != ncp - 1) {
       // recompute this segment's step inputs and phase factors from its checkpoint
-      M2 x = cp[q];
+      M2 x = m2(cp[q]);
       for (int s = s0; s < s1; ++s) {
         const int i = I - 2 - s;
         const cd ea = ph.a(i + 1), eb = ph.b(i + 1);
-        sg[s - s0] = x;
+        sg[s - s0] = s3(x);
         sea[s - s0] = ea;
         seb[s - s0] = eb;
         if (s + 1 < s1) x = kennett_step(x, ea, eb, coef[i]);
@@ -294,7 +301,7 @@ KR_HD void jacobian_pair(int L, cd w, bool free_surface, int seg, const LayerP* 
       const cd ea = sea[s - s0], eb = seb[s - s0];
       M2 rb;
       cd eab, ebb, cbar[10];
-      kennett_step_reverse(sg[s - s0], ea, eb, coef[i], ob, rb, eab, ebb, cbar);
+      kennett_step_reverse(m2(sg[s - s0]), ea, eb, coef[i], ob, rb, eab, ebb, cbar);
       contract(tan[i], cbar, cur, nxt);
       const LayerD& d = dlay[i + 1];
       const cd fa = eab * ea * w, fb = ebb * eb * w;
