@@ -153,7 +153,7 @@ def test_deep_models_recomputed_segments(n_sub):
         arrs[k][l] -= 2 * d
         Rm = O.reflectivity(*arrs, m.Q_alpha, m.Q_beta, p, w, True)
         fd = (Rp - Rm) / (2 * d)
-        # deep layers barely move R (their column is ~1e-6 of the largest): judge each column
+        # deep layers barely move R (their column is ~1e-6 of the largest): compare each column
         # against the Jacobian's overall scale where the finite difference is only noise
         scale = max(np.max(np.abs(fd)), 1e-4 * np.max(np.abs(J)))
         err = np.max(np.abs(J[:, k * L + l] - fd)) / scale
