@@ -64,7 +64,7 @@ def parse():
                     help="device steps only (no e2e, CPU baseline or peak probe): for ncu")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the inversion / batching / serving measurements")
-    ap.add_argument("--profile-kernel", choices=["inversion", "batch"], default=None,
+    ap.add_argument("--profile-kernel", choices=["inversion", "batch", "gmm"], default=None,
                     help="run only a small case of that workload (for ncu), no JSON line")
     return ap.parse_args()
 
@@ -892,6 +892,14 @@ def profile_case(kind):
         for _ in range(3):
             D.misfit_gradient(tab, p, w, R_obs)
             D.jacobian(tab, p, w, want_R=False)
+    elif kind == "gmm":
+        from seismicinversion_b200.earth_models import damped_gather_grid, random_layered_model
+
+        _, omd, p, _, _, _ = damped_gather_grid(64.0, 2048, 8192, 1.2)
+        tab = D.layer_table(random_layered_model(20, seed=1), dev)
+        p_t, w_t = torch.as_tensor(p, device=dev), torch.as_tensor(omd, device=dev)
+        for _ in range(2):
+            D.gmm_reflectivity(tab, p_t, w_t, True)
     else:
         from seismicinversion_b200.batch import BatchItem, ModelBatch
         from seismicinversion_b200.earth_models import uneven_batch_specs
