@@ -66,8 +66,9 @@ class _Problem:
     """Fixed data of one tau-p inversion, resident on the device."""
 
     def __init__(self, alpha_ref, beta_ref, rho_ref, thickness_ref, Q_alpha, Q_beta, p_values,
-                 omega, R_obs):
+                 omega, R_obs, free_surface: bool = False):
         self.dev = D.require_cuda()
+        self.fs = bool(free_surface)
         self.ref = [torch.as_tensor(x, dtype=_FDTYPE).detach().cpu()
                     for x in (alpha_ref, beta_ref, rho_ref, thickness_ref)]
         self.Q = [torch.as_tensor(x, dtype=_FDTYPE).detach().cpu() for x in (Q_alpha, Q_beta)]
@@ -82,12 +83,12 @@ class _Problem:
         return D.table_from_tensors(a, b, r, h, *self.Q, self.dev)
 
     def chi_grad(self, phys: np.ndarray):
-        out, _ = D.misfit_gradient(self.table(phys), self.p, self.omega, self.R_obs)
+        out, _ = D.misfit_gradient(self.table(phys), self.p, self.omega, self.R_obs, self.fs)
         out = out.cpu().numpy()
         return float(out[4 * self.L]), out[self.idx]
 
     def chi(self, phys: np.ndarray) -> float:
-        R = D.reflectivity(self.table(phys), self.p, self.omega)
+        R = D.reflectivity(self.table(phys), self.p, self.omega, self.fs)
         r = R - self.R_obs
         return float((r.real**2 + r.imag**2).sum())
 
@@ -99,33 +100,41 @@ class _Problem:
                                   self.Q[1].numpy()))
         return out
 
-    def hessian_exact(self, phys: np.ndarray, step: float = 1e-5) -> np.ndarray:
-        """Central differences of the exact adjoint gradient, all 2P perturbed models in one
-        batched launch (the batch is built on the first call and updated in place after)."""
+    # central-difference stencils of the gradient: (offsets in steps, weights); column j of H
+    # is sum_k w_k g(m + o_k d_j e_j) / d_j
+    _STENCILS = {2: ((1, -1), (0.5, -0.5)),
+                 4: ((2, 1, -1, -2), (-1.0 / 12, 8.0 / 12, -8.0 / 12, 1.0 / 12))}
+
+    def hessian_exact(self, phys: np.ndarray, step: float = 1e-5, stencil: int = 2) -> np.ndarray:
+        """Central differences of the exact adjoint gradient, all perturbed models in one
+        batched launch (the batch is built on the first call and updated in place after).
+        ``stencil`` 2 (error O(d^2): ~1e-7 relative at the default step, the LM's choice) or
+        4 (fourth order, four gradients per parameter: ~1e-10 relative)."""
         from .batch import BatchItem, ModelBatch
 
-        P = len(phys)
+        offs, wts = self._STENCILS[stencil]
+        P, K = len(phys), len(offs)
         d = step * np.maximum(np.abs(phys), 1e-3)
-        rows = np.repeat(phys[None, :], 2 * P, axis=0)
-        rows[np.arange(P), np.arange(P)] += d
-        rows[P + np.arange(P), np.arange(P)] -= d
+        rows = np.repeat(phys[None, :], K * P, axis=0)
+        for k, o in enumerate(offs):
+            rows[k * P + np.arange(P), np.arange(P)] += o * d
         models = self._models(rows)
         batch = getattr(self, "_hbatch", None)
-        if batch is None or len(batch.desc) != 2 * P:
-            items = [BatchItem(m, self.p, self.omega, gradient=True, R_obs=self.R_obs)
-                     for m in models]
+        if batch is None or len(batch.desc) != K * P:
+            items = [BatchItem(m, self.p, self.omega, gradient=True, R_obs=self.R_obs,
+                               free_surface=self.fs) for m in models]
             batch = self._hbatch = ModelBatch(items, device=self.dev)
         else:
             batch.update_layers(models)
         batch.launch()
         # every item is a gradient model with L layers: rows of 4L + 1 (gradient, chi) in order
-        rows = batch.chi_grad[:2 * P * (4 * self.L + 1)].view(2 * P, 4 * self.L + 1)
+        rows = batch.chi_grad[:K * P * (4 * self.L + 1)].view(K * P, 4 * self.L + 1)
         g = rows[:, self.idx].cpu().numpy()
-        H = (g[:P] - g[P:]).T / (2.0 * d[None, :])
+        H = sum(w * g[k * P:(k + 1) * P] for k, w in enumerate(wts)).T / d[None, :]
         return 0.5 * (H + H.T)
 
     def hessian_gn(self, phys: np.ndarray) -> np.ndarray:
-        _, J = D.jacobian(self.table(phys), self.p, self.omega, want_R=False)
+        _, J = D.jacobian(self.table(phys), self.p, self.omega, self.fs, want_R=False)
         Jp = J[:, self.idx, :]  # (n_p, P, n_w)
         H = 2.0 * torch.einsum("jaw,jbw->ab", Jp.conj(), Jp).real
         return H.cpu().numpy()

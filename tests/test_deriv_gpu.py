@@ -3,8 +3,8 @@
 References: the reference's torch.func.jacrev ``jacobian`` and ``hessian`` and its
 ``invert_taup`` run (golden vectors), plus central finite differences of the oracle.
 Tolerances: Jacobian vs jacrev 1e-10 relative (both exact derivatives); gradient vs the
-Jacobian contraction 1e-12; vs finite differences 1e-6; Hessian (central differences of the
-exact gradient) vs torch.func.hessian 1e-6.
+Jacobian contraction 1e-12; vs finite differences 1e-6; Hessian (fourth-order central
+differences of the exact gradient) vs torch.func.hessian 1e-9.
 """
 
 import numpy as np
@@ -215,7 +215,35 @@ def test_hessian_vs_reference(golden):
     a[1] *= 1.02
     H = hessian(a, t["beta"], t["rho"], t["thickness"], t["Q_alpha"], t["Q_beta"], 0.2,
                 torch.as_tensor(g["omega"]), R_obs=torch.as_tensor(g["R_obs_p0.2"]))
-    assert rel_err(H.numpy(), g["H_p0.2_alpha1x1.02"]) < 1e-6
+    assert rel_err(H.cpu().numpy(), g["H_p0.2_alpha1x1.02"]) < 1e-9
+
+
+def test_hessian_free_surface_and_step_independence():
+    """hessian() with the free surface: equal to second-order central differences of the plain
+    gradient path within their O(d^2) error, and independent of its step to 1e-9."""
+    from seismicinversion_b200.earth_models import random_layered_model
+    from seismicinversion_b200.kennett_torch import (_pack_params, hessian,
+                                                     misfit_gradient_packed, model_to_tensors)
+
+    t = model_to_tensors(random_layered_model(5, seed=8))
+    w = torch.arange(1, 97, dtype=torch.float64) * (2 * np.pi / 64.0) + 1j * (np.pi / 64)
+    args = (t["alpha"], t["beta"], t["rho"], t["thickness"], t["Q_alpha"], t["Q_beta"], 0.3, w)
+    R_obs = 0.9 * torch.as_tensor(O.reflectivity(*[x.numpy() for x in args[:6]], [0.3],
+                                                  w.numpy(), True)[0])
+    H = hessian(*args, R_obs=R_obs, free_surface=True).cpu().numpy()
+    H2 = hessian(*args, R_obs=R_obs, free_surface=True, step=2e-5).cpu().numpy()
+    assert rel_err(H, H2) < 1e-9
+    m0 = _pack_params(t["alpha"], t["beta"], t["rho"], t["thickness"]).numpy()
+    Hs = np.empty_like(H)
+    for j in range(len(m0)):
+        d = 1e-5 * max(abs(m0[j]), 1e-3)
+        mp, mm = m0.copy(), m0.copy()
+        mp[j] += d
+        mm[j] -= d
+        gp = misfit_gradient_packed(mp, *args[:6], 0.3, w, R_obs, True)[1].cpu().numpy()
+        gm = misfit_gradient_packed(mm, *args[:6], 0.3, w, R_obs, True)[1].cpu().numpy()
+        Hs[:, j] = (gp - gm) / (2 * d)
+    assert rel_err(H, 0.5 * (Hs + Hs.T)) < 1e-5
 
 
 def test_batched_exact_hessian_matches_sequential_differences():
