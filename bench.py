@@ -370,7 +370,8 @@ def bench_batched(torch, dev, reps, n_models=4096):
         else:
             items.append(BatchItem(m, p, w))
     batch = ModelBatch(items, device=dev)
-    best, times = autotune(batch, candidates=[(32, 128), (64, 128), (128, 256), (128, 512)],
+    best, times = autotune(batch, candidates=[(32, 128), (64, 128), (128, 256), (128, 512),
+                                              (128, 1024), (128, 2048)],
                            reps=1)
     batch.capture()
     st = torch.cuda.current_stream(dev)

@@ -32,7 +32,7 @@ __all__ = ["BatchItem", "ModelBatch", "autotune", "SCHEDULES"]
 #: Candidate schedules: (threads per block, frequencies per work item).  32 threads is the
 #: warp-per-pair schedule: one warp owns a (model, slowness) pair's frequency range.
 SCHEDULES = [(32, 64), (32, 128), (64, 64), (64, 128), (128, 128), (128, 256), (128, 512),
-             (64, 256)]
+             (64, 256), (128, 1024), (128, 2048)]
 
 
 @dataclass

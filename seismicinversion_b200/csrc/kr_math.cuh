@@ -90,11 +90,13 @@ KR_HD cd cexp_(cd z) {
   return mk(e * c, e * s);
 }
 
-// Complex slowness of a layer with velocity v and quality factor Q.
+// Complex slowness of a layer with velocity v and quality factor Q.  The multiply-add is an
+// explicit fma so that every kernel rounds it alike whatever nvcc's contraction decides in
+// the surrounding code (kernels that must agree bit for bit all call this).
 KR_HD cd complex_slowness(double v, double Q) {
   double q2 = 2.0 * Q;
   double q2sq = q2 * q2;
-  double den = (1.0 + q2sq) * v;
+  double den = fma(q2, q2, 1.0) * v;
   return mk(q2sq / den, q2 / den);
 }
 
