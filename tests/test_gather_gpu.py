@@ -80,6 +80,31 @@ def test_bessel_sum_random_and_ragged():
     assert torch.count_nonzero(U) == 0
 
 
+def test_bessel_sum_zeros_and_orderings():
+    """Exact zeros (p = 0 in a uniform grid, omega = 0, offset 0: J0 = 1 and zero weights),
+    a uniform grid reaching the fast Hankel path at large arguments, and the same slownesses in
+    descending order (no rotation scheme: every term on the per-term path)."""
+    from seismicinversion_b200 import device as D
+
+    rng = np.random.default_rng(9)
+    n_p, dp = 700, 1.2 / 700
+    p = np.arange(n_p) * dp  # starts at 0
+    pw = 0.5 * (1.0 + np.cos(np.pi * p / 1.2)) * p
+    om = np.r_[0.0, np.linspace(0.01, 200.0, 45)]
+    r = np.r_[0.0, 0.5, 7.0, 49.5]
+    R = rng.standard_normal((n_p, len(om))) + 1j * rng.standard_normal((n_p, len(om)))
+    taper = np.divide(pw, p, out=np.zeros_like(p), where=p > 0)
+    Uo = O.bessel_sum(R, p, om, r, dp, taper=taper)
+    U = D.bessel_sum(torch.as_tensor(R, device="cuda"), p, pw, dp, om, r).cpu().numpy()
+    assert np.isfinite(U).all()
+    assert rel_err(U, Uo) < TOL
+    assert np.all(U[:, 0] == 0)  # omega = 0
+    rev = slice(None, None, -1)
+    Ur = D.bessel_sum(torch.as_tensor(R[rev].copy(), device="cuda"), p[rev].copy(),
+                      pw[rev].copy(), dp, om, r).cpu().numpy()
+    assert rel_err(Ur, Uo) < TOL
+
+
 def test_traces_vs_numpy():
     from seismicinversion_b200 import device as D
 
