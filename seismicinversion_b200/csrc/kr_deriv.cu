@@ -270,13 +270,11 @@ static kr_status launch_sweep_v(unsigned blocks, size_t smem, cudaStream_t st, i
                                 const LayerP* lay, const LayerD* dlay, const Iface* coef,
                                 const ScatTan* tan, const double2* R_obs, double2* R, double2* J,
                                 double* partial) {
+  static SmemLimit lim;
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(deriv_sweep_kernel<GRAD, MINB>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) {
-      set_last_error("kr_deriv: smem attribute", e);
-      return KR_ERR_CUDA;
-    }
+    const kr_status a = raise_smem_limit((const void*)deriv_sweep_kernel<GRAD, MINB>, smem, lim,
+                                         "kr_deriv: smem attribute");
+    if (a != KR_OK) return a;
   }
   deriv_sweep_kernel<GRAD, MINB><<<blocks, kDerThreads, smem, st>>>(
       L, p, n_p, omega, n_w, n_wtiles, fs, seg, stage, table, lay, dlay, coef, tan, R_obs, R, J,

@@ -136,13 +136,11 @@ static kr_status launch_forward(const double* layers, int n_layers, const double
   }
   const long long blocks = (long long)n_p * ((n_wtiles + tpb - 1) / tpb);
   if (blocks > 0x7fffffffLL) return KR_ERR_TOO_LARGE;
+  static SmemLimit lim;
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(reflectivity_kernel<MINB>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) {
-      set_last_error("kr_reflectivity: smem attribute", e);
-      return KR_ERR_CUDA;
-    }
+    const kr_status a = raise_smem_limit((const void*)reflectivity_kernel<MINB>, smem, lim,
+                                         "kr_reflectivity: smem attribute");
+    if (a != KR_OK) return a;
   }
   reflectivity_kernel<MINB><<<(unsigned)blocks, kFwdThreads, smem, st>>>(
       layers, n_layers, p, n_p, reinterpret_cast<const double2*>(omega), n_w, n_wtiles, tpb,

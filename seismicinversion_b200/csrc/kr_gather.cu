@@ -319,16 +319,10 @@ __global__ void reduce_slices_kernel(const double2* __restrict__ partial, int n_
 }
 
 // The R ring lives in dynamic shared memory above the 48 KB default (with the static arrays
-// ~59 KB per block, two blocks per SM); the limit is raised on the current device per call.
+// ~59 KB per block, two blocks per SM); the limit is raised once per device.
+static SmemLimit g_ring_limit;
 static kr_status bessel_ring_attribute(const char* where) {
-  cudaError_t e = cudaFuncSetAttribute(bessel_partial_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)kRingBytes);
-  if (e != cudaSuccess) {
-    set_last_error(where, e);
-    return KR_ERR_CUDA;
-  }
-  return KR_OK;
+  return raise_smem_limit((const void*)bessel_partial_kernel, kRingBytes, g_ring_limit, where);
 }
 
 struct BesselPlan {
@@ -544,7 +538,6 @@ namespace kr {
 constexpr size_t kNoAllocScratchBytes = (size_t)16 << 20;
 static __device__ __align__(256) unsigned char g_bessel_scratch[kNoAllocScratchBytes];
 
-constexpr int kMaxDevices = 64;
 static std::mutex g_scratch_mu;
 static void* g_scratch_addr[kMaxDevices];
 

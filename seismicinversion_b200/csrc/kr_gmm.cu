@@ -281,13 +281,11 @@ extern "C" kr_status kr_gmm_reflectivity(const double* layers, int32_t n_layers,
   const bool table = phase_table_model(n_layers);
   const size_t smem = gmm_smem(n_layers, table);
   cudaStream_t st = (cudaStream_t)stream;
+  static SmemLimit lim;
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(gmm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) {
-      set_last_error("kr_gmm_reflectivity: smem attribute", e);
-      return KR_ERR_CUDA;
-    }
+    const kr_status a = raise_smem_limit((const void*)gmm_kernel, smem, lim,
+                                         "kr_gmm_reflectivity: smem attribute");
+    if (a != KR_OK) return a;
   }
   gmm_kernel<<<(unsigned)blocks, kGmmThreads, smem, st>>>(
       layers, n_layers, p, n_p, reinterpret_cast<const double2*>(omega), n_w, n_wtiles, (int)tpb,

@@ -27,6 +27,34 @@ inline bool aligned16(const void* ptr) { return ((uintptr_t)ptr & 15u) == 0; }
 void set_last_error(const char* where, cudaError_t e);
 void set_last_error_msg(const char* msg);
 
+// Raises a kernel's dynamic shared-memory limit to `bytes` on the current device, calling the
+// runtime only when the limit recorded for that device is lower: after the first call per
+// device (and larger size) a launcher makes no runtime call but the launch, so it can be
+// captured into a CUDA graph.  `lim` is the launcher's own per-kernel table (zero-initialised
+// static storage).
+constexpr int kMaxDevices = 64;
+struct SmemLimit {
+  int bytes[kMaxDevices];
+};
+inline kr_status raise_smem_limit(const void* fn, size_t bytes, SmemLimit& lim,
+                                  const char* where) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    set_last_error(where, e);
+    return KR_ERR_CUDA;
+  }
+  const bool known = dev >= 0 && dev < kMaxDevices;
+  if (known && lim.bytes[dev] >= (int)bytes) return KR_OK;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e != cudaSuccess) {
+    set_last_error(where, e);
+    return KR_ERR_CUDA;
+  }
+  if (known) lim.bytes[dev] = (int)bytes;
+  return KR_OK;
+}
+
 inline kr_status check_launch(const char* where) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
