@@ -437,6 +437,26 @@ def bench_batched(torch, dev, reps, n_models=4096):
             "graph_captured": True}
 
 
+def bench_training_data(torch, dev, n=50_000):
+    """Amortized-inference training data as the reference's ``generate_training_data``: n prior
+    samples of the default 6-layer model, 12 slownesses x 64 frequencies, written in the
+    reference's .pt layout; wall time of the whole call (sampling, batched forward launches,
+    float32 conversion, host copy, file write), after one small untimed call."""
+    from seismicinversion_b200.training_data import DataGenConfig, generate_training_data
+
+    with tempfile.TemporaryDirectory() as d:
+        generate_training_data(d, DataGenConfig(n_train=2000, n_val=0, n_test=0), device=dev)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        generate_training_data(d, DataGenConfig(n_train=n, n_val=0, n_test=0), device=dev)
+        dt = time.perf_counter() - t0
+    return {"workload": f"{n} samples, default 6-layer model prior, 12 p x 64 omega, .pt output",
+            "samples": n, "seconds": dt, "samples_per_s": n / dt,
+            "reference_published_seconds_50k": 4747.0,
+            "note": "the reference's figure (NeuralInversion/README.md, hardware not stated) "
+                    "uses its global-matrix forward; this one the Kennett kernels"}
+
+
 def bench_serving(torch, dev, rates=(100, 1000, 3000, 10000, 20000), duration=1.0,
                   max_requests=3000):
     """Serving workload: Poisson arrivals (seed 7) of requests drawn as in the batching
@@ -810,6 +830,7 @@ def run_ours(args, rank, world, local):
         extra["gmm"] = bench_gmm(torch, D, tab, p_t, w_t, R, max(args.steps, 3))
         extra["inversion"] = bench_inversion(torch, dev, max(args.steps, 3))
         extra["batched"] = bench_batched(torch, dev, max(args.steps, 2))
+        extra["training_data"] = bench_training_data(torch, dev)
         extra["serving"] = bench_serving(torch, dev)
 
     if rank == 0:
