@@ -457,6 +457,46 @@ def bench_training_data(torch, dev, n=50_000):
                     "uses its global-matrix forward; this one the Kennett kernels"}
 
 
+def bench_published_configs(torch, dev, reps=5):
+    """The configurations the reference publishes timings for (Apple Silicon, its README
+    files), run through this library's public drop-ins with host inputs and outputs; the
+    reference's figures beside each (best of ``reps`` wall times after one untimed call)."""
+    from seismicinversion_b200.earth_models import default_ocean_crust_model
+    from seismicinversion_b200.kennett_gather_gpu import compute_gather_gpu
+    from seismicinversion_b200.kennett_torch import hessian, jacobian, model_to_tensors
+
+    m = default_ocean_crust_model()
+    offs = np.arange(0.5, 50.0 + 0.25, 0.5)
+    t = model_to_tensors(m)
+    args = (t["alpha"], t["beta"], t["rho"], t["thickness"], t["Q_alpha"], t["Q_beta"], 0.2)
+
+    def best(fn):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return min(ts) * 1e3
+
+    out = {}
+    for n_p, pub in ((2048, 30.0), (4096, 60.0)):
+        ms = best(lambda: compute_gather_gpu(m, offs, T=64.0, nw=2048, np_slow=n_p))
+        out[f"gather_np{n_p}"] = {"ms": ms, "reference_published_s": pub,
+                                  "reference_setup": "compute_gather, 10-core M-series CPU"}
+    w127 = torch.as_tensor(np.arange(1, 128) * (2 * np.pi / 64))
+    ms = best(lambda: jacobian(*args, w127))
+    out["jacobian_5layer_nfreq127"] = {"ms": ms, "reference_published_ms": 89.0,
+                                       "reference_setup": "torch.func.jacrev, Apple Silicon"}
+    w31 = torch.as_tensor(np.arange(1, 32) * (2 * np.pi / 64))
+    ms = best(lambda: hessian(*args, w31))
+    out["hessian_5layer_nfreq31"] = {"ms": ms, "reference_published_ms": 70.0,
+                                     "reference_setup": "torch.func.hessian, Apple Silicon"}
+    return out
+
+
 def bench_serving(torch, dev, rates=(100, 1000, 3000, 10000, 20000), duration=1.0,
                   max_requests=3000):
     """Serving workload: Poisson arrivals (seed 7) of requests drawn as in the batching
@@ -831,6 +871,7 @@ def run_ours(args, rank, world, local):
         extra["inversion"] = bench_inversion(torch, dev, max(args.steps, 3))
         extra["batched"] = bench_batched(torch, dev, max(args.steps, 2))
         extra["training_data"] = bench_training_data(torch, dev)
+        extra["published_configs"] = bench_published_configs(torch, dev)
         extra["serving"] = bench_serving(torch, dev)
 
     if rank == 0:
