@@ -544,9 +544,14 @@ def bench_serving(torch, dev, rates=(100, 1000, 3000, 10000, 20000), duration=1.
             r.wait(120)
         del warm
     torch.cuda.synchronize()
+    import gc
+
     for lam in rates:
         n = int(min(max_requests, lam * duration))
         gaps = rng.exponential(1.0 / lam, n)
+        # the previous run's requests are garbage with reference cycles: collect them now
+        # rather than in a collection that lands inside this run
+        gc.collect()
         with KennettServer(executor=ex, hbm_budget_bytes=120 * 10**9, max_batch_requests=64,
                            max_inflight=2) as srv:
             t_start = time.perf_counter()
