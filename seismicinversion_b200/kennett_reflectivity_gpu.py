@@ -7,7 +7,6 @@ the CUDA device; there is no MPS/CPU alternative.
 
 from __future__ import annotations
 
-import numpy as np
 import torch
 
 from . import device as _dev
