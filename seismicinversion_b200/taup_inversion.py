@@ -112,12 +112,8 @@ class _Problem:
         4 (fourth order, four gradients per parameter: ~1e-10 relative)."""
         from .batch import BatchItem, ModelBatch
 
-        offs, wts = self._STENCILS[stencil]
-        P, K = len(phys), len(offs)
-        d = step * np.maximum(np.abs(phys), 1e-3)
-        rows = np.repeat(phys[None, :], K * P, axis=0)
-        for k, o in enumerate(offs):
-            rows[k * P + np.arange(P), np.arange(P)] += o * d
+        rows, d = self.stencil_rows(phys, step, stencil)
+        P, K = len(phys), len(self._STENCILS[stencil][0])
         models = self._models(rows)
         batch = getattr(self, "_hbatch", None)
         if batch is None or len(batch.desc) != K * P:
@@ -129,7 +125,25 @@ class _Problem:
         batch.launch()
         # every item is a gradient model with L layers: rows of 4L + 1 (gradient, chi) in order
         rows = batch.chi_grad[:K * P * (4 * self.L + 1)].view(K * P, 4 * self.L + 1)
-        g = rows[:, self.idx].cpu().numpy()
+        return self.stencil_hessian(rows[:, self.idx].cpu().numpy(), d, stencil)
+
+    @classmethod
+    def stencil_rows(cls, phys: np.ndarray, step: float, stencil: int):
+        """The K * P perturbed parameter rows of a stencil (block k: every parameter moved by
+        offset k times its step) and the steps d."""
+        offs = cls._STENCILS[stencil][0]
+        P = len(phys)
+        d = step * np.maximum(np.abs(phys), 1e-3)
+        rows = np.repeat(np.asarray(phys, dtype=np.float64)[None, :], len(offs) * P, axis=0)
+        for k, o in enumerate(offs):
+            rows[k * P + np.arange(P), np.arange(P)] += o * d
+        return rows, d
+
+    @classmethod
+    def stencil_hessian(cls, g: np.ndarray, d: np.ndarray, stencil: int) -> np.ndarray:
+        """Symmetrised Hessian from the gradients g (K * P rows, in stencil_rows order)."""
+        wts = cls._STENCILS[stencil][1]
+        P = len(d)
         H = sum(w * g[k * P:(k + 1) * P] for k, w in enumerate(wts)).T / d[None, :]
         return 0.5 * (H + H.T)
 
