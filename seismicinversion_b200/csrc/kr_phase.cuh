@@ -35,7 +35,7 @@ __host__ __device__ inline size_t phase_table_bytes(int n_layers, int tiles) {
 }
 
 // Which models tabulate: those whose forward-kernel block (prologue + a table of 16 tiles)
-// stays within 50 KB of shared memory, i.e. up to 33 layers.  Every kernel applies the same
+// stays within 50 KB of shared memory, i.e. up to 30 layers.  Every kernel applies the same
 // per-model rule, so a model's phases come from the same source everywhere.
 constexpr int kFwdTabTiles = 16;
 constexpr size_t kFwdTabSmemMax = 50 * 1024;

@@ -80,7 +80,7 @@ def test_gradient_is_the_adjoint_of_the_same_function():
 
 @pytest.mark.parametrize("n_sub", [1, 2, 5, 20, 40, 99])
 def test_vs_oracle_and_kennett(n_sub):
-    """Random models of 2 to 100 layers (those above 33 layers evaluate their phases
+    """Random models of 2 to 100 layers (those above 30 layers evaluate their phases
     directly), damped frequencies, both surface conditions."""
     from seismicinversion_b200 import device as D
     from seismicinversion_b200.earth_models import random_layered_model
