@@ -42,3 +42,38 @@ def test_table_accuracy_vs_scipy():
     for n in range(T.shape[1] - 1, -1, -1):
         v = v * t + T[k, n]
     assert np.max(np.abs(v - j0(x))) < 5e-16
+
+
+def _hankel_a(k):
+    num, den = 1.0, 1.0
+    for j in range(1, k + 1):
+        num *= -float((2 * j - 1) ** 2)
+        den *= 8.0 * j
+    return num / den
+
+
+def _j0_asym(x, nt):
+    """The kernel's j0_asym_scaled times its amplitude: sqrt(1 / (pi x)) (P u + Q y v) with
+    u = cos x + sin x, v = cos x - sin x, y = 1 / x and nt terms of P and Q."""
+    y = 1.0 / x
+    q = y * y
+    P = np.full_like(x, (-1.0) ** (nt - 1) * _hankel_a(2 * (nt - 1)))
+    Q = np.full_like(x, (-1.0) ** (nt - 1) * _hankel_a(2 * (nt - 1) + 1))
+    for m in range(nt - 2, -1, -1):
+        P = P * q + (-1.0) ** m * _hankel_a(2 * m)
+        Q = Q * q + (-1.0) ** m * _hankel_a(2 * m + 1)
+    c, s = np.cos(x), np.sin(x)
+    return (P * (c + s) + Q * (y * (c - s))) / np.sqrt(np.pi * x)
+
+
+def test_hankel_branch_accuracy_vs_scipy():
+    """The fast path's expansion lengths (7 / 5 / 4 / 3 / 2 terms from x = 25 / 60 / 100 / 300 /
+    3000, as in kr_gather.cu) reproduce SciPy's j0 to within 1e-15 absolute in each range."""
+    src = (CSRC / "kr_gather.cu").read_text()
+    assert ("x_first >= 3000.0 ? 2 : x_first >= 300.0 ? 3 : x_first >= 100.0 ? 4"
+            in src.replace("\n", " ").replace("  ", " ").replace("  ", " "))
+    for lo, hi, nt in ((25, 60, 7), (60, 100, 5), (100, 300, 4), (300, 3000, 3),
+                       (3000, 20000, 2)):
+        x = np.linspace(lo, hi, 200001)
+        err = np.max(np.abs(_j0_asym(x, nt) - j0(x)))
+        assert err < 1e-15, (lo, hi, nt, err)
