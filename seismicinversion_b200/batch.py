@@ -76,8 +76,9 @@ def _cat_into(out: torch.Tensor, parts):
 
 
 def _size_class(nbytes: int) -> int:
-    """Allocation size for a batch block: eight classes per power of two (<= 12.5 % slack),
-    at least 1 MiB, so that batches of similar size reuse the same cached blocks."""
+    """Allocation size for a batch block: four classes per power of two (multiples of a
+    quarter of the power of two below: at most 25 % slack), at least 1 MiB, so that batches of
+    similar size reuse the same cached blocks."""
     nbytes = max(int(nbytes), 1 << 20)
     step = 1 << max(0, (nbytes - 1).bit_length() - 3)
     return (nbytes + step - 1) // step * step
