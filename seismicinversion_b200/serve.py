@@ -71,16 +71,24 @@ class Request:
 
 
 def request_bytes(model: LayerModel, n_p: int, n_w: int, gradient: bool) -> int:
-    """Device bytes one request occupies while admitted: inputs, outputs and its share of
-    the batch plan (per-slowness coefficient blocks)."""
+    """Device bytes one request occupies while admitted, an upper bound: its inputs and outputs
+    and its share of the batch plan (per slowness: layer terms, interface coefficients and, for
+    gradients, derivative factors and coefficient tangents, each section padded to 256 B as
+    the plan lays them out, plus its pair record and work items), times 1.25 for the size-class
+    rounding of the batch's single device block.  Left out: that block's 1 MiB minimum, at most
+    1 MiB per batch in flight."""
     L = model.n_layers
     I = L - 1
+
+    def a256(x):
+        return (x + 255) // 256 * 256
+
     b = 48 * L + 8 * n_p + 16 * n_w + 16 * n_p * n_w  # layers, p, omega, R
-    coef = 96 * L + 336 * I + 512
+    coef = a256(96 * L) + a256(336 * I) + 256  # LayerP, Iface; pair record and work items
     if gradient:
         b += 16 * n_p * n_w + 8 * (4 * L + 1)  # R_obs, chi_grad
-        coef += 112 * L + 960 * I + 256
-    return int(b + n_p * coef + 64)
+        coef += a256(112 * L) + a256(960 * I)  # LayerD, ScatTan
+    return int(1.25 * (b + n_p * coef + 1024))
 
 
 class GpuBatchExecutor:

@@ -24,3 +24,34 @@ def test_size_classes():
 def test_schedules_are_valid_configurations():
     for threads, tile_w in SCHEDULES:
         assert threads in (32, 64, 128) and 32 <= tile_w <= 8192
+
+
+def test_request_bytes_bounds_the_batch_footprint():
+    """serve.request_bytes is an upper bound on a request's device footprint: its buffers and
+    its plan (kr_batch_plan_bytes, host-only, for the server's schedule) times the 1.25 slack of
+    the batch block's size class, for random model depths, grids and request kinds."""
+    import ctypes
+
+    from seismicinversion_b200 import _lib
+    from seismicinversion_b200.earth_models import random_layered_model
+    from seismicinversion_b200.serve import request_bytes
+
+    h = _lib.lib()
+    cfg = _lib.BatchConfig(128, 256, 0, 0)  # GpuBatchExecutor's schedule
+    rng = np.random.default_rng(0)
+    for t in range(200):
+        n_sub = int(rng.integers(2, 64))
+        n_p = int(rng.integers(1, 257))
+        n_w = int(rng.choice([16, 256, 512, 1024, 2048]))
+        grad = bool(rng.random() < 0.5)
+        m = random_layered_model(n_sub, seed=t)
+        L = m.n_layers
+        desc = np.zeros(1, dtype=_lib.MODEL_DESC_FIELDS)
+        desc["n_layers"], desc["n_p"], desc["n_w"] = L, n_p, n_w
+        desc["flags"] = (_lib.KR_BATCH_GRADIENT | _lib.KR_BATCH_STORE_R) if grad else 0
+        plan = h.kr_batch_plan_bytes(desc.ctypes.data, 1, ctypes.byref(cfg))
+        assert plan > 0
+        buf = 48 * L + 8 * n_p + 16 * n_w + 16 * n_p * n_w
+        if grad:
+            buf += 16 * n_p * n_w + 8 * (4 * L + 1)
+        assert request_bytes(m, n_p, n_w, grad) >= 1.25 * (buf + plan), (L, n_p, n_w, grad)
