@@ -38,3 +38,24 @@ def test_grid_inputs_cache():
     for k in range(12):
         K._grid_inputs(*args, np.array([2.0 + k]).tobytes())
     assert len(K._GRID_CACHE) <= 8
+
+
+def test_output_file_formats(tmp_path):
+    """The reference CLIs' file formats: a .npz gather with keys time / offsets / gather
+    (kennett_gather_gpu.py:429-436) and a two-column %.8e text seismogram
+    (kennett_seismogram.py:294-296)."""
+    from seismicinversion_b200.kennett_seismogram import save_seismogram_txt
+
+    rng = np.random.default_rng(1)
+    t = np.arange(16) * 0.25
+    offs = np.array([0.5, 1.0, 1.5])
+    g = rng.standard_normal((3, 16))
+    out = K.save_gather_npz(tmp_path / "gather.png", t, offs, g)
+    assert out.suffix == ".npz"
+    z = np.load(out)
+    assert sorted(z.files) == ["gather", "offsets", "time"]
+    assert np.array_equal(z["gather"], g) and np.array_equal(z["offsets"], offs)
+    s = rng.standard_normal(16)
+    save_seismogram_txt(tmp_path / "s.txt", t, s)
+    lines = (tmp_path / "s.txt").read_text().splitlines()
+    assert len(lines) == 16 and lines[1] == f"{t[1]:.8e} {s[1]:.8e}"
