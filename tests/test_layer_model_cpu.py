@@ -51,3 +51,26 @@ def test_half_space_conventions_and_layout():
         complex_slowness(0.0, 100.0)
     with pytest.raises(ValueError):
         complex_slowness(1.5, 0.0)
+
+
+@pytest.mark.parametrize("n_sub,seed", [(5, 0), (20, 1), (20, 2), (63, 3)])
+def test_random_model_generator(n_sub, seed):
+    """The seeded benchmark models: 1 km water (Vp 1.5, Vs 0, rho 1.0) over n_sub layers with
+    Vp ~ U(1.8, 5.0) increasing with depth, Vs = Vp / U(1.7, 2.0), rho = 0.31 (1000 Vp)^0.25,
+    h ~ U(0.2, 1.0), an infinite half-space, Q_alpha = 100 and Q_beta = 50; the same seed gives
+    the same model."""
+    from seismicinversion_b200.earth_models import random_layered_model
+
+    m = random_layered_model(n_sub, seed=seed)
+    assert m.n_layers == n_sub + 1
+    assert (m.alpha[0], m.beta[0], m.rho[0], m.thickness[0]) == (1.5, 0.0, 1.0, 1.0)
+    vp, vs = m.alpha[1:], m.beta[1:]
+    assert np.all(np.diff(vp) >= 0) and np.all((vp >= 1.8) & (vp <= 5.0))
+    assert np.all((vp / vs >= 1.7) & (vp / vs <= 2.0))
+    assert np.allclose(m.rho[1:], 0.31 * (1000.0 * vp) ** 0.25, rtol=0, atol=1e-15)
+    assert np.all((m.thickness[1:-1] >= 0.2) & (m.thickness[1:-1] <= 1.0))
+    assert np.isinf(m.thickness[-1])
+    assert np.all(m.Q_alpha == 100.0) and np.all(m.Q_beta == 50.0)
+    m2 = random_layered_model(n_sub, seed=seed)
+    assert all(np.array_equal(getattr(m, k), getattr(m2, k))
+               for k in ("alpha", "beta", "rho", "thickness"))
