@@ -74,3 +74,20 @@ def test_random_model_generator(n_sub, seed):
     m2 = random_layered_model(n_sub, seed=seed)
     assert all(np.array_equal(getattr(m, k), getattr(m2, k))
                for k in ("alpha", "beta", "rho", "thickness"))
+
+
+def test_uneven_batch_workload():
+    """The uneven-batching workload: total layers U{3..64}, n_omega in {256, 512, 1024, 2048}
+    with omega_k = k 2 pi / 64, n_p U{16..256} with p_j = j 0.8 / n_p; seeded."""
+    from seismicinversion_b200.earth_models import uneven_batch_specs
+
+    specs = uneven_batch_specs(512, seed=3)
+    Ls = np.array([m.n_layers for m, _, _ in specs])
+    assert Ls.min() >= 3 and Ls.max() <= 64 and len(set(Ls)) > 40
+    for m, p, w in specs[:64]:
+        assert len(w) in (256, 512, 1024, 2048)
+        assert np.allclose(w, np.arange(1, len(w) + 1) * (2 * np.pi / 64), rtol=0, atol=0)
+        assert 16 <= len(p) <= 256 and p[-1] == pytest.approx(0.8)
+        assert np.allclose(np.diff(p), 0.8 / len(p))
+    again = uneven_batch_specs(512, seed=3)
+    assert all(np.array_equal(a[0].alpha, b[0].alpha) for a, b in zip(specs, again))
