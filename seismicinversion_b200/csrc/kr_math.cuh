@@ -303,11 +303,12 @@ KR_HD Iface interface_coeffs(double p, int iface, const LayerP& up, const LayerP
 // evaluation carries such a part, and carrying one of its off-diagonals for both positions
 // turns it into error (1e-8 at large slowness).  The symmetric form has none by
 // construction and avoids forming N's entries, whose products cancel when the interface
-// determinants do: on the reference's 5-layer default model, over the 8192-slowness gather
-// grid, its worst relative error against an 80-bit evaluation of the reference's form is
-// 1.7e-10 (no free surface) and 8.1e-11 (free surface), against 8.9e-10 and 2.4e-10 for the
-// full-matrix form in double; on 21-layer models both stay near 1e-12.  ~120 FP64 operations
-// per step instead of ~190.  RRd = [[a, b], [c, d]] with c = b.
+// determinants do: on the reference's 5-layer default model, at every 64th slowness of the
+// 8192-slowness gather grid (every third frequency), its worst relative error against an
+// 80-bit evaluation of the reference's form is 1.7e-10 (no free surface) and 8.1e-11 (free
+// surface), against 8.9e-10 and 2.4e-10 for the full-matrix form in double; on 21-layer models
+// both stay near 1e-12.  ~120 FP64 operations per step instead of ~190.
+// RRd = [[a, b], [c, d]] with c = b.
 // ---------------------------------------------------------------------------------------
 struct M2 {
   cd a, b, c, d;
