@@ -13,6 +13,12 @@
  * acoustic ocean = layer 0), rho, thickness (+inf or >= 1e30 marks the half-space), Q_alpha,
  * Q_beta.  Layer 0 is the ocean, layer n_layers-1 the half-space.
  *
+ * Stream capture: the launch entry points (kr_reflectivity, kr_gmm_reflectivity,
+ * kr_bessel_sum[_noalloc], kr_traces, kr_jacobian, kr_misfit_gradient, kr_batch_launch) make
+ * no CUDA runtime call besides their launches once they have been called on that device with
+ * the same sizes (the first call raises kernel shared-memory limits, creates the cuFFT plan
+ * or looks up static scratch), so later calls can be recorded into a CUDA graph.
+ *
  * Each entry point names the reference (tmnestor/SeismicInversion) interface it replaces.
  */
 #ifndef KENNETT_B200_H
