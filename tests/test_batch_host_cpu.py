@@ -55,3 +55,46 @@ def test_request_bytes_bounds_the_batch_footprint():
         if grad:
             buf += 16 * n_p * n_w + 8 * (4 * L + 1)
         assert request_bytes(m, n_p, n_w, grad) >= 1.25 * (buf + plan), (L, n_p, n_w, grad)
+
+
+class _FakeBatch:
+    """Stands in for a ModelBatch: a signature and a schedule setter; launch time per schedule
+    comes from a table (the timing itself is patched)."""
+
+    def __init__(self, sig, costs):
+        self.sig, self.costs, self.schedule, self.set_calls = sig, costs, None, 0
+
+    def signature(self):
+        return self.sig
+
+    def set_schedule(self, sch):
+        self.schedule = tuple(sch)
+        self.set_calls += 1
+
+
+def test_autotune_picks_fastest_and_caches(tmp_path, monkeypatch):
+    import json
+
+    from seismicinversion_b200 import batch as B
+
+    monkeypatch.setattr(B, "_time_launch", lambda b, reps: b.costs[b.schedule])
+    monkeypatch.setattr(B, "_TUNE_CACHE", {})
+    costs = {(32, 128): 5.0, (128, 256): 2.0, (128, 512): 1.5, (64, 128): 3.0}
+    cache = tmp_path / "tune.json"
+    fb = _FakeBatch("sigA", costs)
+    best, times = B.autotune(fb, candidates=list(costs), cache_file=str(cache))
+    assert best == (128, 512) and fb.schedule == (128, 512) and times == costs
+    assert json.loads(cache.read_text()) == {"sigA": [128, 512]}
+    # memory cache: no timing on the second call
+    fb2 = _FakeBatch("sigA", {})
+    assert B.autotune(fb2, candidates=list(costs)) == ((128, 512), {})
+    assert fb2.schedule == (128, 512) and fb2.set_calls == 1
+    # disk cache survives a fresh process (empty memory cache)
+    monkeypatch.setattr(B, "_TUNE_CACHE", {})
+    fb3 = _FakeBatch("sigA", {})
+    assert B.autotune(fb3, cache_file=str(cache))[0] == (128, 512)
+    # a corrupt cache file is ignored and rewritten
+    cache.write_text("{not json")
+    fb4 = _FakeBatch("sigB", costs)
+    assert B.autotune(fb4, candidates=list(costs), cache_file=str(cache))[0] == (128, 512)
+    assert json.loads(cache.read_text()) == {"sigB": [128, 512]}
