@@ -50,3 +50,37 @@ def test_fourth_order_beats_second_order():
         H = _Problem.stencil_hessian(np.stack([_grad(r, A) for r in rows]), d, stencil)
         errs.append(np.abs(H - _hess(m, A)).max())
     assert errs[1] < 1e-3 * errs[0]
+
+
+class _FakeProblem:
+    """chi(m) = sum_i c_i m_i^3 with analytic gradient and Hessian (physical parameters)."""
+
+    def __init__(self, c):
+        self.c = c
+
+    def chi_grad(self, m):
+        return float(np.sum(self.c * m**3)), 3 * self.c * m**2
+
+    def hessian_exact(self, m):
+        return np.diag(6 * self.c * m)
+
+    hessian_gn = hessian_exact
+
+
+def test_log_space_gradient_and_hessian():
+    """taup_misfit_grad_hessian's chain rule to log parameters (taup_inversion.py:183-185):
+    g_log = m g and H_log = m m^T H + diag(g m), against the derivatives of chi(exp(x))."""
+    from seismicinversion_b200.taup_inversion import _chi_g_h, newton_lm_step
+
+    rng = np.random.default_rng(3)
+    c = rng.uniform(0.5, 2.0, 5)
+    x = rng.uniform(-0.5, 0.5, 5)
+    chi, g_log, H_log = _chi_g_h(_FakeProblem(c), x, "exact")
+    m = np.exp(x)
+    assert chi == pytest.approx(np.sum(c * m**3))
+    assert np.allclose(g_log, 3 * c * m**3)            # d/dx c e^{3x} = 3 c e^{3x}
+    assert np.allclose(H_log, np.diag(9 * c * m**3))   # d2/dx2 = 9 c e^{3x}
+    with pytest.raises(ValueError):
+        _chi_g_h(_FakeProblem(c), x, "newton")
+    dx = newton_lm_step(g_log, H_log, 0.1)
+    assert np.allclose((H_log + 0.1 * np.eye(5)) @ dx, -g_log)
