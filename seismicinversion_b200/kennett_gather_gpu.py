@@ -185,7 +185,8 @@ def compute_gather_gpu(model: LayerModel, offsets, T: float = 64.0, nw: int = 20
     8192 x 2047 grid at ~57 GB/s; more blocks shorten the launches below full waves).
     With ``use_graph`` a grid seen before (same sizes, offsets, source, layer count and
     options) replays a captured CUDA graph.  Returned arrays may share their pinned buffers
-    with the next call; copy them to keep them.
+    with the next call; copy them to keep them.  Calls share module-level staging buffers,
+    grid caches and graphs: callers on several threads must serialise them.
     """
     dev = _dev.require_cuda(device)
     if gamma is None:
