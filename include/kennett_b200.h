@@ -14,7 +14,8 @@
  * Q_beta.  Layer 0 is the ocean, layer n_layers-1 the half-space.
  *
  * Stream capture: the launch entry points (kr_reflectivity, kr_gmm_reflectivity,
- * kr_bessel_sum[_noalloc], kr_traces, kr_jacobian, kr_misfit_gradient, kr_batch_launch) make
+ * kr_bessel_sum[_noalloc], kr_traces, kr_jacobian, kr_misfit_gradient, kr_vjp,
+ * kr_batch_launch) make
  * no CUDA runtime call besides their launches once they have been called on that device with
  * the same sizes (the first call raises kernel shared-memory limits, creates the cuFFT plan
  * or looks up static scratch), so later calls can be recorded into a CUDA graph.
@@ -131,6 +132,27 @@ kr_status kr_misfit_gradient(const double* layers, int32_t n_layers, const doubl
                              const double* R_obs, double* R, double* chi_grad, void* workspace,
                              size_t workspace_bytes, void* stream);
 
+/* Bytes of device workspace kr_vjp needs. */
+size_t kr_vjp_workspace_bytes(int32_t n_layers, int32_t n_p, int32_t n_w);
+
+/*
+ * Vector-Jacobian product of the reflectivity for a caller's cotangent, without forming the
+ * Jacobian:  grad[k*L + l] = Re sum_{p, w} conj(gR[p][w]) * dR(p, w) / d theta  (theta as in
+ * kr_jacobian; PyTorch's convention for real inputs of a complex output).  Replaces the
+ * reverse pass of kennett_reflectivity_torch's autograd graph
+ * (Kennett_Reflectivity/kennett_torch.py:312-480) as torch.autograd.grad / backward() drive
+ * it with an arbitrary upstream gradient (taup_inversion.py:169-171).  The reverse sweep of
+ * kr_misfit_gradient seeded with conj(gR), per-layer recomputation instead of a stored tape of
+ * every (p, w, layer) intermediate; block partials reduced in a fixed order (deterministic).
+ *   gR   : device complex [n_p][n_w] cotangent
+ *   R    : device complex [n_p][n_w] output (the forward result), or NULL
+ *   grad : device float64 [4*n_layers] output
+ *   workspace : >= kr_vjp_workspace_bytes(n_layers, n_p, n_w) bytes
+ */
+kr_status kr_vjp(const double* layers, int32_t n_layers, const double* p, int32_t n_p,
+                 const double* omega, int32_t n_w, uint32_t flags, const double* gR, double* R,
+                 double* grad, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Bytes of device workspace kr_bessel_sum needs for these sizes. */
 size_t kr_bessel_sum_workspace_bytes(int32_t n_p, int32_t n_w, int32_t n_r);
 
@@ -163,7 +185,8 @@ kr_status kr_bessel_sum(const double* R, const double* p, const double* pw, int3
  * a 16 MiB file-scope device array that every GPU loading the library holds until exit.
  * Limit: n_r * n_w <= 1048576 (one slice must fit), else KR_ERR_TOO_LARGE.  No cudaMalloc,
  * cudaFree or allocating library call is made.  The first call on each device looks up the
- * array's device address (cudaGetSymbolAddress); make that first call before any stream
+ * array's device address (cudaGetSymbolAddress), and so does the first call after the
+ * device's context changed (cudaDeviceReset); make such a first call before any stream
  * capture.  All calls share the array: calls that overlap on the GPU (other streams, other
  * host threads) race and must be serialised by the caller.
  */

@@ -1,7 +1,7 @@
 // Jacobian and misfit gradient of the reflectivity with respect to every layer's
 // (alpha, beta, rho, h): the hand-written adjoint of the Kennett recursion.
 //
-// Three kernels:
+// Three kernels (JAC, GRAD and VJP modes of the sweep):
 //   deriv_layer_kernel : per (p, layer)      layer terms + derivative factors  -> workspace
 //   deriv_iface_kernel : per (p, interface)  coefficients + 10x6 tangents      -> workspace
 //   deriv_sweep_kernel : per (omega, p)      forward sweep with checkpoints every <= 64 steps, then the
@@ -9,12 +9,13 @@
 //                        checkpoint: per-layer recomputation instead of a full tape), giving
 //                        dR/d(theta) for all 4L parameters.  JAC mode writes them
 //                        (J[p][k*L + l][omega], k = alpha, beta, rho, h); GRAD mode contracts
-//                        them with the residual, 2 Re(conj(R - R_obs) dR/dtheta), and reduces
-//                        over the block in a fixed order; a last kernel adds the block
-//                        partials in order (deterministic).
+//                        them with the residual, 2 Re(conj(R - R_obs) dR/dtheta), VJP mode
+//                        with a caller's cotangent, Re(conj(gR) dR/dtheta); both reduce over
+//                        the block in a fixed order and a last kernel adds the block partials
+//                        in order (deterministic).
 // Replaces the torch autograd graph of kennett_reflectivity_torch (kennett_torch.py:312-480),
-// jacobian (:611-641) and the per-slowness gradient of taup_misfit_grad_hessian
-// (taup_inversion.py:112-187).
+// jacobian (:611-641), its reverse pass under torch.autograd.grad, and the per-slowness
+// gradient of taup_misfit_grad_hessian (taup_inversion.py:112-187).
 #include <stdlib.h>
 
 #include <type_traits>
@@ -115,14 +116,21 @@ __device__ __forceinline__ void finalize_layer(int l, int L, const AccR& acc, bo
   }
 }
 
+// Sweep modes: JAC writes dR/dtheta per (omega, p); GRAD seeds the reverse sweep with
+// 2 conj(R - R_obs) (misfit gradient, plus chi); VJP seeds it with conj(gR) for a caller's
+// cotangent gR (Re sum conj(gR) dR/dtheta, no chi).  GRAD and VJP accumulate real parts only.
+constexpr int kModeJac = 0;
+constexpr int kModeGrad = 1;
+constexpr int kModeVjp = 2;
+
 // Receives R and the per-layer derivatives of one thread's (omega, p) pair.
-template <bool GRAD>
+template <int MODE>
 struct PairSink {
-  typedef typename std::conditional<GRAD, AccR, Acc>::type AccT;
-  static constexpr bool kSeeded = GRAD;
+  typedef typename std::conditional<MODE != kModeJac, AccR, Acc>::type AccT;
+  static constexpr bool kSeeded = MODE != kModeJac;
   int L, ip, iw, n_w;
   bool valid;
-  const double2* R_obs;
+  const double2* R_obs;  // GRAD: observed R; VJP: the cotangent gR
   double2* R_out;
   double2* J;
   double* s_wacc;
@@ -131,20 +139,21 @@ struct PairSink {
     res = mk(0.0, 0.0);
     if (!valid) return mk(0.0, 0.0);
     if (R_out) R_out[(size_t)ip * n_w + iw] = make_double2(R.x, R.y);
-    if (!GRAD) return mk(1.0, 0.0);
+    if (MODE == kModeJac) return mk(1.0, 0.0);
     const double2 o = R_obs[(size_t)ip * n_w + iw];
+    if (MODE == kModeVjp) return mk(o.x, -o.y);  // conj(gR)
     res = mk(R.x - o.x, R.y - o.y);
     return mk(2.0 * res.x, -2.0 * res.y);  // 2 conj(res)
   }
   __device__ void layer(int l, const AccT& acc) {
-    if constexpr (GRAD)
+    if constexpr (MODE != kModeJac)
       finalize_layer(l, L, acc, valid, s_wacc);
     else
       finalize_layer(l, L, acc, valid, ip, iw, n_w, J);
   }
 };
 
-template <bool GRAD, int MINB>
+template <int MODE, int MINB>
 __global__ void __launch_bounds__(kDerThreads, MINB)
 deriv_sweep_kernel(int L, const double* __restrict__ p, int n_p,
                    const double2* __restrict__ omega, int n_w, int n_wtiles, int free_surface,
@@ -156,6 +165,7 @@ deriv_sweep_kernel(int L, const double* __restrict__ p, int n_p,
   // dynamic smem: [warps][4L + 1] per-warp accumulators (GRAD), then, if `stage`, this
   // block's slowness data (tangents, coefficients, layer terms, layer derivatives), then, if
   // `table`, the phase-factor table of this block's frequency tile (kr_phase.cuh)
+  constexpr bool GRAD = MODE != kModeJac;
   extern __shared__ __align__(16) double s_wacc[];
   __shared__ unsigned s_bad;
   const int ip = blockIdx.x / n_wtiles;
@@ -205,7 +215,7 @@ deriv_sweep_kernel(int L, const double* __restrict__ p, int n_p,
                1u) != 0;
   const PhaseAuto ph{use_tab, phase_at(s_ph, kPhHead + 1, valid ? iw : tile * kDerThreads, tile),
                      PhaseDirect{w, lay}};
-  PairSink<GRAD> sink;
+  PairSink<MODE> sink;
   sink.L = L;
   sink.ip = ip;
   sink.iw = iw;
@@ -231,14 +241,15 @@ deriv_sweep_kernel(int L, const double* __restrict__ p, int n_p,
   }
 }
 
-// out[k] = sum_b partial[b][k]: one block per k, fixed-shape tree (deterministic).
+// out[k] = sum_b partial[b][k] for k < gridDim.x (rows of `stride` doubles): one block per
+// k, fixed-shape tree (deterministic).
 __global__ void __launch_bounds__(256)
-reduce_partials_kernel(const double* __restrict__ partial, int n_blocks, int n,
+reduce_partials_kernel(const double* __restrict__ partial, int n_blocks, int stride,
                        double* __restrict__ out) {
   __shared__ double s[256];
   const int k = blockIdx.x;
   double t = 0.0;
-  for (int b = threadIdx.x; b < n_blocks; b += 256) t += partial[(size_t)b * n + k];
+  for (int b = threadIdx.x; b < n_blocks; b += 256) t += partial[(size_t)b * stride + k];
   s[threadIdx.x] = t;
   __syncthreads();
   for (int o = 128; o > 0; o >>= 1) {
@@ -263,7 +274,7 @@ static int deriv_minb() {
   return g_deriv_minb;
 }
 
-template <bool GRAD, int MINB>
+template <int MODE, int MINB>
 static kr_status launch_sweep_v(unsigned blocks, size_t smem, cudaStream_t st, int L,
                                 const double* p, int n_p, const double2* omega, int n_w,
                                 int n_wtiles, int fs, int seg, int stage, int table,
@@ -272,17 +283,17 @@ static kr_status launch_sweep_v(unsigned blocks, size_t smem, cudaStream_t st, i
                                 double* partial) {
   static SmemLimit lim;
   if (smem > 48 * 1024) {
-    const kr_status a = raise_smem_limit((const void*)deriv_sweep_kernel<GRAD, MINB>, smem, lim,
+    const kr_status a = raise_smem_limit((const void*)deriv_sweep_kernel<MODE, MINB>, smem, lim,
                                          "kr_deriv: smem attribute");
     if (a != KR_OK) return a;
   }
-  deriv_sweep_kernel<GRAD, MINB><<<blocks, kDerThreads, smem, st>>>(
+  deriv_sweep_kernel<MODE, MINB><<<blocks, kDerThreads, smem, st>>>(
       L, p, n_p, omega, n_w, n_wtiles, fs, seg, stage, table, lay, dlay, coef, tan, R_obs, R, J,
       partial);
   return KR_OK;
 }
 
-template <bool GRAD>
+template <int MODE>
 static kr_status launch_sweep(int minb, unsigned blocks, size_t smem, cudaStream_t st, int L,
                               const double* p, int n_p, const double2* omega, int n_w,
                               int n_wtiles, int fs, int seg, int stage, int table,
@@ -290,17 +301,18 @@ static kr_status launch_sweep(int minb, unsigned blocks, size_t smem, cudaStream
                               const ScatTan* tan, const double2* R_obs, double2* R, double2* J,
                               double* partial) {
   if (minb == 3)
-    return launch_sweep_v<GRAD, 3>(blocks, smem, st, L, p, n_p, omega, n_w, n_wtiles, fs, seg,
+    return launch_sweep_v<MODE, 3>(blocks, smem, st, L, p, n_p, omega, n_w, n_wtiles, fs, seg,
                                    stage, table, lay, dlay, coef, tan, R_obs, R, J, partial);
-  return launch_sweep_v<GRAD, 2>(blocks, smem, st, L, p, n_p, omega, n_w, n_wtiles, fs, seg,
+  return launch_sweep_v<MODE, 2>(blocks, smem, st, L, p, n_p, omega, n_w, n_wtiles, fs, seg,
                                  stage, table, lay, dlay, coef, tan, R_obs, R, J, partial);
 }
 
-template <bool GRAD>
+template <int MODE>
 static kr_status launch_deriv(const double* layers, int L, const double* p, int n_p,
                               const double* omega, int n_w, uint32_t flags, const double* R_obs,
                               double* R, double* J, double* chi_grad, void* ws, size_t ws_bytes,
                               cudaStream_t st) {
+  constexpr bool GRAD = MODE != kModeJac;
   const int n_wtiles = (n_w + kDerThreads - 1) / kDerThreads;
   const size_t n_blocks = (size_t)n_p * n_wtiles;
   if (n_blocks > 0x7fffffffULL) return KR_ERR_TOO_LARGE;
@@ -324,7 +336,7 @@ static kr_status launch_deriv(const double* layers, int L, const double* p, int 
   // kr_reflectivity, so R here is bit-identical to the forward kernel's)
   const int table = (stage && phase_table_model(L)) ? 1 : 0;
   const size_t smem = acc + (stage ? pair : 0) + (table ? phase_table_bytes(L, 1) : 0);
-  s = launch_sweep<GRAD>(deriv_minb(), (unsigned)n_blocks, smem, st, L, p, n_p,
+  s = launch_sweep<MODE>(deriv_minb(), (unsigned)n_blocks, smem, st, L, p, n_p,
                          reinterpret_cast<const double2*>(omega), n_w, n_wtiles,
                          (flags & KR_FREE_SURFACE) ? 1 : 0, seg, stage, table, w.lay, w.dlay, w.coef,
                          w.tan, reinterpret_cast<const double2*>(R_obs),
@@ -332,8 +344,10 @@ static kr_status launch_deriv(const double* layers, int L, const double* p, int 
   if (s != KR_OK) return s;
   s = check_launch("kr_deriv: sweep");
   if (s != KR_OK || !GRAD) return s;
-  const int n = 4 * L + 1;
-  reduce_partials_kernel<<<n, 256, 0, st>>>(w.partial, (int)n_blocks, n, chi_grad);
+  // GRAD: gradient then chi (4L + 1 values); VJP: the gradient only (4L)
+  const int nv = 4 * L + 1;
+  reduce_partials_kernel<<<MODE == kModeGrad ? nv : nv - 1, 256, 0, st>>>(w.partial, (int)n_blocks,
+                                                                          nv, chi_grad);
   return check_launch("kr_deriv: reduce");
 }
 
@@ -369,7 +383,7 @@ extern "C" kr_status kr_jacobian(const double* layers, int32_t n_layers, const d
   if (s != KR_OK) return s;
   if (n_p == 0 || n_w == 0) return KR_OK;
   if (!J || !aligned16(J) || (R && !aligned16(R))) return KR_ERR_INVALID_ARGUMENT;
-  return launch_deriv<false>(layers, n_layers, p, n_p, omega, n_w, flags, nullptr, R, J, nullptr,
+  return launch_deriv<kModeJac>(layers, n_layers, p, n_p, omega, n_w, flags, nullptr, R, J, nullptr,
                              workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
@@ -394,6 +408,28 @@ extern "C" kr_status kr_misfit_gradient(const double* layers, int32_t n_layers, 
     return cuda_status(e);
   }
   if (!R_obs || !aligned16(R_obs) || (R && !aligned16(R))) return KR_ERR_INVALID_ARGUMENT;
-  return launch_deriv<true>(layers, n_layers, p, n_p, omega, n_w, flags, R_obs, R, nullptr,
+  return launch_deriv<kModeGrad>(layers, n_layers, p, n_p, omega, n_w, flags, R_obs, R, nullptr,
                             chi_grad, workspace, workspace_bytes, st);
+}
+
+extern "C" size_t kr_vjp_workspace_bytes(int32_t n_layers, int32_t n_p, int32_t n_w) {
+  return kr_misfit_gradient_workspace_bytes(n_layers, n_p, n_w);
+}
+
+extern "C" kr_status kr_vjp(const double* layers, int32_t n_layers, const double* p, int32_t n_p,
+                            const double* omega, int32_t n_w, uint32_t flags, const double* gR,
+                            double* R, double* grad, void* workspace, size_t workspace_bytes,
+                            void* stream) {
+  kr_status s = deriv_args(layers, n_layers, p, n_p, omega, n_w, flags);
+  if (s != KR_OK) return s;
+  if (!grad) return KR_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (n_p == 0 || n_w == 0) {
+    cudaError_t e = cudaMemsetAsync(grad, 0, sizeof(double) * 4 * (size_t)n_layers, st);
+    if (e != cudaSuccess) set_last_error("kr_vjp: memset", e);
+    return cuda_status(e);
+  }
+  if (!gR || !aligned16(gR) || (R && !aligned16(R))) return KR_ERR_INVALID_ARGUMENT;
+  return launch_deriv<kModeVjp>(layers, n_layers, p, n_p, omega, n_w, flags, gR, R, nullptr, grad,
+                                workspace, workspace_bytes, st);
 }

@@ -539,11 +539,32 @@ constexpr size_t kNoAllocScratchBytes = (size_t)16 << 20;
 static __device__ __align__(256) unsigned char g_bessel_scratch[kNoAllocScratchBytes];
 
 static std::mutex g_scratch_mu;
-static void* g_scratch_addr[kMaxDevices];
+struct ScratchSlot {
+  void* ctx;   // the context the address belongs to
+  void* addr;  // device address of g_bessel_scratch in that context
+};
+static ScratchSlot g_scratch[kMaxDevices];
 
-// Device address of g_bessel_scratch on the current device.  The host-side symbol is only a
-// stand-in, so the address is looked up once per device (with that device current) and
-// cached.
+// cuCtxGetCurrent through the runtime's driver entry-point table (no link against libcuda).
+typedef int (*CtxGetCurrentFn)(void**);
+static CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<CtxGetCurrentFn>(f);
+  }
+  return fn;
+}
+
+// Device address of g_bessel_scratch in the current device's current context.  The
+// host-side symbol is only a stand-in, so the address is looked up (with that device
+// current) on the first call per device and again whenever the device's context has changed
+// since (cudaDeviceReset makes a new primary context, in which the array lives elsewhere).
 static kr_status scratch_address(void** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -555,17 +576,23 @@ static kr_status scratch_address(void** out) {
     set_last_error_msg("kr_bessel_sum_noalloc: device index beyond 63");
     return KR_ERR_TOO_LARGE;
   }
+  void* ctx = nullptr;
+  CtxGetCurrentFn get = ctx_get_current();
+  if (get) get(&ctx);
   std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (!g_scratch_addr[dev]) {
+  ScratchSlot& slot = g_scratch[dev];
+  if (!slot.addr || !ctx || slot.ctx != ctx) {
     void* ptr = nullptr;
     e = cudaGetSymbolAddress(&ptr, g_bessel_scratch);
     if (e != cudaSuccess || !ptr) {
       set_last_error("kr_bessel_sum_noalloc: cudaGetSymbolAddress", e);
       return KR_ERR_CUDA;
     }
-    g_scratch_addr[dev] = ptr;
+    if (!ctx && get) get(&ctx);  // the lookup made the primary context current
+    slot.addr = ptr;
+    slot.ctx = ctx;
   }
-  *out = g_scratch_addr[dev];
+  *out = slot.addr;
   return KR_OK;
 }
 

@@ -22,6 +22,7 @@ __all__ = [
     "traces",
     "jacobian",
     "misfit_gradient",
+    "vjp",
     "table_from_tensors",
     "stream_handle",
 ]
@@ -209,6 +210,36 @@ def misfit_gradient(layers: torch.Tensor, p, omega, R_obs, free_surface: bool = 
                               flags, Ro.data_ptr(), _ptr(R), out.data_ptr(), ws.data_ptr(),
                               ws_bytes, stream_handle(dev))
     _lib.check(st, "kr_misfit_gradient")
+    return out, R
+
+
+def vjp(layers: torch.Tensor, p, omega, gR, free_surface: bool = False, want_R: bool = False,
+        out: torch.Tensor | None = None):
+    """grad [4L] = Re sum_{p, w} conj(gR[p, w]) dR(p, w)/d theta on the device: ``kr_vjp``.
+
+    ``gR`` is the cotangent of R (shape (n_p, n_w), complex); theta = (alpha, beta, rho, h) of
+    every layer in the order of ``jacobian``.  Returns ``(grad, R or None)``.
+    """
+    dev = layers.device
+    L = layers.shape[1]
+    p_t = _dev_f64(p, dev).reshape(-1)
+    w_t = _dev_c128(omega, dev).reshape(-1)
+    n_p, n_w = p_t.numel(), w_t.numel()
+    g = _dev_c128(gR, dev)
+    if g.numel() != n_p * n_w:
+        raise ValueError(f"gR must have {n_p} x {n_w} values, got {tuple(g.shape)}")
+    g = g.reshape(n_p, n_w).contiguous()
+    h = _lib.lib()
+    ws_bytes = h.kr_vjp_workspace_bytes(L, n_p, n_w)
+    ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
+    R = torch.empty((n_p, n_w), dtype=torch.complex128, device=dev) if want_R else None
+    if out is None:
+        out = torch.empty(4 * L, dtype=torch.float64, device=dev)
+    flags = _lib.KR_FREE_SURFACE if free_surface else 0
+    st = h.kr_vjp(layers.data_ptr(), L, p_t.data_ptr(), n_p, w_t.data_ptr(), n_w, flags,
+                  g.data_ptr(), _ptr(R), out.data_ptr(), ws.data_ptr(), ws_bytes,
+                  stream_handle(dev))
+    _lib.check(st, "kr_vjp")
     return out, R
 
 

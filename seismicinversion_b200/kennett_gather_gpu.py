@@ -175,7 +175,7 @@ def compute_gather_gpu(model: LayerModel, offsets, T: float = 64.0, nw: int = 20
                        np_slow: int = 4096, p_max: float = 1.2, gamma=None, source_func=None,
                        free_surface: bool = False, device=None,
                        return_reflectivity: bool = False, copy_chunks: int = 2,
-                       use_graph: bool = True):
+                       use_graph: bool = True, copy_outputs: bool = True):
     """``(time, offsets, gather)`` exactly as ``compute_gather_gpu`` (``kennett_gather_gpu.py:169-284``).
 
     With ``return_reflectivity=True`` the full R(p, omega + i gamma) grid is returned as a
@@ -184,9 +184,11 @@ def compute_gather_gpu(model: LayerModel, offsets, T: float = 64.0, nw: int = 20
     sum run, so the host copy overlaps the compute (two blocks hide the 268 MB copy of the
     8192 x 2047 grid at ~57 GB/s; more blocks shorten the launches below full waves).
     With ``use_graph`` a grid seen before (same sizes, offsets, source, layer count and
-    options) replays a captured CUDA graph.  Returned arrays may share their pinned buffers
-    with the next call; copy them to keep them.  Calls share module-level staging buffers,
-    grid caches and graphs: callers on several threads must serialise them.
+    options) replays a captured CUDA graph.  Every returned array is the caller's own, as in
+    the reference.  ``copy_outputs=False`` instead returns the R grid as a view of this
+    module's pinned receive buffer (no 268 MB host copy on the 8192 x 2047 grid), valid until
+    the next call with the same grid overwrites it.  Calls share module-level staging
+    buffers, grid caches and graphs: callers on several threads must serialise them.
     """
     dev = _dev.require_cuda(device)
     if gamma is None:
@@ -223,7 +225,9 @@ def compute_gather_gpu(model: LayerModel, offsets, T: float = 64.0, nw: int = 20
         copy.synchronize()
     main.synchronize()
     if return_reflectivity:
-        return time.copy(), np.asarray(offsets), gh.numpy(), Rh.numpy()
+        Rn = Rh.numpy()
+        return (time.copy(), np.asarray(offsets), gh.numpy().copy(),
+                Rn.copy() if copy_outputs else Rn)
     return time.copy(), np.asarray(offsets), gh.numpy().copy()
 
 

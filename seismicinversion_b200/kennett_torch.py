@@ -1,11 +1,17 @@
 """Drop-in for ``Kennett_Reflectivity.kennett_torch`` (``kennett_torch.py:312-725``).
 
 ``kennett_reflectivity_torch`` keeps the reference signature and returns the same complex128
-R(omega), differentiable with respect to ``alpha, beta, rho, thickness``: the forward and its
-Jacobian come from the hand-written adjoint kernel (``kr_jacobian``), wrapped in a
-``torch.autograd.Function`` whose backward / jvp are plain tensor contractions with that
-Jacobian, so ``backward()``, ``torch.autograd.grad``, ``torch.func.jacrev`` / ``jacfwd`` /
-``vjp`` / ``jvp`` all work.  Second derivatives through the Function treat the Jacobian as
+R(omega), differentiable with respect to ``alpha, beta, rho, thickness``, through a
+``torch.autograd.Function`` over the hand-written adjoint kernels:
+
+* plain inference computes R only (``kr_reflectivity``);
+* ``backward()`` / ``torch.autograd.grad`` run the vector-Jacobian product kernel
+  (``kr_vjp``) with the upstream gradient: one reverse sweep per (p, omega) that recomputes
+  the forward layer by layer, so no Jacobian and no per-layer intermediates are stored,
+  whatever n_omega * n_p * layers;
+* ``torch.func`` transforms (``jacrev`` / ``jacfwd`` / ``vjp`` / ``jvp`` / ``vmap``) and
+  forward-mode AD get R and the Jacobian (``kr_jacobian``) and contract it with tensor
+  operations.  Second derivatives through the Function treat the Jacobian as
 constant, so ``torch.func.hessian`` of a misfit built on it gives the Gauss-Newton matrix
 2 Re(J^H J); ``hessian()`` below gives the full Hessian (fourth-order central differences of
 the exact adjoint gradient).  ``Q_alpha``, ``Q_beta``, ``p`` and ``omega`` are constants (no gradient).
@@ -42,6 +48,16 @@ def _device_for(*tensors) -> torch.device:
     return D.require_cuda()
 
 
+# How much derivative information a forward call must produce:
+#   NONE : R only (no input needs a derivative);
+#   VJP  : R only; backward() runs the adjoint kernel kr_vjp with the upstream gradient
+#          (plain torch.autograd: the Jacobian is never formed, the adjoint recomputes the
+#          forward per layer);
+#   JAC  : R and the Jacobian J [n_p, 4L, n_w] (functorch transforms -- jacrev, jacfwd,
+#          vmap, hessian -- and forward-mode AD contract J with tensor operations).
+_NONE, _VJP, _JAC = 0, 1, 2
+
+
 def _compute(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface, need_jac):
     """R (and J if ``need_jac``) for the given layer arrays, on the compute device.
 
@@ -56,57 +72,98 @@ def _compute(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surfac
     return D.reflectivity(tab, p_t, w, free_surface), None
 
 
+def _vjp(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface, gR):
+    """grad [4L] = Re sum_{p, w} conj(gR) dR/dtheta by the adjoint kernel (``kr_vjp``)."""
+    dev = _device_for(alpha, omega)
+    tab = D.table_from_tensors(alpha, beta, rho, thickness, Q_alpha, Q_beta, dev)
+    p_t = torch.as_tensor(p, dtype=_FDTYPE).detach().reshape(-1)
+    g, _ = D.vjp(tab, p_t, torch.as_tensor(omega).detach(), gR, free_surface)
+    return g
+
+
 class _KennettFunction(torch.autograd.Function):
-    """R(alpha, beta, rho, thickness) with the adjoint-kernel Jacobian as its derivative."""
+    """R(alpha, beta, rho, thickness) with the hand-written adjoint as its derivative.
+
+    Outputs ``(R, J)``; J is the Jacobian in JAC mode and an empty placeholder otherwise.
+    """
 
     @staticmethod
-    def forward(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface, need_jac):
+    def forward(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface, mode):
         R, J = _compute(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface,
-                        need_jac)
+                        mode == _JAC)
         out_dev = omega.device
-        L = alpha.shape[0]
+        scalar_p = torch.as_tensor(p).dim() == 0
+        R = R.to(out_dev)
         if J is None:
-            J = torch.zeros((R.shape[0], 4 * L, R.shape[1]), dtype=_CDTYPE, device=R.device)
-        R, J = R.to(out_dev), J.to(out_dev)
-        if torch.as_tensor(p).dim() == 0:
-            R, J = R[0], J[0]
+            J = torch.empty(0, dtype=_CDTYPE, device=out_dev)
+        else:
+            J = J.to(out_dev)
+            if scalar_p:
+                J = J[0]
+        if scalar_p:
+            R = R[0]
         return R, J
 
     @staticmethod
     def setup_context(ctx, inputs, output):
         _, J = output
         ctx.mark_non_differentiable(J)
-        ctx.save_for_backward(J)
-        ctx.save_for_forward(J)
+        ctx.mode = inputs[9]
         ctx.L = inputs[0].shape[0]
         ctx.dtypes = [x.dtype for x in inputs[:4]]
+        ctx.devices = [x.device for x in inputs[:4]]
+        ctx.free_surface = inputs[8]
+        if ctx.mode == _JAC:
+            ctx.save_for_backward(J)
+            ctx.save_for_forward(J)
+        else:
+            # VJP mode keeps the (value-only) model for the adjoint launch in backward(); real
+            # inputs as float64 (a Python float p would otherwise become float32)
+            ctx.save_for_backward(*(torch.as_tensor(x, dtype=_FDTYPE).detach() for x in inputs[:7]),
+                                  torch.as_tensor(inputs[7]).detach())
 
     @staticmethod
     def backward(ctx, gR, gJ):
-        (J,) = ctx.saved_tensors
         L = ctx.L
+        if ctx.mode == _JAC:
+            (J,) = ctx.saved_tensors
+        else:
+            args = ctx.saved_tensors
+            wrapped = torch._C._functorch.is_functorch_wrapped_tensor(gR)
+            if not wrapped and not torch.is_grad_enabled():
+                # the adjoint kernel: one reverse sweep per (p, omega), no Jacobian formed
+                g = _vjp(*args, ctx.free_surface, gR.detach())
+                return tuple(g[k * L:(k + 1) * L].to(device=ctx.devices[k], dtype=ctx.dtypes[k])
+                             for k in range(4)) + (None,) * 6
+            # a transformed or differentiable backward (vmap over cotangents,
+            # create_graph=True): contract the Jacobian with tensor operations
+            _, J = _compute(*args, ctx.free_surface, True)
+            if args[6].dim() == 0:
+                J = J[0]
+            J = J.to(gR.device)
         # d loss / d theta = Re(sum_w conj(gR[w]) J[theta, w])  (PyTorch complex convention)
         g = (gR.conj().unsqueeze(-2) * J).real.sum(-1)
         if g.dim() > 1:
             g = g.sum(-2)
-        ga, gb, gr, gh = (g[..., k * L:(k + 1) * L].to(ctx.dtypes[k]) for k in range(4))
+        ga, gb, gr, gh = (g[..., k * L:(k + 1) * L].to(device=ctx.devices[k], dtype=ctx.dtypes[k])
+                          for k in range(4))
         return ga, gb, gr, gh, None, None, None, None, None, None
 
     @staticmethod
     def vmap(info, in_dims, alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega,
-             free_surface, need_jac):
+             free_surface, mode):
         # One evaluation per batch element (each is one kernel launch over all p and omega).
         args = (alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega)
         Rs, Js = [], []
         for b in range(info.batch_size):
             sl = [x if d is None else x.select(d, b) for x, d in zip(args, in_dims[:8])]
-            R, J = _KennettFunction.apply(*sl, free_surface, need_jac)
+            R, J = _KennettFunction.apply(*sl, free_surface, mode)
             Rs.append(R)
             Js.append(J)
         return (torch.stack(Rs), torch.stack(Js)), (0, 0)
 
     @staticmethod
-    def jvp(ctx, ta, tb, tr, th, tqa, tqb, tp, tw, tfs, tneed):
+    def jvp(ctx, ta, tb, tr, th, tqa, tqb, tp, tw, tfs, tmode):
         (J,) = ctx.saved_tensors
         L = ctx.L
         parts = []
@@ -118,21 +175,28 @@ class _KennettFunction(torch.autograd.Function):
         return dR, None
 
 
-def _needs_grad(*tensors) -> bool:
-    """Whether any layer input carries reverse- or forward-mode derivative information."""
+def _derivative_mode(*tensors) -> int:
+    """JAC when a functorch transform or forward-mode AD sees the layer inputs, VJP when only
+    plain reverse-mode autograd needs their gradient, else NONE."""
+    mode = _NONE
     for t in tensors:
         if not isinstance(t, torch.Tensor):
             continue
-        if t.requires_grad and torch.is_grad_enabled():
-            return True
         if torch._C._functorch.is_functorch_wrapped_tensor(t):
-            return True
+            return _JAC
         try:
             if torch.autograd.forward_ad.unpack_dual(t).tangent is not None:
-                return True
+                return _JAC
         except RuntimeError:
             pass
-    return False
+        if t.requires_grad and torch.is_grad_enabled():
+            mode = _VJP
+    return mode
+
+
+def _needs_grad(*tensors) -> bool:
+    """Whether any layer input carries reverse- or forward-mode derivative information."""
+    return _derivative_mode(*tensors) != _NONE
 
 
 def kennett_reflectivity_torch(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega,
@@ -145,9 +209,9 @@ def kennett_reflectivity_torch(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, 
     """
     if not isinstance(omega, torch.Tensor):
         omega = torch.as_tensor(omega)
-    need = _needs_grad(alpha, beta, rho, thickness)
+    mode = _derivative_mode(alpha, beta, rho, thickness)
     R, _ = _KennettFunction.apply(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega,
-                                  bool(free_surface), need)
+                                  bool(free_surface), mode)
     return R
 
 

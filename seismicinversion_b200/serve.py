@@ -12,8 +12,11 @@ gradient requests the observed R) from any thread; each returns a ``Request`` wh
   ``n_streams`` streams, keeping up to ``max_inflight`` batches on the GPU at once, so
   requests that arrive while others run are batched into the next launch and their work
   overlaps on the device;
-* polls completion events, marks requests done (results stay on the device as tensors, in
-  the batch's buffers, until the client drops them) and returns their memory to the budget.
+* polls completion events and marks requests done.  Results stay on the device as tensors
+  (views of the batch's single device block), so the budget keeps a batch's bytes charged
+  until every request of that batch has released its results: ``Request.release()``, or
+  garbage collection of the request together with every result tensor it handed out.  A
+  client that keeps results resident therefore holds budget, exactly as it holds HBM.
 
 The executor is pluggable (``executor=``); the default runs ``ModelBatch`` on the GPU.
 Latency is measured from ``submit`` to the moment the scheduler sets ``done``.
@@ -24,6 +27,7 @@ from __future__ import annotations
 import collections
 import threading
 import time
+import weakref
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -57,6 +61,7 @@ class Request:
     result: dict | None = None
     error: BaseException | None = None
     cancelled: bool = False
+    _lease: object = None
 
     def wait(self, timeout: float | None = None) -> dict:
         if not self.done.wait(timeout):
@@ -64,6 +69,13 @@ class Request:
         if self.error is not None:
             raise self.error
         return self.result
+
+    def release(self) -> None:
+        """Drop this request's results.  Its batch's bytes return to the server's budget once
+        every request of the batch has released them (or been collected along with the result
+        tensors it handed out): the batch's results share one device block."""
+        self.result = None
+        self._lease = None
 
     @property
     def latency(self) -> float:
@@ -89,6 +101,47 @@ def request_bytes(model: LayerModel, n_p: int, n_w: int, gradient: bool) -> int:
         b += 16 * n_p * n_w + 8 * (4 * L + 1)  # R_obs, chi_grad
         coef += a256(112 * L) + a256(960 * I)  # LayerD, ScatTan
     return int(1.25 * (b + n_p * coef + 1024))
+
+
+class _Lease:
+    """Budget share of one completed batch: its requests' bytes return to the server when the
+    last reference goes (the requests' ``_lease``, the result dicts and result tensors)."""
+
+    def __init__(self, released: collections.deque, nbytes: int):
+        self.nbytes = nbytes
+        weakref.finalize(self, released.append, nbytes)
+
+
+class _Result(dict):
+    """A request's result dict; keeps its batch's lease alive while the client holds it."""
+
+    __slots__ = ("_lease",)
+
+
+def _attach(res, lease):
+    out = _Result(res)
+    out._lease = lease
+    for v in res.values():
+        try:  # tensors carry the lease too, so a result tensor alone keeps its bytes charged
+            v._kr_lease = lease
+        except AttributeError:
+            pass
+    return out
+
+
+@dataclass
+class _Record:
+    """Timing record of a finished request (the server keeps these, not the requests)."""
+
+    t_submit: float
+    t_admit: float
+    t_launched: float
+    t_done: float
+    ok: bool
+
+    @property
+    def latency(self) -> float:
+        return self.t_done - self.t_submit
 
 
 class GpuBatchExecutor:
@@ -165,6 +218,12 @@ class KennettServer:
                  max_batch_requests: int = 256, max_inflight: int = 2,
                  max_pending: int = 1_000_000, poll_interval: float = 50e-6,
                  min_batch_wait: float = 0.0, prewarm_bytes: int = 0):
+        """``executor``: runs admitted groups (default ``GpuBatchExecutor``).
+        ``hbm_budget_bytes``: device bytes of admitted and unreleased requests (see the module
+        docstring).  ``max_batch_requests``: requests per launch.  ``max_inflight``: batches on
+        the GPU at once.  ``max_pending``: waiting requests before submissions are rejected.
+        ``min_batch_wait``: seconds the first waiting request may wait for others when the GPU
+        is idle.  ``prewarm_bytes``: device bytes to reserve in the executor's pool."""
         # one more stream than batches in flight: the stream a new batch is built on has
         # always finished its previous batch, so host-side uploads never wait on the GPU
         self.executor = (executor if executor is not None
@@ -180,18 +239,16 @@ class KennettServer:
         self._pending: collections.deque[Request] = collections.deque()
         self._inflight: list[tuple[object, list[Request]]] = []
         self._used = 0
+        # bytes of released batches, appended by lease finalizers from any thread (a deque
+        # append needs no lock) and drained by the scheduler
+        self._released: collections.deque[int] = collections.deque()
         self._lock = threading.Lock()
         self._wake = threading.Condition(self._lock)
         self._stop = False
         self._next_id = 0
-        self.completed: list[Request] = []
+        self.completed: list[_Record] = []
         self.batches_launched = 0
         self.peak_bytes = 0
-        # long-lived objects (models, pools, the caller's data) move to the permanent
-        # generation so periodic collections stay short while requests stream through
-        import gc
-
-        gc.freeze()
         self._thread = threading.Thread(target=self._loop, name="kennett-server", daemon=True)
         self._thread.start()
 
@@ -255,8 +312,20 @@ class KennettServer:
     def __exit__(self, *a):
         self.close()
 
+    @property
+    def used_bytes(self) -> int:
+        """Budget held by admitted requests whose results have not been released."""
+        with self._lock:
+            self._drain_released()
+            return self._used
+
     # -- scheduler -----------------------------------------------------------------------
+    def _drain_released(self) -> None:
+        while self._released:
+            self._used -= self._released.popleft()
+
     def _admit(self) -> list[Request]:
+        self._drain_released()
         group: list[Request] = []
         while self._pending and len(group) < self.max_batch:
             r = self._pending[0]
@@ -279,12 +348,21 @@ class KennettServer:
                 except BaseException as e:  # device-side failure reported by the library
                     res, err = [None] * len(reqs), e
                 now = time.perf_counter()
+                lease = None
+                if err is None:
+                    lease = _Lease(self._released, sum(r.nbytes for r in reqs))
                 with self._lock:
                     for r, x in zip(reqs, res):
-                        r.result, r.error, r.t_done = x, err, now
-                        self._used -= r.nbytes
+                        if err is None:
+                            r.result, r._lease = _attach(x, lease), lease
+                        else:
+                            r.error = err
+                            self._used -= r.nbytes
+                        r.t_done = now
                         r.done.set()
-                        self.completed.append(r)
+                        self.completed.append(_Record(r.t_submit, r.t_admit, r.t_launched,
+                                                      r.t_done, err is None))
+                del lease, res
             else:
                 still.append((handle, reqs))
         self._inflight = still
@@ -327,7 +405,7 @@ class KennettServer:
     # -- statistics ----------------------------------------------------------------------
     def stats(self, since: float = 0.0) -> dict:
         with self._lock:
-            done = [r for r in self.completed if r.t_submit >= since and r.error is None]
+            done = [r for r in self.completed if r.t_submit >= since and r.ok]
             waiting = len(self._pending)
         if not done:
             return {"completed": 0, "waiting": waiting}

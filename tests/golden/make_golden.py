@@ -239,7 +239,9 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2 or sys.argv[1].startswith("--"):
+        sys.exit("usage: make_golden.py <reference checkout> [--training-data-only | --gmm-only]")
+    root = sys.argv[1]
     if "--training-data-only" in sys.argv:
         training_data_golden(root)
     elif "--gmm-only" in sys.argv:

@@ -207,3 +207,27 @@ def test_graph_replay_matches_eager(return_reflectivity):
             for a, b in zip(out, ref):
                 assert np.array_equal(a, b)
     assert len(K._GRAPHS) >= min(n_graphs + 1, K._GRAPH_MAX)
+
+
+def test_consecutive_calls_return_independent_arrays():
+    """Every array compute_gather_gpu returns belongs to the caller (the reference returns
+    fresh arrays): a second call on the same grid, through the replayed graph, leaves the
+    first call's R grid and gather untouched; copy_outputs=False returns the receive buffer
+    itself, which the next call overwrites."""
+    from seismicinversion_b200 import compute_gather_gpu
+    from seismicinversion_b200.earth_models import random_layered_model
+
+    offs = np.array([1.0, 4.0, 9.0])
+    kw = dict(T=32.0, nw=256, np_slow=300, p_max=1.0, free_surface=True,
+              return_reflectivity=True)
+    m1, m2 = random_layered_model(6, seed=31), random_layered_model(6, seed=32)
+    for _ in range(3):  # eager, capture, replay
+        _, _, g1, R1 = compute_gather_gpu(m1, offs, **kw)
+        keep = (g1.copy(), R1.copy())
+        _, _, g2, R2 = compute_gather_gpu(m2, offs, **kw)
+        assert np.array_equal(g1, keep[0]) and np.array_equal(R1, keep[1])
+        assert not np.array_equal(R1, R2) and not np.shares_memory(R1, R2)
+    _, _, _, V1 = compute_gather_gpu(m1, offs, copy_outputs=False, **kw)
+    v1 = V1.copy()
+    _, _, _, V2 = compute_gather_gpu(m2, offs, copy_outputs=False, **kw)
+    assert np.shares_memory(V1, V2) and np.array_equal(V2, R2) and not np.array_equal(V1, v1)

@@ -1,6 +1,7 @@
 """Host logic of the continuous-batching server with a fake executor (no GPU):
-admission by memory budget, FIFO order, rejection of requests that can never fit, queue-full
-and invalid requests, cancellation of waiting requests, bounded in-flight batches."""
+admission by memory budget (held results stay charged until released), FIFO order, rejection
+of requests that can never fit, queue-full and invalid requests, cancellation of waiting
+requests, bounded in-flight batches."""
 
 import threading
 import time
@@ -73,6 +74,7 @@ def test_budget_admission_waits_and_never_exceeds():
         reqs = [_req(srv) for _ in range(12)]
         for r in reqs:
             r.wait(10)
+            r.release()  # the client consumes each result: its bytes return to the budget
         assert srv.peak_bytes <= 3 * one
     assert all(len(g) <= 3 for g in ex.groups) and len(ex.groups) >= 4
 
@@ -114,3 +116,38 @@ def test_cancel_waiting_request():
         first.wait(5)
         assert not srv.cancel(first)
     assert [second.id] not in ex.groups
+
+
+def test_held_results_hold_budget():
+    """A completed request's bytes stay charged while its results are held (the results are
+    views of its batch's device block); release() or dropping them returns the bytes."""
+    m = random_layered_model(3, seed=0)
+    one = request_bytes(m, 4, 16, False)
+    ex = FakeExecutor(delay=0.005)
+    with KennettServer(executor=ex, hbm_budget_bytes=2 * one, max_batch_requests=1,
+                       max_inflight=2) as srv:
+        a, b = _req(srv), _req(srv)
+        a.wait(5)
+        b.wait(5)
+        assert srv.used_bytes == 2 * one
+        c = _req(srv)
+        time.sleep(0.2)
+        assert not c.done.is_set()  # waits: a and b still hold their results
+        held = a.result  # a result dict on its own keeps a's batch charged
+        a.release()
+        time.sleep(0.2)
+        assert not c.done.is_set() and srv.used_bytes == 2 * one
+        del held
+        c.wait(5)  # a's bytes came back: c was admitted
+        b.release()
+        c.release()
+    assert srv.used_bytes == 0
+
+
+def test_server_leaves_global_gc_state_alone():
+    import gc
+
+    before = gc.get_freeze_count()
+    with KennettServer(executor=FakeExecutor()) as srv:
+        _req(srv).wait(5)
+    assert gc.get_freeze_count() == before

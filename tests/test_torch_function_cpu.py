@@ -30,9 +30,26 @@ def _fake_compute(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_s
     return R, (J if need_jac else None)
 
 
+CALLS = []
+
+
+def _recording_compute(*args):
+    CALLS.append(("compute", bool(args[-1])))
+    return _fake_compute(*args)
+
+
+def _fake_vjp(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface, gR):
+    CALLS.append(("vjp", tuple(gR.shape)))
+    _, J = _fake_compute(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface, True)
+    g = gR.reshape(J.shape[0], -1).conj().unsqueeze(-2) * J
+    return g.real.sum(-1).sum(0)
+
+
 @pytest.fixture
 def fake(monkeypatch):
-    monkeypatch.setattr(KT, "_compute", _fake_compute)
+    CALLS.clear()
+    monkeypatch.setattr(KT, "_compute", _recording_compute)
+    monkeypatch.setattr(KT, "_vjp", _fake_vjp)
 
 
 def _model():
@@ -57,6 +74,43 @@ def test_backward_matches_jacobian(fake):
     g = (2 * Rf[0].conj().unsqueeze(0) * J[0]).real.sum(-1)
     for k, name in enumerate(("alpha", "beta", "rho", "thickness")):
         assert torch.allclose(t[name].grad, g[k * L:(k + 1) * L], rtol=1e-12, atol=1e-12)
+    # plain autograd: the forward formed no Jacobian and backward ran the VJP entry point
+    assert CALLS[0] == ("compute", False)
+    assert ("vjp", (8,)) in CALLS and ("compute", True) not in CALLS
+
+
+def test_inference_forms_no_jacobian(fake):
+    t = _model()
+    w = torch.arange(1, 9, dtype=torch.float64) * 0.5
+    p = torch.tensor([0.1, 0.2, 0.3], dtype=torch.float64)
+    R = KT.kennett_reflectivity_torch(**t, p=p, omega=w)
+    assert R.shape == (3, 8)
+    assert CALLS == [("compute", False)]
+    _, J = KT._KennettFunction.apply(*(t[k] for k in ("alpha", "beta", "rho", "thickness",
+                                                      "Q_alpha", "Q_beta")), p, w, False, KT._NONE)
+    assert J.numel() == 0  # no Jacobian placeholder of size n_p x 4L x n_w
+
+
+def test_vector_p_backward_and_double_backward(fake):
+    t = _model()
+    for k in ("alpha", "beta", "rho"):
+        t[k] = t[k].clone().requires_grad_(True)
+    w = torch.arange(1, 7, dtype=torch.float64) * 0.4
+    p = torch.tensor([0.1, 0.25], dtype=torch.float64)
+    R = KT.kennett_reflectivity_torch(**t, p=p, omega=w)
+    gR = torch.randn(2, 6, dtype=torch.complex128, generator=torch.Generator().manual_seed(0))
+    ga = torch.autograd.grad(R, t["alpha"], gR, retain_graph=True)[0]
+    _, J = _fake_compute(t["alpha"], t["beta"], t["rho"], t["thickness"], 0, 0, p, w, False, True)
+    L = t["alpha"].shape[0]
+    want = (gR.conj().unsqueeze(-2) * J).real.sum(-1).sum(0)[:L]
+    assert torch.allclose(ga, want, rtol=1e-12, atol=1e-12)
+    assert ("vjp", (2, 6)) in CALLS
+    # create_graph=True: backward is itself differentiable in gR (Jacobian contraction)
+    gR2 = gR.clone().requires_grad_(True)
+    ga2 = torch.autograd.grad(R, t["alpha"], gR2, create_graph=True)[0]
+    assert torch.allclose(ga2, want, rtol=1e-12, atol=1e-12)
+    (d,) = torch.autograd.grad(ga2.sum(), gR2)
+    assert torch.allclose(d, J[:, :L].sum(1), rtol=1e-12, atol=1e-12)
 
 
 def test_jacrev_jacfwd_and_gauss_newton_hessian(fake):
