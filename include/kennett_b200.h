@@ -15,7 +15,7 @@
  *
  * Stream capture: the launch entry points (kr_reflectivity, kr_gmm_reflectivity,
  * kr_bessel_sum[_noalloc], kr_traces, kr_jacobian, kr_misfit_gradient, kr_vjp,
- * kr_batch_launch) make
+ * kr_misfit_hvp, kr_jacobian_dot, kr_batch_launch) make
  * no CUDA runtime call besides their launches once they have been called on that device with
  * the same sizes (the first call raises kernel shared-memory limits, creates the cuFFT plan
  * or looks up static scratch), so later calls can be recorded into a CUDA graph.
@@ -152,6 +152,48 @@ size_t kr_vjp_workspace_bytes(int32_t n_layers, int32_t n_p, int32_t n_w);
 kr_status kr_vjp(const double* layers, int32_t n_layers, const double* p, int32_t n_p,
                  const double* omega, int32_t n_w, uint32_t flags, const double* gR, double* R,
                  double* grad, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Bytes of device workspace kr_misfit_hvp needs for n_dir directions. */
+size_t kr_misfit_hvp_workspace_bytes(int32_t n_layers, int32_t n_p, int32_t n_w, int32_t n_dir);
+
+/*
+ * Exact Hessian-vector products of the misfit chi = sum_{p, w} |R - R_obs|^2:
+ *   HV[d][j] = sum_i (d^2 chi / d theta_j d theta_i) V[d][i],   d = 0 .. n_dir-1,
+ * theta = (alpha_l, beta_l, rho_l, h_l) in the order of kr_jacobian (index k*L + l).
+ * Replaces torch.func.hessian of the reference's misfit (Kennett_Reflectivity/
+ * taup_inversion.py:177, kennett_torch.py:644-684): the tangent of the adjoint -- the
+ * forward sweep, the seed 2 conj(R - R_obs) and the reverse sweep of kr_misfit_gradient
+ * carried in dual numbers along each direction, with second derivatives of the interface
+ * coefficients from nested dual numbers -- so no step size enters.  One launch for all
+ * directions; block partials reduced in a fixed order (deterministic).
+ *   R_obs : device complex [n_p][n_w];  V : device float64 [n_dir][4*n_layers]
+ *   HV    : device float64 [n_dir][4*n_layers] output
+ *   workspace : >= kr_misfit_hvp_workspace_bytes(n_layers, n_p, n_w, n_dir) bytes
+ * Limits: n_dir <= 65535, n_layers <= 258 (KR_ERR_TOO_LARGE).
+ */
+kr_status kr_misfit_hvp(const double* layers, int32_t n_layers, const double* p, int32_t n_p,
+                        const double* omega, int32_t n_w, uint32_t flags, const double* R_obs,
+                        const double* V, int32_t n_dir, double* HV, void* workspace,
+                        size_t workspace_bytes, void* stream);
+
+/* Bytes of device workspace kr_jacobian_dot needs for n_dir directions. */
+size_t kr_jacobian_dot_workspace_bytes(int32_t n_layers, int32_t n_p, int32_t n_w,
+                                       int32_t n_dir);
+
+/*
+ * Directional derivatives of the Jacobian: Jdot[d][j][k*L + l][w] = sum_i
+ * (d^2 R(p_j, w) / d theta_{k*L+l} d theta_i) V[d][i] (complex), the second derivative of
+ * the reflectivity along each direction.  Replaces the forward-over-reverse derivative that
+ * torch.func.hessian takes through kennett_reflectivity_torch (kennett_torch.py:644-684), so
+ * that a Hessian built on the differentiable forward is exact rather than Gauss-Newton.
+ * Same method and limits as kr_misfit_hvp (seed 1 instead of the misfit's).
+ *   V    : device float64 [n_dir][4*n_layers]
+ *   Jdot : device complex [n_dir][n_p][4*n_layers][n_w] output
+ */
+kr_status kr_jacobian_dot(const double* layers, int32_t n_layers, const double* p, int32_t n_p,
+                          const double* omega, int32_t n_w, uint32_t flags, const double* V,
+                          int32_t n_dir, double* Jdot, void* workspace, size_t workspace_bytes,
+                          void* stream);
 
 /* Bytes of device workspace kr_bessel_sum needs for these sizes. */
 size_t kr_bessel_sum_workspace_bytes(int32_t n_p, int32_t n_w, int32_t n_r);

@@ -60,6 +60,12 @@ _SIGNATURES = {
                                   _size_t, _vp]),
     "kr_vjp_workspace_bytes": (_size_t, [_i32, _i32, _i32]),
     "kr_vjp": (_i32, [_vp, _i32, _vp, _i32, _vp, _i32, _u32, _vp, _vp, _vp, _vp, _size_t, _vp]),
+    "kr_misfit_hvp_workspace_bytes": (_size_t, [_i32, _i32, _i32, _i32]),
+    "kr_misfit_hvp": (_i32, [_vp, _i32, _vp, _i32, _vp, _i32, _u32, _vp, _vp, _i32, _vp, _vp,
+                             _size_t, _vp]),
+    "kr_jacobian_dot_workspace_bytes": (_size_t, [_i32, _i32, _i32, _i32]),
+    "kr_jacobian_dot": (_i32, [_vp, _i32, _vp, _i32, _vp, _i32, _u32, _vp, _i32, _vp, _vp,
+                               _size_t, _vp]),
     "kr_bessel_sum_workspace_bytes": (_size_t, [_i32, _i32, _i32]),
     "kr_bessel_sum": (_i32, [_vp, _vp, _vp, _i32, ctypes.c_double, _vp, _i32, _vp, _i32, _vp,
                              _vp, _size_t, _vp]),

@@ -23,6 +23,8 @@ __all__ = [
     "jacobian",
     "misfit_gradient",
     "vjp",
+    "misfit_hvp",
+    "jacobian_dot",
     "table_from_tensors",
     "stream_handle",
 ]
@@ -241,6 +243,72 @@ def vjp(layers: torch.Tensor, p, omega, gR, free_surface: bool = False, want_R: 
                   stream_handle(dev))
     _lib.check(st, "kr_vjp")
     return out, R
+
+
+# Directions per launch of the second-derivative kernels: bounds their per-direction
+# workspace (coefficients with tangents, about 1.6 KB per (direction, slowness, interface)).
+_HVP_WS_MAX = 1 << 30
+
+
+def _dir_chunks(per_dir_bytes: int, n_dir: int) -> int:
+    return max(1, min(n_dir, _HVP_WS_MAX // max(per_dir_bytes, 1)))
+
+
+def misfit_hvp(layers: torch.Tensor, p, omega, R_obs, V, free_surface: bool = False):
+    """Exact H V of chi = sum |R - R_obs|^2 for directions V [n_dir, 4L]: ``kr_misfit_hvp``.
+
+    Returns HV [n_dir, 4L] float64 on the device (theta order of ``jacobian``).
+    """
+    dev = layers.device
+    L = layers.shape[1]
+    p_t = _dev_f64(p, dev).reshape(-1)
+    w_t = _dev_c128(omega, dev).reshape(-1)
+    n_p, n_w = p_t.numel(), w_t.numel()
+    Ro = _dev_c128(R_obs, dev).reshape(n_p, n_w).contiguous()
+    Vt = _dev_f64(V, dev).reshape(-1, 4 * L).contiguous()
+    n_dir = Vt.shape[0]
+    out = torch.empty((n_dir, 4 * L), dtype=torch.float64, device=dev)
+    h = _lib.lib()
+    flags = _lib.KR_FREE_SURFACE if free_surface else 0
+    one = h.kr_misfit_hvp_workspace_bytes(L, n_p, n_w, 1)
+    step = _dir_chunks(one, n_dir)
+    for d0 in range(0, n_dir, step):
+        nd = min(step, n_dir - d0)
+        ws_bytes = h.kr_misfit_hvp_workspace_bytes(L, n_p, n_w, nd)
+        ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
+        st = h.kr_misfit_hvp(layers.data_ptr(), L, p_t.data_ptr(), n_p, w_t.data_ptr(), n_w, flags,
+                             Ro.data_ptr(), Vt[d0:].data_ptr(), nd, out[d0:].data_ptr(),
+                             ws.data_ptr(), ws_bytes, stream_handle(dev))
+        _lib.check(st, "kr_misfit_hvp")
+    return out
+
+
+def jacobian_dot(layers: torch.Tensor, p, omega, V, free_surface: bool = False):
+    """d/dv of the Jacobian for directions V [n_dir, 4L]: ``kr_jacobian_dot``.
+
+    Returns Jdot [n_dir, n_p, 4L, n_w] complex128 on the device.
+    """
+    dev = layers.device
+    L = layers.shape[1]
+    p_t = _dev_f64(p, dev).reshape(-1)
+    w_t = _dev_c128(omega, dev).reshape(-1)
+    n_p, n_w = p_t.numel(), w_t.numel()
+    Vt = _dev_f64(V, dev).reshape(-1, 4 * L).contiguous()
+    n_dir = Vt.shape[0]
+    out = torch.empty((n_dir, n_p, 4 * L, n_w), dtype=torch.complex128, device=dev)
+    h = _lib.lib()
+    flags = _lib.KR_FREE_SURFACE if free_surface else 0
+    one = h.kr_jacobian_dot_workspace_bytes(L, n_p, n_w, 1)
+    step = _dir_chunks(one, n_dir)
+    for d0 in range(0, n_dir, step):
+        nd = min(step, n_dir - d0)
+        ws_bytes = h.kr_jacobian_dot_workspace_bytes(L, n_p, n_w, nd)
+        ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
+        st = h.kr_jacobian_dot(layers.data_ptr(), L, p_t.data_ptr(), n_p, w_t.data_ptr(), n_w,
+                               flags, Vt[d0:].data_ptr(), nd, out[d0:].data_ptr(), ws.data_ptr(),
+                               ws_bytes, stream_handle(dev))
+        _lib.check(st, "kr_jacobian_dot")
+    return out
 
 
 def table_from_tensors(alpha, beta, rho, thickness, Q_alpha, Q_beta, device) -> torch.Tensor:

@@ -11,10 +11,14 @@ R(omega), differentiable with respect to ``alpha, beta, rho, thickness``, throug
   whatever n_omega * n_p * layers;
 * ``torch.func`` transforms (``jacrev`` / ``jacfwd`` / ``vjp`` / ``jvp`` / ``vmap``) and
   forward-mode AD get R and the Jacobian (``kr_jacobian``) and contract it with tensor
-  operations.  Second derivatives through the Function treat the Jacobian as
-constant, so ``torch.func.hessian`` of a misfit built on it gives the Gauss-Newton matrix
-2 Re(J^H J); ``hessian()`` below gives the full Hessian (fourth-order central differences of
-the exact adjoint gradient).  ``Q_alpha``, ``Q_beta``, ``p`` and ``omega`` are constants (no gradient).
+  operations.  The Jacobian is itself differentiable: its tangent is the second derivative
+  of R along the input tangent (``kr_jacobian_dot``, the tangent of the adjoint), so
+  ``torch.func.hessian`` of a misfit built on the Function -- forward over reverse, as the
+  reference's ``hessian`` and ``invert_taup`` take it -- is the exact Hessian, and reverse
+  over reverse contracts the full second-derivative tensor.  ``hessian()`` below gives the
+  exact Hessian of the misfit in one launch.
+
+``Q_alpha``, ``Q_beta``, ``p`` and ``omega`` are constants (no gradient).
 
 Inputs may live on the CPU (as in the reference) or on a CUDA device; the result is returned
 on ``omega``'s device.
@@ -72,6 +76,21 @@ def _compute(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surfac
     return D.reflectivity(tab, p_t, w, free_surface), None
 
 
+def _jacobian_dot(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface, V):
+    """d/dv of the Jacobian for directions V [n_dir, 4L]: [n_dir, n_p, 4L, n_w] complex on the
+    compute device (``kr_jacobian_dot``, the tangent of the adjoint)."""
+    dev = _device_for(alpha, omega)
+    tab = D.table_from_tensors(alpha, beta, rho, thickness, Q_alpha, Q_beta, dev)
+    p_t = torch.as_tensor(p, dtype=_FDTYPE).detach().reshape(-1)
+    return D.jacobian_dot(tab, p_t, torch.as_tensor(omega).detach(), V, free_surface)
+
+
+def _second_derivatives(args, free_surface, L):
+    """d^2 R / d theta_m d theta_k for every m: [4L, n_p, 4L, n_w] (one launch over the basis)."""
+    V = torch.eye(4 * L, dtype=_FDTYPE)
+    return _jacobian_dot(*args, free_surface, V)
+
+
 def _vjp(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface, gR):
     """grad [4L] = Re sum_{p, w} conj(gR) dR/dtheta by the adjoint kernel (``kr_vjp``)."""
     dev = _device_for(alpha, omega)
@@ -79,6 +98,12 @@ def _vjp(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface, g
     p_t = torch.as_tensor(p, dtype=_FDTYPE).detach().reshape(-1)
     g, _ = D.vjp(tab, p_t, torch.as_tensor(omega).detach(), gR, free_surface)
     return g
+
+
+def _split(g, L, ctx):
+    """Per-parameter slices of a [..., 4L] gradient on the inputs' devices and dtypes."""
+    return tuple(g[..., k * L:(k + 1) * L].to(device=ctx.devices[k], dtype=ctx.dtypes[k])
+                 for k in range(4)) + (None,) * 6
 
 
 class _KennettFunction(torch.autograd.Function):
@@ -107,47 +132,68 @@ class _KennettFunction(torch.autograd.Function):
     @staticmethod
     def setup_context(ctx, inputs, output):
         _, J = output
-        ctx.mark_non_differentiable(J)
         ctx.mode = inputs[9]
         ctx.L = inputs[0].shape[0]
         ctx.dtypes = [x.dtype for x in inputs[:4]]
         ctx.devices = [x.device for x in inputs[:4]]
         ctx.free_surface = inputs[8]
+        ctx.scalar_p = torch.as_tensor(inputs[6]).dim() == 0
+        # the layer inputs themselves (a differentiable backward re-enters through them) and
+        # the constants as float64 (a Python float p would otherwise become float32)
+        layer = [torch.as_tensor(x) for x in inputs[:4]]
+        const = [torch.as_tensor(x, dtype=_FDTYPE).detach() for x in inputs[4:7]]
+        const.append(torch.as_tensor(inputs[7]).detach())
         if ctx.mode == _JAC:
-            ctx.save_for_backward(J)
-            ctx.save_for_forward(J)
+            # J is differentiable: its tangent (jvp) is the second derivative along the input
+            # tangent, so forward over reverse (torch.func.hessian) is exact
+            ctx.save_for_backward(J, *layer, *const)
+            ctx.save_for_forward(J, *layer, *const)
         else:
-            # VJP mode keeps the (value-only) model for the adjoint launch in backward(); real
-            # inputs as float64 (a Python float p would otherwise become float32)
-            ctx.save_for_backward(*(torch.as_tensor(x, dtype=_FDTYPE).detach() for x in inputs[:7]),
-                                  torch.as_tensor(inputs[7]).detach())
+            ctx.mark_non_differentiable(J)
+            ctx.save_for_backward(*layer, *const)
+
+    @staticmethod
+    def _model(saved):
+        """Value-only model arguments (alpha .. omega) from the saved tensors."""
+        return [x.detach().to(_FDTYPE) for x in saved[:4]] + list(saved[4:8])
 
     @staticmethod
     def backward(ctx, gR, gJ):
         L = ctx.L
         if ctx.mode == _JAC:
-            (J,) = ctx.saved_tensors
+            J, *saved = ctx.saved_tensors
+            args = _KennettFunction._model(saved)
         else:
-            args = ctx.saved_tensors
+            saved = ctx.saved_tensors
+            args = _KennettFunction._model(saved)
             wrapped = torch._C._functorch.is_functorch_wrapped_tensor(gR)
             if not wrapped and not torch.is_grad_enabled():
                 # the adjoint kernel: one reverse sweep per (p, omega), no Jacobian formed
-                g = _vjp(*args, ctx.free_surface, gR.detach())
-                return tuple(g[k * L:(k + 1) * L].to(device=ctx.devices[k], dtype=ctx.dtypes[k])
-                             for k in range(4)) + (None,) * 6
-            # a transformed or differentiable backward (vmap over cotangents,
-            # create_graph=True): contract the Jacobian with tensor operations
-            _, J = _compute(*args, ctx.free_surface, True)
-            if args[6].dim() == 0:
-                J = J[0]
+                return _split(_vjp(*args, ctx.free_surface, gR.detach()), L, ctx)
+            if torch.is_grad_enabled() and not wrapped:
+                # a differentiable backward (create_graph=True): the Jacobian as a
+                # differentiable function of the layer inputs (JAC mode), so that a second
+                # backward sees second derivatives
+                _, J = _KennettFunction.apply(*saved[:8], ctx.free_surface, _JAC)
+            else:
+                # a transformed backward (vmap over cotangents): contract the Jacobian with
+                # tensor operations
+                _, J = _compute(*args, ctx.free_surface, True)
+                if ctx.scalar_p:
+                    J = J[0]
             J = J.to(gR.device)
         # d loss / d theta = Re(sum_w conj(gR[w]) J[theta, w])  (PyTorch complex convention)
         g = (gR.conj().unsqueeze(-2) * J).real.sum(-1)
         if g.dim() > 1:
             g = g.sum(-2)
-        ga, gb, gr, gh = (g[..., k * L:(k + 1) * L].to(device=ctx.devices[k], dtype=ctx.dtypes[k])
-                          for k in range(4))
-        return ga, gb, gr, gh, None, None, None, None, None, None
+        if ctx.mode == _JAC and gJ is not None:
+            # reverse over reverse: sum conj(gJ) d^2 R / d theta_m d theta_k over k, p, omega
+            T = _second_derivatives(args, ctx.free_surface, L).to(gJ.device)
+            if ctx.scalar_p:
+                T = T[:, 0]
+            g2 = (gJ.conj().unsqueeze(0) * T).real
+            g = g + g2.reshape(4 * L, -1).sum(-1)
+        return _split(g, L, ctx)
 
     @staticmethod
     def vmap(info, in_dims, alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega,
@@ -164,15 +210,27 @@ class _KennettFunction(torch.autograd.Function):
 
     @staticmethod
     def jvp(ctx, ta, tb, tr, th, tqa, tqb, tp, tw, tfs, tmode):
-        (J,) = ctx.saved_tensors
+        J, *saved = ctx.saved_tensors
+        args = _KennettFunction._model(saved)
         L = ctx.L
         parts = []
         for t in (ta, tb, tr, th):
             parts.append(torch.zeros(L, dtype=_FDTYPE, device=J.device) if t is None
                          else t.to(device=J.device, dtype=_FDTYPE))
-        t = torch.cat(parts).to(_CDTYPE)
-        dR = (J * t.unsqueeze(-1)).sum(-2)
-        return dR, None
+        v = torch.cat(parts)
+        dR = (J * v.to(_CDTYPE).unsqueeze(-1)).sum(-2)
+        if torch._C._functorch.is_functorch_wrapped_tensor(v):
+            # a batch of tangents (jacfwd, hessian): contract the second-derivative tensor with
+            # tensor operations, which the transform batches
+            T = _second_derivatives(args, ctx.free_surface, L).to(J.device)
+            if ctx.scalar_p:
+                T = T[:, 0]
+            dJ = (T * v.to(_CDTYPE).reshape((4 * L,) + (1,) * (T.dim() - 1))).sum(0)
+        else:
+            dJ = _jacobian_dot(*args, ctx.free_surface, v.detach().reshape(1, -1))[0].to(J.device)
+            if ctx.scalar_p:
+                dJ = dJ[0]
+        return dR, dJ
 
 
 def _derivative_mode(*tensors) -> int:
@@ -302,13 +360,13 @@ def misfit_gradient_packed(params, alpha, beta, rho, thickness, Q_alpha, Q_beta,
 
 
 def hessian(alpha, beta, rho, thickness, Q_alpha, Q_beta, p: float, omega, R_obs=None,
-            free_surface: bool = False, step: float = 1e-5) -> torch.Tensor:
+            free_surface: bool = False) -> torch.Tensor:
     """Hessian of chi = ||R - R_obs||^2 over the packed parameters (``kennett_torch.py:644-684``).
 
-    Column j is the fourth-order central difference of the exact adjoint gradient with a
-    relative step ``step`` in m_j (the 4P perturbed gradients run as one batched launch); the
-    result is symmetrised.  Agrees with the reference's torch.func.hessian to ~1e-10 relative.
-    Returned on ``omega``'s device as float64 (n_params, n_params).
+    Exact: column j is H e_j from the tangent-of-adjoint kernel (``kr_misfit_hvp``, all
+    columns in one launch; forward-mode dual numbers through the adjoint, no step size), the
+    second derivative the reference's torch.func.hessian takes by reverse over reverse.
+    Returned on ``omega``'s device as float64 (n_params, n_params), symmetrised.
     """
     from .taup_inversion import _Problem
 
@@ -319,7 +377,7 @@ def hessian(alpha, beta, rho, thickness, Q_alpha, Q_beta, p: float, omega, R_obs
                         for x in (alpha, beta, rho, thickness)))
     prob = _Problem(alpha, beta, rho, thickness, Q_alpha, Q_beta, [float(p)], omega,
                     torch.as_tensor(R_obs).reshape(1, -1), free_surface=free_surface)
-    H = prob.hessian_exact(m0.numpy(), step=step, stencil=4)
+    H = prob.hessian_exact(m0.numpy())
     return torch.as_tensor(H, dtype=_FDTYPE).to(omega.device)
 
 

@@ -5,10 +5,10 @@
 0.01 max|diag H|, accept -> lambda / 2 (floor 1e-15), reject -> lambda * 5, at most 10 trials,
 stop on ||g|| < tol or relative misfit change < tol) in lockstep.  Per iteration:
 
-* the misfit gradients of all K current points (and, for ``hessian="exact"``, of the 2P
-  perturbed points of every inversion, central differences of the exact adjoint gradient)
-  are one batched adjoint launch (``kr_batch_launch``); the Gauss-Newton Hessian
-  2 Re(J^H J) uses one ``kr_jacobian`` launch per inversion;
+* the misfit gradients of all K current points are one batched adjoint launch
+  (``kr_batch_launch``); the exact Hessian (``hessian="exact"``) is one tangent-of-adjoint
+  launch per inversion (``kr_misfit_hvp``, every packed direction at once), the Gauss-Newton
+  Hessian 2 Re(J^H J) one ``kr_jacobian`` launch per inversion;
 * the log transform, the damping initialisation, the K damped (H + lambda I) solves
   (batched ``torch.linalg.solve``), the trial points and their layer tables are device
   tensor operations;
@@ -72,8 +72,7 @@ class _Tables:
 def invert_taup_batch(true_models: list[LayerModel], p_values, nfreq: int = 64,
                       perturbation: float = 0.15, max_iter: int = 100,
                       seeds: list[int] | None = None, tol: float = 1e-8,
-                      hessian: str = "gauss-newton", initial_params=None,
-                      step: float = 1e-5) -> list[InversionResult]:
+                      hessian: str = "gauss-newton", initial_params=None) -> list[InversionResult]:
     """K concurrent Newton-LM tau-p inversions; returns one ``InversionResult`` each.
 
     ``seeds`` (default 42 for every inversion) and ``initial_params`` (list of packed physical
@@ -118,7 +117,7 @@ def invert_taup_batch(true_models: list[LayerModel], p_values, nfreq: int = 64,
 
     # batches built once (shapes fixed); their layer buffers are rewritten on the device
     exact = hessian == "exact"
-    per = 2 * P + 1 if exact else 1
+    per = 1
     owner_g = torch.arange(K, device=dev).repeat_interleave(per)
     obs = [R_obs[k] for k in range(K)]  # one object per inversion: its items share one copy
     items = [BatchItem(true_models[k], p_t, w_c, gradient=True, R_obs=obs[k])
@@ -128,29 +127,23 @@ def invert_taup_batch(true_models: list[LayerModel], p_values, nfreq: int = 64,
     owner_f = torch.arange(K, device=dev)
     nv = 4 * L + 1
 
+    basis = torch.zeros((P, 4 * L), dtype=_F, device=dev)
+    basis[torch.arange(P), torch.as_tensor(idx)] = 1.0
+
     def grad_and_hessian(x_phys):
-        if exact:
-            d = step * torch.clamp(x_phys.abs(), min=1e-3)  # [K, P]
-            eye = torch.eye(P, dtype=_F, device=dev)
-            pts = torch.cat([x_phys[:, None, :],
-                             x_phys[:, None, :] + d[:, :, None] * eye,
-                             x_phys[:, None, :] - d[:, :, None] * eye], dim=1).reshape(-1, P)
-        else:
-            pts = x_phys
-        gbatch.layers.view(-1, 6, L).copy_(tables(pts, owner_g))
+        gbatch.layers.view(-1, 6, L).copy_(tables(x_phys, owner_g))
         gbatch.launch()
         rows = gbatch.chi_grad[:len(items) * nv].view(K, per, nv)
         chi = rows[:, 0, 4 * L]
         g = rows[:, 0, :4 * L][:, idx]
-        if exact:
-            gp = rows[:, 1:P + 1, :4 * L][:, :, idx]
-            gm = rows[:, P + 1:, :4 * L][:, :, idx]
-            H = ((gp - gm) / (2.0 * d[:, :, None])).transpose(1, 2)
-            H = 0.5 * (H + H.transpose(1, 2))
-        else:
-            tabs = tables(x_phys, owner_f)
-            H = torch.empty((K, P, P), dtype=_F, device=dev)
-            for k in range(K):
+        tabs = tables(x_phys, owner_f)
+        H = torch.empty((K, P, P), dtype=_F, device=dev)
+        for k in range(K):
+            if exact:  # H e_j for every packed j: one tangent-of-adjoint launch
+                HV = D.misfit_hvp(tabs[k].contiguous(), p_t, w_c, R_obs[k], basis)
+                Hk = HV[:, idx]
+                H[k] = 0.5 * (Hk + Hk.T)
+            else:
                 _, J = D.jacobian(tabs[k].contiguous(), p_t, w_c, want_R=False)
                 Jp = J[:, idx, :]
                 H[k] = 2.0 * torch.einsum("jaw,jbw->ab", Jp.conj(), Jp).real

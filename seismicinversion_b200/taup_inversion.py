@@ -7,9 +7,9 @@ lambda0 = 0.01 max|diag H|, accept -> lambda / 2, reject -> lambda * 5, <= 10 tr
 all slownesses are one launch of the adjoint kernel (``kr_misfit_gradient``) instead of a
 per-slowness autograd pass, and the Hessian is either
 
-* ``hessian="exact"`` (default): central differences of the exact adjoint gradient
-  (the 2P perturbed models are one batched gradient launch, ~1e-8 relative), standing in
-  for the reference's ``torch.func.hessian``; or
+* ``hessian="exact"`` (default): the exact Hessian, as the reference's
+  ``torch.func.hessian`` gives it, from one launch of the tangent-of-adjoint kernel
+  (``kr_misfit_hvp``: H e_j for every packed parameter j, no step size); or
 * ``hessian="gauss-newton"``: 2 Re(J^H J) from one ``kr_jacobian`` launch.
 
 The LaTeX / TikZ / plotting writers of the reference module are presentation, not compute,
@@ -105,11 +105,25 @@ class _Problem:
     _STENCILS = {2: ((1, -1), (0.5, -0.5)),
                  4: ((2, 1, -1, -2), (-1.0 / 12, 8.0 / 12, -8.0 / 12, 1.0 / 12))}
 
-    def hessian_exact(self, phys: np.ndarray, step: float = 1e-5, stencil: int = 2) -> np.ndarray:
+    def basis(self) -> torch.Tensor:
+        """Unit directions of the packed parameters in the full [4L] parameter space."""
+        P = len(self.idx)
+        V = torch.zeros((P, 4 * self.L), dtype=_FDTYPE, device=self.dev)
+        V[torch.arange(P), torch.as_tensor(self.idx)] = 1.0
+        return V
+
+    def hessian_exact(self, phys: np.ndarray) -> np.ndarray:
+        """The exact Hessian over the packed parameters: H e_j for every j from one launch of
+        the tangent-of-adjoint kernel (kr_misfit_hvp), symmetrised."""
+        HV = D.misfit_hvp(self.table(phys), self.p, self.omega, self.R_obs, self.basis(), self.fs)
+        H = HV[:, self.idx].cpu().numpy()
+        return 0.5 * (H + H.T)
+
+    def hessian_fd(self, phys: np.ndarray, step: float = 1e-5, stencil: int = 2) -> np.ndarray:
         """Central differences of the exact adjoint gradient, all perturbed models in one
         batched launch (the batch is built on the first call and updated in place after).
-        ``stencil`` 2 (error O(d^2): ~1e-7 relative at the default step, the LM's choice) or
-        4 (fourth order, four gradients per parameter: ~1e-10 relative)."""
+        ``stencil`` 2 (error O(d^2): ~1e-7 relative at the default step) or 4 (fourth order,
+        four gradients per parameter: ~1e-10 relative).  A cross-check of hessian_exact."""
         from .batch import BatchItem, ModelBatch
 
         rows, d = self.stencil_rows(phys, step, stencil)

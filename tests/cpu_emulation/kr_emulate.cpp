@@ -76,3 +76,75 @@ extern "C" void emu_jacobian(const double* tab, int L, const double* p, int n_p,
     }
   }
 }
+
+// ---- second derivatives (kr_hvp.cuh): the per-pair dual-number code the hvp kernels run ----
+#include "../../seismicinversion_b200/csrc/kr_hvp.cuh"
+
+namespace {
+struct HostDualSink {
+  int L, nw, k, mode;  // mode 0: misfit H v (seed 2 conj(R - R_obs)), 1: d/dv of dR/dtheta
+  cd robs;
+  double* hv;   // [4L] accumulated H v (mode 0)
+  double* jd;   // [4L][nw] complex for this slowness (mode 1)
+  DC reflectivity(const DC& R) {
+    if (mode == 1) return dc(mk(1.0, 0.0));
+    const cd r = R.v - robs;
+    return dc(mk(2.0 * r.x, -2.0 * r.y), mk(2.0 * R.t.x, -2.0 * R.t.y));
+  }
+  void layer(int l, const AccD& a) {
+    const DC v[4] = {a.a, a.b, a.r, a.h};
+    for (int q = 0; q < 4; ++q) {
+      if (mode == 0) {
+        hv[q * L + l] += v[q].t.x;
+      } else {
+        jd[2 * ((size_t)(q * L + l) * nw + k)] = v[q].t.x;
+        jd[2 * ((size_t)(q * L + l) * nw + k) + 1] = v[q].t.y;
+      }
+    }
+  }
+};
+}  // namespace
+
+// mode 0: hv[4L] += H v of chi = sum |R - R_obs|^2 (R_obs [n_p][nw] complex);
+// mode 1: jd [n_p][4L][nw] complex = d/dv of dR/dtheta.  v: [4L] direction.
+extern "C" void emu_hvp(const double* tab, int L, const double* p, int n_p, const double* w,
+                        int nw, int fs, const double* v, int mode, const double* R_obs,
+                        double* hv, double* jd) {
+  static LayerP lay[512];
+  static LayerD dlay[512];
+  static LayerD2 d2[512];
+  static LayerV lv[512];
+  static Iface f[512];
+  static IfS<DC> ifs[512];
+  static ScatTan t[512], tt[512];
+  const int I = L - 1;
+  for (int q = 0; q < 4 * L && mode == 0; ++q) hv[q] = 0.0;
+  for (int j = 0; j < n_p; ++j) {
+    for (int l = 0; l < L; ++l) {
+      lay[l] = layer_terms(tab, L, l, p[j]);
+      dlay[l] = layer_derivs(tab, L, l, p[j], lay[l]);
+      d2[l] = layer_derivs2(tab, L, l, lay[l], dlay[l]);
+      const double vl[4] = {v[l], v[L + l], v[2 * L + l], v[3 * L + l]};
+      lv[l] = layer_dot(tab, L, l, lay[l], dlay[l], d2[l], vl);
+    }
+    for (int i = 0; i < I; ++i) {
+      f[i] = interface_coeffs(p[j], i, lay[i], lay[i + 1]);
+      interface_tangents(p[j], i, lay[i], dlay[i], lay[i + 1], dlay[i + 1], t[i]);
+      IfS<DC> c;
+      interface_dot(p[j], i, lv[i], lv[i + 1], c, tt[i]);
+      ifs[i] = iface_dual(f[i], c);
+    }
+    for (int k = 0; k < nw; ++k) {
+      HostDualSink s;
+      s.L = L;
+      s.nw = nw;
+      s.k = k;
+      s.mode = mode;
+      s.robs = mode == 0 ? mk(R_obs[2 * ((size_t)j * nw + k)], R_obs[2 * ((size_t)j * nw + k) + 1])
+                         : mk(0.0, 0.0);
+      s.hv = hv;
+      s.jd = mode == 1 ? jd + 2 * (size_t)j * 4 * L * nw : nullptr;
+      hvp_pair(L, mk(w[2 * k], w[2 * k + 1]), fs != 0, lv, ifs, t, tt, s);
+    }
+  }
+}

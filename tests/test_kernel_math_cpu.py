@@ -265,3 +265,81 @@ def test_symmetric_step_diverse_models(emu, reference_form):
                                     .max(axis=1) / den).max())
     assert worst_kernel < 5e-11, (worst_kernel, worst_ref)
     assert worst_kernel <= worst_ref, (worst_kernel, worst_ref)
+
+
+@pytest.fixture(scope="module")
+def emu_hvp(emu, tmp_path_factory):
+    import glob
+
+    so = sorted(glob.glob(str(tmp_path_factory.getbasetemp() / "emu*" / "libkr_emulate.so")))[-1]
+    lib = ctypes.CDLL(so)
+
+    def run(tab, p, omega, fs, v, mode, R_obs=None):
+        tab = np.ascontiguousarray(tab, dtype=np.float64)
+        L = tab.shape[1]
+        p = np.ascontiguousarray(np.atleast_1d(p), dtype=np.float64)
+        w = np.ascontiguousarray(np.asarray(omega, dtype=np.complex128))
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        Ro = np.ascontiguousarray(np.zeros((len(p), len(w)), complex) if R_obs is None else R_obs)
+        hv = np.zeros(4 * L)
+        jd = np.zeros((len(p), 4 * L, len(w)), dtype=np.complex128)
+        lib.emu_hvp(ctypes.c_void_p(tab.ctypes.data), L, ctypes.c_void_p(p.ctypes.data), len(p),
+                    ctypes.c_void_p(w.ctypes.data), len(w), int(fs), ctypes.c_void_p(v.ctypes.data),
+                    int(mode), ctypes.c_void_p(Ro.ctypes.data), ctypes.c_void_p(hv.ctypes.data),
+                    ctypes.c_void_p(jd.ctypes.data))
+        return hv, jd
+
+    return run
+
+
+@pytest.mark.parametrize("n_sub", [4, 9, 45])
+def test_tangent_of_adjoint_vs_differences(emu_jac, emu_hvp, n_sub):
+    """The dual-number sweep of kr_hvp.cuh (the code the second-derivative kernels run):
+    d/dv of the Jacobian and the misfit Hessian-vector product H v against central
+    differences of the emulated adjoint along v, with and without free surface, for 5, 10 and
+    47 layers (the last over two checkpointed tape segments).  Tolerance 1e-7 (the differences'
+    own truncation and rounding)."""
+    from seismicinversion_b200.earth_models import random_layered_model
+    from seismicinversion_b200.layer_model import pack_layers
+
+    m = random_layered_model(n_sub, seed=3)
+    tab = np.ascontiguousarray(pack_layers(m))
+    L = tab.shape[1]
+    tab[3, -1] = 1e30
+    p = np.array([0.1, 0.35, 0.7])
+    w = np.arange(1, 13 if n_sub > 20 else 41) * (2 * np.pi / 64) + 1j * np.pi / 64
+    rng = np.random.default_rng(n_sub)
+
+    def jac(t, fs):
+        from seismicinversion_b200.layer_model import LayerModel
+
+        mm = LayerModel(*[t[k].copy() for k in range(6)])
+        return emu_jac(mm, p, w, fs)
+
+    for fs in (False, True):
+        v = rng.standard_normal(4 * L) * np.concatenate([tab[0], tab[1], tab[2],
+                                                         np.r_[tab[3, :-1], 0.0]])
+        v[L] = 0.0  # the ocean's beta
+
+        def shifted(s):
+            t = tab.copy()
+            t[0] += s * v[:L]
+            t[1] += s * v[L:2 * L]
+            t[2] += s * v[2 * L:3 * L]
+            t[3, :-1] += s * v[3 * L:4 * L - 1]
+            return t
+
+        eps = 1e-6
+        fd_J = (jac(shifted(eps), fs)[1] - jac(shifted(-eps), fs)[1]) / (2 * eps)
+        _, jd = emu_hvp(tab, p, w, fs, v, 1)
+        assert rel_err(jd, fd_J) < 1e-7
+        R0 = jac(tab, fs)[0]
+        Ro = R0 * 0.9 + 0.01
+
+        def grad(t):
+            R, J = jac(t, fs)
+            return (2 * np.conj(R - Ro)[:, None, :] * J).real.sum((0, 2))
+
+        fd_g = (grad(shifted(eps)) - grad(shifted(-eps))) / (2 * eps)
+        hv, _ = emu_hvp(tab, p, w, fs, v, 0, Ro)
+        assert rel_err(hv, fd_g) < 1e-7

@@ -1,9 +1,10 @@
 """Autograd / torch.func plumbing of the kennett_reflectivity_torch Function, on the CPU.
 
-The device computation is replaced by an analytic stand-in with a known Jacobian (test-only
-monkeypatch of ``_compute``), so the routing of gradients, jacrev / jacfwd, vjp / jvp and the
-Gauss-Newton behaviour of torch.func.hessian are checked without a GPU.  The GPU tests check
-the real kernel through the same Function.
+The device computation is replaced by an analytic stand-in with known first and second
+derivatives (test-only monkeypatches of ``_compute``, ``_vjp`` and ``_jacobian_dot``), so the
+routing of gradients, jacrev / jacfwd, vjp / jvp and the exactness of torch.func.hessian
+(forward over reverse) and torch.autograd.functional.hessian (reverse over reverse) are
+checked without a GPU.  The GPU tests check the real kernels through the same Function.
 """
 
 import numpy as np
@@ -45,11 +46,28 @@ def _fake_vjp(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surfa
     return g.real.sum(-1).sum(0)
 
 
+def _fake_jacobian_dot(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface, V):
+    # d/dv of J[k L + l] = 2 c[k, l] x_k[l]  is  2 c[k, l] v[k L + l]
+    CALLS.append(("jdot", int(V.shape[0])))
+    L = torch.as_tensor(alpha).shape[0]
+    w = torch.as_tensor(omega).detach().to(torch.complex128)
+    p_t = torch.as_tensor(p, dtype=torch.float64).reshape(-1)
+    V = torch.as_tensor(V, dtype=torch.float64).reshape(-1, 4 * L)
+    out = torch.zeros((V.shape[0], p_t.numel(), 4 * L, w.numel()), dtype=torch.complex128)
+    for j, pj in enumerate(p_t):
+        for k in range(4):
+            for l in range(L):
+                c = torch.exp(1j * w * (0.1 * (l + 1) + 0.01 * k)) * (1 + pj)
+                out[:, j, k * L + l] = 2 * c * V[:, k * L + l, None]
+    return out
+
+
 @pytest.fixture
 def fake(monkeypatch):
     CALLS.clear()
     monkeypatch.setattr(KT, "_compute", _recording_compute)
     monkeypatch.setattr(KT, "_vjp", _fake_vjp)
+    monkeypatch.setattr(KT, "_jacobian_dot", _fake_jacobian_dot)
 
 
 def _model():
@@ -113,7 +131,7 @@ def test_vector_p_backward_and_double_backward(fake):
     assert torch.allclose(d, J[:, :L].sum(1), rtol=1e-12, atol=1e-12)
 
 
-def test_jacrev_jacfwd_and_gauss_newton_hessian(fake):
+def test_jacrev_jacfwd_and_exact_hessians(fake):
     t = _model()
     w = torch.arange(1, 6, dtype=torch.float64) * 0.3
     m0 = KT._pack_params(t["alpha"], t["beta"], t["rho"], t["thickness"])
@@ -122,10 +140,11 @@ def test_jacrev_jacfwd_and_gauss_newton_hessian(fake):
         a, b, r, h = KT._unpack_params(m, t["alpha"], t["beta"], t["rho"], t["thickness"])
         return KT.kennett_reflectivity_torch(a, b, r, h, t["Q_alpha"], t["Q_beta"], 0.3, w)
 
-    _, J = _fake_compute(*KT._unpack_params(m0, t["alpha"], t["beta"], t["rho"], t["thickness"]),
-                         0, 0, 0.3, w, False, True)
+    full = KT._unpack_params(m0, t["alpha"], t["beta"], t["rho"], t["thickness"])
+    R0, J = _fake_compute(*full, 0, 0, 0.3, w, False, True)
     L = t["alpha"].shape[0]
-    Jp = J[0][KT.packed_index(L)].T  # (nw, P)
+    idx = KT.packed_index(L)
+    Jp = J[0][idx].T  # (nw, P)
     Jr = torch.func.jacrev(lambda m: f(m).real)(m0) + 1j * torch.func.jacrev(lambda m: f(m).imag)(m0)
     assert torch.allclose(Jr, Jp, rtol=1e-12, atol=1e-12)
     Jf = torch.func.jacfwd(lambda m: torch.view_as_real(f(m)))(m0)
@@ -136,6 +155,17 @@ def test_jacrev_jacfwd_and_gauss_newton_hessian(fake):
         r = f(m) - R_obs
         return (r.real**2 + r.imag**2).sum()
 
-    H = torch.func.hessian(chi)(m0)
-    H_gn = 2 * (Jp.conj().T @ Jp).real
-    assert torch.allclose(H, H_gn, rtol=1e-10, atol=1e-10)
+    # exact: 2 Re(J^H J) + 2 Re sum conj(res) d^2 R, with d^2 R / dm_a^2 = 2 c_a (diagonal)
+    res = R0[0] - R_obs
+    d2 = torch.stack([_fake_jacobian_dot(*full, 0, 0, 0.3, w, False,
+                                         torch.eye(4 * L, dtype=torch.float64)[[i]])[0, 0, i]
+                      for i in idx])  # (P, nw)
+    H_exact = 2 * (Jp.conj().T @ Jp).real + torch.diag(2 * (res.conj() * d2).real.sum(-1))
+    H = torch.func.hessian(chi)(m0)  # forward over reverse, as the reference takes it
+    assert torch.allclose(H, H_exact, rtol=1e-10, atol=1e-10)
+    assert not torch.allclose(H, 2 * (Jp.conj().T @ Jp).real, rtol=1e-6, atol=1e-6)
+    # reverse over reverse through plain autograd (double backward)
+    H2 = torch.autograd.functional.hessian(chi, m0)
+    assert torch.allclose(H2, H_exact, rtol=1e-10, atol=1e-10)
+    H3 = torch.func.jacrev(torch.func.jacrev(chi))(m0)
+    assert torch.allclose(H3, H_exact, rtol=1e-10, atol=1e-10)
