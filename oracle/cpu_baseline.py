@@ -83,3 +83,39 @@ class GatherBaseline:
     def close(self):
         self.pool.close()
         self.pool.join()
+
+
+def _refl_chunk(args):
+    layers, p, omega, fs = args
+    return O.reflectivity(*layers, p, omega, fs)
+
+
+class ReflectivityPool:
+    """The oracle's reflectivity over a slowness grid, split into slowness chunks across a
+    ``spawn`` process pool (test infrastructure: full-size parity checks of the batched and
+    served paths, and CPU baselines of those workloads)."""
+
+    def __init__(self, workers=None):
+        self.workers = workers or len(os.sched_getaffinity(0))
+        self.pool = mp.get_context("spawn").Pool(self.workers, initializer=_init_worker)
+
+    def reflectivity(self, model, p, omega, free_surface=False):
+        layers = tuple(np.asarray(getattr(model, k), dtype=np.float64) for k in
+                       ("alpha", "beta", "rho", "thickness", "Q_alpha", "Q_beta"))
+        p = np.asarray(p, dtype=np.float64)
+        omega = np.asarray(omega, dtype=np.complex128)
+        n = max(1, min(len(p), 2 * self.workers))
+        chunks = [c for c in np.array_split(p, n) if len(c)]
+        res = self.pool.map(_refl_chunk, [(layers, c, omega, free_surface) for c in chunks],
+                            chunksize=1)
+        return np.concatenate(res, axis=0)
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -87,6 +87,91 @@ def gmm_golden(ref_root: str) -> None:
     np.savez_compressed(HERE / "gmm_reflectivity.npz", **out)
 
 
+def c2_derivs_golden(ref_root: str) -> None:
+    """The tau-p inversion workload's derivatives at its own frequency count: 21-layer model
+    (seed 2), start = true * exp(0.1 N(0, 1)) (seed 2), omega_k = k 2 pi / 64 (k = 1..1024),
+    jacrev Jacobians at 4 of the 64 slownesses and the misfit gradient (autograd.grad, as
+    taup_misfit_grad_hessian takes it) over those 4 slownesses."""
+    sys.path.insert(0, ref_root)
+    import torch
+    from Kennett_Reflectivity.kennett_torch import (
+        _pack_params,
+        _unpack_params,
+        jacobian,
+        kennett_reflectivity_torch,
+        model_to_tensors,
+    )
+    from Kennett_Reflectivity.layer_model import LayerModel
+
+    from seismicinversion_b200.earth_models import random_layered_model
+
+    torch.set_num_threads(max(1, os.cpu_count() or 1))
+    true = random_layered_model(20, seed=2)
+    start = random_layered_model(20, seed=2)
+    rng = np.random.default_rng(2)
+    for name in ("alpha", "beta", "rho"):
+        getattr(start, name)[1:] *= np.exp(0.1 * rng.standard_normal(20))
+    start.thickness[1:-1] *= np.exp(0.1 * rng.standard_normal(19))
+
+    def tens(m):
+        return model_to_tensors(LayerModel.from_arrays(m.alpha, m.beta, m.rho, m.thickness,
+                                                       m.Q_alpha, m.Q_beta))
+
+    tt, ts = tens(true), tens(start)
+    om = torch.arange(1, 1025, dtype=torch.float64) * (2 * np.pi / 64.0)
+    p_all = np.linspace(0.05, 0.6, 64)
+    sel = np.array([0, 21, 42, 63])
+    out = {f"start_{k}": v for k, v in _model_arrays(start).items()}
+    out.update({f"true_{k}": v for k, v in _model_arrays(true).items()})
+    out["p"], out["omega"] = p_all[sel], om.numpy()
+    m0 = _pack_params(ts["alpha"], ts["beta"], ts["rho"], ts["thickness"]).detach()
+    grad = torch.zeros_like(m0)
+    chi = 0.0
+    for k, p in enumerate(p_all[sel]):
+        J = jacobian(ts["alpha"], ts["beta"], ts["rho"], ts["thickness"], ts["Q_alpha"],
+                     ts["Q_beta"], float(p), om)
+        out[f"J_{k}"] = J.detach().numpy()
+        R_obs = kennett_reflectivity_torch(**tt, p=float(p), omega=om).detach()
+        out[f"R_obs_{k}"] = R_obs.numpy()
+        m = m0.clone().requires_grad_(True)
+        a, b, r, h = _unpack_params(m, ts["alpha"], ts["beta"], ts["rho"], ts["thickness"])
+        R = kennett_reflectivity_torch(a, b, r, h, ts["Q_alpha"], ts["Q_beta"], float(p), om)
+        res = R - R_obs
+        misfit = (res.real**2 + res.imag**2).sum()
+        (g,) = torch.autograd.grad(misfit, m)
+        grad += g
+        chi += float(misfit)
+    out["grad"], out["chi"] = grad.numpy(), chi
+    np.savez_compressed(HERE / "derivs_c2_1024.npz", **out)
+
+
+def c2_inversion_golden(ref_root: str) -> None:
+    """The reference's own invert_taup on the tau-p inversion workload: 21-layer model
+    (seed 2), 64 slownesses on [0.05, 0.6], nfreq = 1024, its uniform +-10 % start (seed 42),
+    exact Hessian (torch.func.hessian per slowness), 10 iterations.  Hours of CPU time."""
+    sys.path.insert(0, ref_root)
+    import torch
+    from Kennett_Reflectivity.layer_model import LayerModel
+    from Kennett_Reflectivity.taup_inversion import invert_taup
+
+    from seismicinversion_b200.earth_models import random_layered_model
+
+    torch.set_num_threads(max(1, os.cpu_count() or 1))
+    m = random_layered_model(20, seed=2)
+    rm = LayerModel.from_arrays(m.alpha, m.beta, m.rho, m.thickness, m.Q_alpha, m.Q_beta)
+    res = invert_taup(rm, list(np.linspace(0.05, 0.6, 64)), nfreq=1024, perturbation=0.1,
+                      max_iter=10, seed=42, tol=0.0)
+    np.savez_compressed(
+        HERE / "invert_c2.npz",
+        misfit=np.array(res.misfit_history), grad_norm=np.array(res.grad_norm_history),
+        param_err=np.array(res.param_error_history), n_iter=res.n_iterations,
+        init_alpha=res.initial_model.alpha, init_beta=res.initial_model.beta,
+        init_rho=res.initial_model.rho, init_thickness=res.initial_model.thickness,
+        rec_alpha=res.recovered_model.alpha, rec_beta=res.recovered_model.beta,
+        rec_rho=res.recovered_model.rho, rec_thickness=res.recovered_model.thickness,
+    )
+
+
 def main(ref_root: str) -> None:
     sys.path.insert(0, ref_root)
     os.environ.setdefault("TQDM_DISABLE", "1")
@@ -240,13 +325,20 @@ def main(ref_root: str) -> None:
 
 if __name__ == "__main__":
     if len(sys.argv) < 2 or sys.argv[1].startswith("--"):
-        sys.exit("usage: make_golden.py <reference checkout> [--training-data-only | --gmm-only]")
+        sys.exit("usage: make_golden.py <reference checkout> [--training-data-only | --gmm-only"
+                 " | --c2-derivs-only | --c2-inversion-only]")
     root = sys.argv[1]
     if "--training-data-only" in sys.argv:
         training_data_golden(root)
     elif "--gmm-only" in sys.argv:
         gmm_golden(root)
+    elif "--c2-derivs-only" in sys.argv:
+        c2_derivs_golden(root)
+    elif "--c2-inversion-only" in sys.argv:
+        c2_inversion_golden(root)
     else:
         main(root)
         training_data_golden(root)
         gmm_golden(root)
+        c2_derivs_golden(root)
+        c2_inversion_golden(root)

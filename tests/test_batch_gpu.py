@@ -124,3 +124,56 @@ def test_invalid_batches_rejected():
         ModelBatch([BatchItem(m, np.array([0.1]), np.array([1.0]), gradient=True)])
     with pytest.raises(ValueError):
         ModelBatch([BatchItem(m, np.array([0.1]), np.array([1.0]))], schedule=(96, 128))
+
+
+def test_largest_uneven_models_forward_and_gradient_vs_oracle():
+    """The two largest models of the 4096-model uneven workload (seed 3; 64 and 61 layers,
+    ~256 slownesses x 2048 frequencies), batched among small models, against the oracle at
+    full size (a spawned process pool over the slownesses): the forward R grid to 1e-10; the
+    gradient model's stored R to 1e-10, its chi to 1e-10 and four gradient components (a
+    deep layer's alpha, beta, rho and h) to central differences of the oracle misfit, 1e-6."""
+    from oracle.cpu_baseline import ReflectivityPool
+    from seismicinversion_b200.batch import BatchItem, ModelBatch
+    from seismicinversion_b200.earth_models import uneven_batch_specs
+    from seismicinversion_b200.layer_model import LayerModel
+
+    specs = uneven_batch_specs(4096, seed=3)
+    order = sorted(range(len(specs)), key=lambda b: -(specs[b][0].n_layers * len(specs[b][1])
+                                                      * len(specs[b][2])))
+    fa, ga = order[0], order[1]
+    mf, pf, wf = specs[fa]
+    mg, pg, wg = specs[ga]
+    assert mf.n_layers >= 61 and mg.n_layers >= 61 and len(wf) == len(wg) == 2048
+    f = np.exp(0.03 * np.sin(np.arange(mg.n_layers)))
+    perturbed = LayerModel(mg.alpha * f, mg.beta * f, mg.rho, mg.thickness, mg.Q_alpha, mg.Q_beta)
+    with ReflectivityPool() as pool:
+        Rf_o = pool.reflectivity(mf, pf, wf)
+        R_obs = pool.reflectivity(perturbed, pg, wg)
+        Rg_o = pool.reflectivity(mg, pg, wg)
+        chi_o = float(np.sum(np.abs(Rg_o - R_obs) ** 2))
+        L = mg.n_layers
+        base = [mg.alpha, mg.beta, mg.rho, mg.thickness]
+        fd = {}
+        for k, l in [(0, L - 10), (1, L // 2), (2, 5), (3, L - 3)]:
+            arrs = [b.copy() for b in base]
+            d = 1e-6 * arrs[k][l]
+            arrs[k][l] += d
+            cp = np.sum(np.abs(pool.reflectivity(LayerModel(*arrs, mg.Q_alpha, mg.Q_beta), pg, wg)
+                               - R_obs) ** 2)
+            arrs[k][l] -= 2 * d
+            cm = np.sum(np.abs(pool.reflectivity(LayerModel(*arrs, mg.Q_alpha, mg.Q_beta), pg, wg)
+                               - R_obs) ** 2)
+            fd[(k, l)] = (cp - cm) / (2 * d)
+    small = [BatchItem(m, p, w) for (m, p, w) in specs[:8]]
+    items = small + [BatchItem(mf, pf, wf),
+                     BatchItem(mg, pg, wg, gradient=True, R_obs=R_obs, store_R=True)]
+    batch = ModelBatch(items, schedule=(128, 2048))
+    batch.launch()
+    torch.cuda.synchronize()
+    assert rel_err(batch.reflectivity(8).cpu().numpy(), Rf_o) < 1e-10
+    assert rel_err(batch.reflectivity(9).cpu().numpy(), Rg_o) < 1e-10
+    chi, g = batch.misfit_gradient(9)
+    assert abs(float(chi) - chi_o) / chi_o < 1e-10
+    g = g.cpu().numpy()
+    for (k, l), v in fd.items():
+        assert abs(g[k * L + l] - v) / np.max(np.abs(g)) < 1e-6, (k, l, g[k * L + l], v)

@@ -509,3 +509,44 @@ def test_torch_backward_at_gather_size_forms_no_jacobian():
         want += (gR[j0:j0 + 512].conj().unsqueeze(1) * J).real.sum((0, 2))
         del J
     assert rel_err(got, want.cpu().numpy()) < 1e-12
+
+
+def test_c2_1024_jacobians_and_gradient_vs_reference(golden):
+    """The tau-p inversion workload at its own size (21 layers, 79 packed parameters,
+    1024 frequencies) from its lognormal start: kr_jacobian at 4 of the 64 slownesses against
+    the reference's jacrev (1e-10), the misfit gradient over those slownesses against the
+    reference's autograd gradient (1e-10), and the exact Hessian (tangent of the adjoint)
+    against torch.func.hessian of the differentiable CPU oracle at one slowness (1e-10)."""
+    from oracle import torch_oracle as T
+    from seismicinversion_b200.kennett_torch import (_pack_params, _unpack_params, jacobian,
+                                                     misfit_gradient_packed, model_to_tensors)
+    from seismicinversion_b200.layer_model import LayerModel
+    from seismicinversion_b200.taup_inversion import _Problem
+
+    g = golden("derivs_c2_1024.npz")
+    start = LayerModel(*[g["start_" + k] for k in ("alpha", "beta", "rho", "thickness",
+                                                   "Q_alpha", "Q_beta")])
+    t = model_to_tensors(start)
+    om = torch.as_tensor(g["omega"])
+    for k, p in enumerate(g["p"]):
+        J = jacobian(t["alpha"], t["beta"], t["rho"], t["thickness"], t["Q_alpha"],
+                     t["Q_beta"], float(p), om)
+        assert rel_err(J.numpy(), g[f"J_{k}"]) < 1e-10, k
+    m0 = _pack_params(t["alpha"], t["beta"], t["rho"], t["thickness"]).numpy()
+    R_obs = np.stack([g[f"R_obs_{k}"] for k in range(4)])
+    chi, grad = misfit_gradient_packed(m0, t["alpha"], t["beta"], t["rho"], t["thickness"],
+                                       t["Q_alpha"], t["Q_beta"], g["p"], om, R_obs)
+    assert abs(chi - float(g["chi"])) / float(g["chi"]) < 1e-10
+    assert rel_err(grad.cpu().numpy(), g["grad"]) < 1e-10
+    prob = _Problem(t["alpha"], t["beta"], t["rho"], t["thickness"], t["Q_alpha"], t["Q_beta"],
+                    g["p"][2:3], om, R_obs[2:3])
+    H = prob.hessian_exact(m0)
+    m = torch.as_tensor(m0)
+
+    def chi_cpu(mm):
+        a, b, r, h = _unpack_params(mm, t["alpha"], t["beta"], t["rho"], t["thickness"])
+        return T.misfit(T.reflectivity(a, b, r, h, t["Q_alpha"], t["Q_beta"], g["p"][2:3], om),
+                        torch.as_tensor(R_obs[2:3]))
+
+    H_ref = torch.func.hessian(chi_cpu)(m).numpy()
+    assert rel_err(H, H_ref) < 1e-10

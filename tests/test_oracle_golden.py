@@ -119,3 +119,61 @@ def test_gmm_oracle_vs_reference(golden, tag):
     # the two methods compute one reflectivity
     Rk = O.reflectivity(*m, g[f"{tag}_p"], g[f"{tag}_omega"], False)
     assert rel_err(g[f"{tag}_R_fs0"], Rk) < 1e-9
+
+
+def _torch_model(g, prefix=""):
+    import torch
+
+    return {k: torch.as_tensor(np.asarray(g[prefix + k], dtype=np.float64))
+            for k in ("alpha", "beta", "rho", "thickness", "Q_alpha", "Q_beta")}
+
+
+def test_torch_oracle_matches_numpy_oracle_and_reference_forward(golden):
+    """The differentiable torch oracle (the CPU baseline of the derivative workloads) gives the
+    NumPy oracle's R and the reference's torch forward golden."""
+    import torch
+
+    from oracle import torch_oracle as T
+
+    g = golden("derivs_c2.npz")
+    t = _torch_model(g)
+    for p in (0.05, 0.3):
+        R = T.reflectivity(**t, p=p, omega=torch.as_tensor(g["omega"]))[0]
+        assert rel_err(R.numpy(), g[f"R_p{p}"]) < 1e-12
+    d = golden("default_model_R.npz")
+    td = _torch_model(d)
+    for tag in ("damped_fs0", "damped_fs1"):
+        R = T.reflectivity(**td, p=d["p"][:5], omega=torch.as_tensor(d["omega_" + tag]),
+                           free_surface=tag.endswith("1"))
+        Rn = O.reflectivity(*_m(d), d["p"][:5], d["omega_" + tag], free_surface=tag.endswith("1"))
+        assert rel_err(R.numpy(), Rn) < 1e-12
+
+
+def test_torch_oracle_derivatives_vs_reference_c2_1024(golden):
+    """The tau-p inversion workload at its own 1024 frequencies: the torch oracle's autograd
+    misfit gradient over 4 of the 64 slownesses equals the reference's (autograd.grad, as
+    taup_misfit_grad_hessian takes it) to 1e-10 (the reference's jacrev Jacobians in the same
+    fixture are compared with the CUDA kernels directly, in the GPU tests)."""
+    import torch
+
+    from oracle import torch_oracle as T
+    from seismicinversion_b200.kennett_torch import _pack_params, _unpack_params, packed_index
+
+    g = golden("derivs_c2_1024.npz")
+    ts = _torch_model(g, "start_")
+    om = torch.as_tensor(g["omega"])
+    m0 = _pack_params(ts["alpha"], ts["beta"], ts["rho"], ts["thickness"]).clone()
+
+    def chi(m):
+        a, b, r, h = _unpack_params(m, ts["alpha"], ts["beta"], ts["rho"], ts["thickness"])
+        R = T.reflectivity(a, b, r, h, ts["Q_alpha"], ts["Q_beta"], g["p"], om)
+        Ro = torch.stack([torch.as_tensor(g[f"R_obs_{k}"]) for k in range(4)])
+        return T.misfit(R, Ro)
+
+    m = m0.clone().requires_grad_(True)
+    c = chi(m)
+    (grad,) = torch.autograd.grad(c, m)
+    assert abs(float(c) - float(g["chi"])) / float(g["chi"]) < 1e-12
+    assert rel_err(grad.numpy(), g["grad"]) < 1e-10
+
+    assert len(packed_index(ts["alpha"].shape[0])) == g["J_1"].shape[1] == 79
