@@ -279,12 +279,101 @@ def bench_gmm(torch, D, tab, p_t, w_t, R_kennett, reps):
             "max_rel_diff_vs_kennett_p_le_1": diff}
 
 
-def bench_inversion(torch, dev, reps):
+def _rel(x, ref) -> float:
+    """max|x - ref| / max|ref| (the reference's error metric)."""
+    x, ref = np.asarray(x), np.asarray(ref)
+    return float(np.max(np.abs(x - ref)) / (np.max(np.abs(ref)) + 1e-300))
+
+
+def accuracy_c0():
+    """The single-trace configuration (6 layers, p = 0.2, 2047 frequencies, free surface,
+    Ricker 10 Hz) through the public drop-ins against the oracle: R and the 4096-sample trace."""
+    from oracle import kennett_oracle as O
+    from seismicinversion_b200 import compute_seismogram, kennett_reflectivity
+    from seismicinversion_b200.earth_models import random_layered_model
+    from seismicinversion_b200.source import ricker_10hz
+
+    m = random_layered_model(5, seed=0)
+    arrs = [m.alpha, m.beta, m.rho, m.thickness, m.Q_alpha, m.Q_beta]
+    _, tr = compute_seismogram(m, 0.2, T=64.0, nw=2048, source_func=ricker_10hz,
+                               free_surface=True)
+    om = np.arange(1, 2048) * (2 * np.pi / 64.0)
+    R = kennett_reflectivity(m, 0.2, om, free_surface=True)
+    _, tro, Ro = O.seismogram(*arrs, 0.2, T=64.0, nw=2048, free_surface=True,
+                              source=lambda w, wm: O.ricker_spectrum(w, 100 * np.pi))
+    return {"c0_R": _rel(R, Ro), "c0_trace": _rel(tr, tro)}
+
+
+def taup_cpu_baseline(torch, true, start, p, w, n_grad=8):
+    """CPU baseline of the tau-p derivative workload, as the reference computes it: per
+    slowness, the differentiable forward on the CPU and torch.autograd.grad of the misfit
+    (taup_inversion.py:153-172), torch.func.hessian of it (:177) and jacrev
+    (kennett_torch.py:611-641), through the differentiable oracle with torch threads = host
+    cores.  Gradients timed on n_grad of the slownesses, the Hessian and jacrev on one,
+    extrapolated to all of them."""
+    from oracle import torch_oracle as T
+    from seismicinversion_b200.kennett_torch import _pack_params, _unpack_params
+
+    cores = len(os.sched_getaffinity(0))
+    threads = torch.get_num_threads()
+    torch.set_num_threads(cores)
+    n_hw = 64  # frequencies of the timed Hessian (its cost is linear in them)
+    try:
+        tt = {k: torch.as_tensor(getattr(true, k)) for k in
+              ("alpha", "beta", "rho", "thickness", "Q_alpha", "Q_beta")}
+        ts = {k: torch.as_tensor(getattr(start, k)) for k in tt}
+        om = torch.as_tensor(w)
+        m0 = _pack_params(ts["alpha"], ts["beta"], ts["rho"], ts["thickness"])
+        sel = np.linspace(0, len(p) - 1, n_grad).round().astype(int)
+
+        def chi_p(m, pj):
+            a, b, r, h = _unpack_params(m, ts["alpha"], ts["beta"], ts["rho"], ts["thickness"])
+            R = T.reflectivity(a, b, r, h, ts["Q_alpha"], ts["Q_beta"], [pj], om)
+            Ro = T.reflectivity(*tt.values(), [pj], om).detach()
+            return T.misfit(R, Ro)
+
+        chi_p(m0.clone().requires_grad_(True), float(p[0]))  # warm (allocator, threads)
+        t0 = time.perf_counter()
+        for j in sel:
+            m = m0.clone().requires_grad_(True)
+            torch.autograd.grad(chi_p(m, float(p[j])), m)
+        grad_s = (time.perf_counter() - t0) / len(sel) * len(p)
+        j = int(sel[len(sel) // 2])
+        om_full = om
+        om = om_full[:n_hw]
+        t0 = time.perf_counter()
+        torch.func.hessian(lambda m: chi_p(m, float(p[j])))(m0)
+        hess_s = (time.perf_counter() - t0) * len(p) * len(om_full) / n_hw
+        om = om_full
+
+        def f(m):
+            a, b, r, h = _unpack_params(m, ts["alpha"], ts["beta"], ts["rho"], ts["thickness"])
+            return T.reflectivity(a, b, r, h, ts["Q_alpha"], ts["Q_beta"], [float(p[j])], om)[0]
+
+        t0 = time.perf_counter()
+        torch.func.jacrev(lambda m: f(m).real)(m0)
+        torch.func.jacrev(lambda m: f(m).imag)(m0)
+        jac_s = time.perf_counter() - t0
+    finally:
+        torch.set_num_threads(threads)
+    return {"grad_evals_per_s": 1.0 / grad_s, "seconds_per_grad_eval": grad_s,
+            "seconds_per_exact_hessian": hess_s, "seconds_per_jacobian_one_slowness": jac_s,
+            "seconds_per_exact_lm_iteration_est": grad_s + hess_s, "unit": "grad evals/s",
+            "cores": cores, "kind": "port",
+            "sample": f"autograd gradient on {len(sel)} of {len(p)} slownesses and jacrev "
+                      f"(Re, Im) on 1, per slowness as the reference loops them, extrapolated "
+                      f"to {len(p)}; torch.func.hessian on 1 slowness x {n_hw} of the "
+                      f"{len(w)} frequencies, extrapolated linearly; differentiable torch "
+                      f"restatement of the oracle, torch threads = {cores}",
+            "host": host_info(cores)}
+
+
+def bench_inversion(torch, dev, reps, cpu=True):
     """tau-p inversion workload: 21-layer model (79 packed parameters), 64 slownesses on
     [0.05, 0.6], omega_k = k 2pi/64 (k = 1..1024), start = true * exp(0.1 N(0,1)) (seed 2)."""
     from seismicinversion_b200 import device as D
     from seismicinversion_b200.earth_models import random_layered_model
-    from seismicinversion_b200.kennett_torch import model_to_tensors
+    from seismicinversion_b200.kennett_torch import model_to_tensors, packed_index
     from seismicinversion_b200.taup_inversion import invert_taup
 
     true = random_layered_model(20, seed=2)
@@ -308,12 +397,38 @@ def bench_inversion(torch, dev, reps):
     peak = fp64_peak(torch, dev)
     alg = FLOPS_PER_ADJOINT_UPDATE * upd / (ms_grad * 1e-3) / 1e12
     out = {"workload": "tau-p LM, 21 layers / 79 params, 64 p x 1024 omega",
+           "grad_units": "gradient evaluations over all 64 slownesses per second",
            "grad_evals_per_s": 1e3 / ms_grad, "ms_per_grad_eval": ms_grad,
            "adjoint_updates_per_s": upd / (ms_grad * 1e-3),
            "adjoint_alg_tflops": alg, "adjoint_frac_of_fp64_peak": alg / peak,
            "ms_per_jacobian": ms_jac, "ms_per_forward": ms_fwd}
+    basis = torch.eye(4 * 21, dtype=torch.float64, device=dev)[torch.as_tensor(packed_index(21))]
+    ms_hvp = _events(torch, st, lambda: D.misfit_hvp(tab, p_t, w_t, R_obs, basis), reps)
+    out["ms_per_exact_hessian"] = ms_hvp
+    out["exact_hessian_method"] = ("79 Hessian-vector products (tangent of the adjoint, "
+                                   "kr_misfit_hvp) in one launch")
+    # accuracy against the reference's own jacrev / autograd at 1024 frequencies (the start
+    # model above at 4 of the 64 slownesses: tests/golden/derivs_c2_1024.npz)
+    from seismicinversion_b200.kennett_torch import _pack_params, jacobian, misfit_gradient_packed
+
+    gold = ROOT / "tests" / "golden" / "derivs_c2_1024.npz"
+    if gold.exists():
+        with np.load(gold) as g:
+            ts = model_to_tensors(start)
+            om = torch.as_tensor(g["omega"])
+            errs = [_rel(jacobian(ts["alpha"], ts["beta"], ts["rho"], ts["thickness"],
+                                  ts["Q_alpha"], ts["Q_beta"], float(pk), om).numpy(),
+                         g[f"J_{k}"]) for k, pk in enumerate(g["p"])]
+            m0 = _pack_params(ts["alpha"], ts["beta"], ts["rho"], ts["thickness"]).numpy()
+            _, gr = misfit_gradient_packed(m0, ts["alpha"], ts["beta"], ts["rho"],
+                                           ts["thickness"], ts["Q_alpha"], ts["Q_beta"], g["p"],
+                                           om, np.stack([g[f"R_obs_{k}"] for k in range(4)]))
+            out["max_rel_err_vs_reference"] = {
+                "jacobian_4p_1024w": max(errs), "gradient_4p_1024w": _rel(gr.cpu().numpy(),
+                                                                          g["grad"]),
+                "reference": "jacrev and autograd.grad of the reference's torch forward"}
     for hess in ("gauss-newton", "exact"):
-        its = 10 if hess == "gauss-newton" else 2
+        its = 10
         # one untimed iteration first: library handles, allocator pools and plans are made
         # on first use, and a cold first call would count them
         invert_taup(true, list(p), nfreq=1024, max_iter=1, hessian=hess, initial_params=init,
@@ -326,8 +441,25 @@ def bench_inversion(torch, dev, reps):
         dt = time.perf_counter() - t0
         out[f"lm_{hess}"] = {"iterations": res.n_iterations, "seconds": dt,
                              "s_per_iteration": dt / max(res.n_iterations, 1),
-                             "param_err_first_last": [res.param_error_history[0],
-                                                      res.param_error_history[-1]]}
+                             "param_err_history": list(map(float, res.param_error_history)),
+                             "misfit_history": list(map(float, res.misfit_history))}
+    # the reference's own start (uniform +-10 %, seed 42) and its invert_taup trajectory on
+    # this workload (tests/golden/invert_c2.npz, the reference run on the CPU)
+    gold = ROOT / "tests" / "golden" / "invert_c2.npz"
+    res = invert_taup(true, list(p), nfreq=1024, perturbation=0.1, max_iter=10, seed=42,
+                      hessian="exact", tol=0.0)
+    traj = {"param_err_history": list(map(float, res.param_error_history)),
+            "misfit_history": list(map(float, res.misfit_history))}
+    if gold.exists():
+        with np.load(gold) as g:
+            n = min(len(g["param_err"]), res.n_iterations)
+            traj["reference_param_err_history"] = list(map(float, g["param_err"]))
+            traj["reference_misfit_history"] = list(map(float, g["misfit"]))
+            traj["max_abs_diff_param_err"] = float(np.max(np.abs(
+                np.array(res.param_error_history[:n]) - g["param_err"][:n])))
+            traj["max_rel_diff_misfit"] = float(np.max(np.abs(
+                np.array(res.misfit_history[:n]) - g["misfit"][:n]) / g["misfit"][:n]))
+    out["lm_exact_reference_start"] = traj
     # K concurrent inversions (true models seeds 2..2+K-1, lognormal starts), LM state on
     # the device: one batched gradient (+ exact-Hessian) launch and one batched trial launch
     # per round for all K
@@ -343,7 +475,7 @@ def bench_inversion(torch, dev, reps):
         trues.append(tm)
         inits.append(x0)
     for hess in ("gauss-newton", "exact"):
-        its = 5 if hess == "gauss-newton" else 2
+        its = 5
         invert_taup_batch(trues, list(p), nfreq=1024, max_iter=1, hessian=hess,
                           initial_params=inits, tol=0.0)
         torch.cuda.synchronize()
@@ -359,10 +491,51 @@ def bench_inversion(torch, dev, reps):
             "s_per_round_all_inversions": dt / its,
             "inversion_iterations_per_s": n_it / dt,
             "speedup_vs_sequential_invert_taup": (n_it * seq) / dt}
+    if cpu:
+        cb = taup_cpu_baseline(torch, true, start, p, np.arange(1, 1025) * (2 * np.pi / 64))
+        cb["value"] = cb["grad_evals_per_s"]
+        out["cpu_baseline"] = cb
+        out["grad_evals_speedup_vs_cpu"] = out["grad_evals_per_s"] / cb["grad_evals_per_s"]
+        out["exact_lm_iteration_speedup_vs_cpu"] = (
+            cb["seconds_per_exact_lm_iteration_est"] / out["lm_exact"]["s_per_iteration"])
     return out
 
 
-def bench_batched(torch, dev, reps, n_models=4096):
+def uneven_cpu_baseline(specs, pool, n_models=256, max_p=8):
+    """CPU rates of the uneven-batching workload on a stratified sample: every
+    (4096 / n_models)-th model in order of work (smallest to largest), each on up to ``max_p``
+    of its slownesses (evenly spaced) with all its frequencies and layers; even models forward
+    (the NumPy oracle, as the reference's kennett_reflectivity), odd models forward + misfit
+    gradient (torch autograd through the differentiable oracle, as kennett_reflectivity_torch
+    and taup_misfit_grad_hessian); one model per task on a spawned pool of every host core.
+    Returns (forward updates/s, gradient updates/s, description)."""
+    from oracle.cpu_baseline import _grad_chunk, _layers, _refl_chunk
+
+    order = sorted(range(len(specs)), key=lambda b: specs[b][0].n_layers * len(specs[b][1])
+                   * len(specs[b][2]))
+    pick = [order[int(k)] for k in np.linspace(0, len(order) - 1, n_models).round()]
+    fwd, grad = [], []
+    fu = gu = 0
+    for b in pick:
+        m, p, w = specs[b]
+        ps = p[np.unique(np.linspace(0, len(p) - 1, min(max_p, len(p))).round().astype(int))]
+        u = len(ps) * len(w) * (m.n_layers - 1)
+        if b % 2:
+            grad.append((_layers(m), ps, w, np.zeros((len(ps), len(w)), complex), False))
+            gu += u
+        else:
+            fwd.append((_layers(m), ps, w, False))
+            fu += u
+    pool.warm()
+    tf = pool.timed_jobs(_refl_chunk, fwd)
+    tg = pool.timed_jobs(_grad_chunk, grad)
+    desc = (f"{len(pick)} models stratified by work ({len(fwd)} forward, {len(grad)} forward + "
+            f"gradient), <= {max_p} slownesses each with all frequencies and layers, spawned "
+            f"pool of {pool.workers} processes; full-workload time extrapolated per update")
+    return fu / tf, gu / tg, desc
+
+
+def bench_batched(torch, dev, reps, n_models=4096, pool=None):
     """Uneven batching workload: 4096 models, total layers U{3..64}, n_omega in
     {256, 512, 1024, 2048}, n_p U{16..256} on (0, 0.8] (seed 3); odd models ask for forward +
     gradient against the R of an independently perturbed model (seed 4)."""
@@ -442,6 +615,34 @@ def bench_batched(torch, dev, reps, n_models=4096):
     alg = (FLOPS_PER_UPDATE * work["forward_updates"]
            + FLOPS_PER_ADJOINT_UPDATE * work["gradient_updates"]) / (ms * 1e-3) / 1e12
     peak = fp64_peak(torch, dev)
+    extra = {}
+    if pool is not None:
+        # accuracy: the largest forward model and the largest gradient model of the batch at
+        # full size against the oracle (reflectivity; chi and gradient by autograd)
+        order = sorted(range(n_models), key=lambda b: -(specs[b][0].n_layers * len(specs[b][1])
+                                                        * len(specs[b][2])))
+        bf = next(b for b in order if b % 2 == 0)
+        bg = next(b for b in order if b % 2 == 1)
+        mf, pf, wf = specs[bf]
+        Rf = pool.reflectivity(mf, pf, wf)
+        mg, pg, wg = specs[bg]
+        obs = items[bg].R_obs.cpu().numpy().reshape(len(pg), len(wg))
+        chi_o, g_o = pool.misfit_gradient(mg, pg, wg, obs)
+        chi, g = batch.misfit_gradient(bg)
+        extra["max_rel_err_vs_oracle"] = {
+            "forward_largest_model": _rel(batch.reflectivity(bf).cpu().numpy(), Rf),
+            "gradient_largest_model": _rel(g.cpu().numpy(), g_o),
+            "chi_largest_model": abs(float(chi) - chi_o) / chi_o,
+            "models": f"forward: {mf.n_layers} layers x {len(pf)} p x {len(wf)} w; gradient: "
+                      f"{mg.n_layers} layers x {len(pg)} p x {len(wg)} w"}
+        fr, gr, desc = uneven_cpu_baseline(specs, pool)
+        cpu_s = work["forward_updates"] / fr + work["gradient_updates"] / gr
+        extra["cpu_baseline"] = {
+            "value": n_models / cpu_s, "unit": "models/s", "cores": pool.workers, "kind": "port",
+            "forward_updates_per_s": fr, "gradient_updates_per_s": gr,
+            "seconds_full_batch_extrapolated": cpu_s, "sample": desc,
+            "host": host_info(pool.workers)}
+        extra["speedup_vs_cpu"] = (n_models / (ms * 1e-3)) / (n_models / cpu_s)
     return {"workload": "4096 uneven models, half forward+gradient", "schedule": list(best),
             "autotune_ms": {str(k): v for k, v in times.items()}, "ms_per_batch": ms,
             "models_per_s": batched_models_per_s, **work,
@@ -451,7 +652,7 @@ def bench_batched(torch, dev, reps, n_models=4096):
             "plain_per_slowness_call_models_per_s": n_models / (per_pair_call * n_pairs),
             "speedup_vs_per_model_calls": batched_models_per_s * per_model,
             "speedup_vs_per_slowness_calls": batched_models_per_s * per_pair_call * n_pairs / n_models,
-            "graph_captured": True}
+            "graph_captured": True, **extra}
 
 
 def bench_training_data(torch, dev, n=50_000):
@@ -537,7 +738,7 @@ def _plain_per_request(torch, D, dev, pool, arrivals):
 
 
 def bench_serving(torch, dev, rates=(100, 300, 1000, 3000, 10000, 20000), duration=1.0,
-                  max_requests=3000):
+                  max_requests=3000, pool=None, cpu_rates=None):
     """Serving workload: Poisson arrivals (seed 7) of requests drawn as in the batching
     workload (50/50 forward / forward+gradient), device-resident inputs, 120 GB budget; the
     client consumes results in arrival order and releases them.  At every rate the same
@@ -550,14 +751,14 @@ def bench_serving(torch, dev, rates=(100, 300, 1000, 3000, 10000, 20000), durati
     from seismicinversion_b200.serve import KennettServer
 
     specs = uneven_batch_specs(256, seed=5)
-    pool = []
+    poolreq = []
     for b, (m, p, w) in enumerate(specs):
         p_t = torch.as_tensor(p, device=dev)
         w_t = torch.as_tensor(w, device=dev).to(torch.complex128)
         obs = None
         if b % 2:
             obs = D.reflectivity(D.layer_table(m, dev), p_t, w_t) * 1.01
-        pool.append((m, p_t, w_t, b % 2 == 1, obs))
+        poolreq.append((m, p_t, w_t, b % 2 == 1, obs))
     torch.cuda.synchronize()
     rng = np.random.default_rng(7)
     rng_w = np.random.default_rng(8)
@@ -576,7 +777,7 @@ def bench_serving(torch, dev, rates=(100, 300, 1000, 3000, 10000, 20000), durati
     # pinned staging buffers: the whole pool at once, then a short stream at a high rate
     with KennettServer(executor=ex, hbm_budget_bytes=120 * 10**9, max_batch_requests=64,
                        max_inflight=2) as srv:
-        warm = [srv.submit(m, p_t, w_t, gradient=g, R_obs=obs) for m, p_t, w_t, g, obs in pool]
+        warm = [srv.submit(m, p_t, w_t, gradient=g, R_obs=obs) for m, p_t, w_t, g, obs in poolreq]
         for r in warm:
             r.wait(120)
             r.release()
@@ -587,13 +788,13 @@ def bench_serving(torch, dev, rates=(100, 300, 1000, 3000, 10000, 20000), durati
             dt = t_next - time.perf_counter()
             if dt > 0:
                 time.sleep(dt)
-            m, p_t, w_t, g, obs = pool[k % len(pool)]
+            m, p_t, w_t, g, obs = poolreq[k % len(poolreq)]
             warm.append(srv.submit(m, p_t, w_t, gradient=g, R_obs=obs))
         for r in warm:
             r.wait(120)
             r.release()
         del warm
-    _plain_per_request(torch, D, dev, pool, [time.perf_counter()] * 64)  # untimed warm-up
+    _plain_per_request(torch, D, dev, poolreq, [time.perf_counter()] * 64)  # untimed warm-up
     torch.cuda.synchronize()
 
     for lam in rates:
@@ -613,7 +814,7 @@ def bench_serving(torch, dev, rates=(100, 300, 1000, 3000, 10000, 20000), durati
                 dt = t_next - time.perf_counter()
                 if dt > 0:
                     time.sleep(dt)  # releases the GIL to the scheduler thread
-                m, p_t, w_t, g, obs = pool[k % len(pool)]
+                m, p_t, w_t, g, obs = poolreq[k % len(poolreq)]
                 reqs.append(srv.submit(m, p_t, w_t, gradient=g, R_obs=obs))
                 while consumed < len(reqs) and reqs[consumed].done.is_set():
                     reqs[consumed].release()
@@ -627,11 +828,42 @@ def bench_serving(torch, dev, rates=(100, 300, 1000, 3000, 10000, 20000), durati
                                      "mean_device_ms")}
         gc.collect()
         t0 = time.perf_counter() + 1e-3
-        plain = _plain_per_request(torch, D, dev, pool, list(t0 + np.cumsum(gaps)))
+        plain = _plain_per_request(torch, D, dev, poolreq, list(t0 + np.cumsum(gaps)))
         row["plain_per_request"] = plain
         row["throughput_vs_plain"] = row["throughput_rps"] / plain["throughput_rps"]
         out[f"rate_{lam}"] = row
     gc.unfreeze()
+    if pool is not None:
+        # accuracy: 4 forward and 4 forward + gradient requests served in one session, each
+        # against the oracle at its full size
+        sample = list(range(8))
+        with KennettServer(executor=ex, max_batch_requests=64, max_inflight=2) as srv:
+            reqs = [srv.submit(poolreq[k][0], poolreq[k][1], poolreq[k][2], gradient=poolreq[k][3],
+                               R_obs=poolreq[k][4]) for k in sample]
+            res = [r.wait(120) for r in reqs]
+        ef = eg = 0.0
+        for k, r in zip(sample, res):
+            m, p_t, w_t, g, obs = poolreq[k]
+            pn, wn = p_t.cpu().numpy(), w_t.cpu().numpy()
+            if g:
+                chi_o, g_o = pool.misfit_gradient(m, pn, wn, obs.cpu().numpy())
+                eg = max(eg, _rel(r["grad"].cpu().numpy(), g_o), abs(float(r["chi"]) - chi_o) / chi_o)
+            else:
+                ef = max(ef, _rel(r["R"].cpu().numpy(), pool.reflectivity(m, pn, wn)))
+        for r in reqs:
+            r.release()
+        out["max_rel_err_vs_oracle"] = {"forward_4_requests": ef, "gradient_4_requests": eg}
+    if cpu_rates is not None:
+        # per-request CPU replay of the request mix, at the CPU rates of the uneven-batching
+        # sample (same model distribution): seconds per request, one request at a time on
+        # every host core
+        fr, gr = cpu_rates
+        secs = [len(p_t) * len(w_t) * (m.n_layers - 1) / (gr if g else fr)
+                for m, p_t, w_t, g, _ in poolreq]
+        out["cpu_baseline"] = {"value": 1.0 / float(np.mean(secs)), "unit": "requests/s",
+                               "kind": "port", "sample": "the request pool (256 requests, 50/50 "
+                               "forward / forward + gradient) at the per-update CPU rates of the "
+                               "uneven-batching baseline"}
     return out
 
 
@@ -767,11 +999,13 @@ def run_ours(args, rank, world, local):
 
     cpu_base = None
     if rank == 0 and world == 1 and not (args.no_cpu_baseline or args.profile):
-        from oracle.cpu_baseline import GatherBaseline  # checker / baseline leg only
+        from oracle import kennett_oracle as O  # checker / baseline leg only
+        from oracle.cpu_baseline import GatherBaseline
 
-        cores = len(os.sched_getaffinity(0))
-        n_sample = args.cpu_sample or max(256, 4 * cores)
-        cpu_base = GatherBaseline(model, offsets, T, nw, npp, pmax, True, n_sample)
+        # the whole workload (every slowness) in one timed sample: it also gives the error of
+        # the full R grid and of every trace against the oracle
+        n_sample = args.cpu_sample or npp
+        cpu_base = GatherBaseline(model, offsets, T, nw, npp, pmax, True, n_sample, chunk=16)
 
     tab = D.layer_table(model, dev)
     p_t = torch.as_tensor(p, device=dev)
@@ -889,30 +1123,53 @@ def run_ours(args, rank, world, local):
                 "nominal_peak": round(NOMINAL_FP64_TFLOPS, 2)}
 
     cpu = None
-    accuracy = None
+    accuracy = {}
     if cpu_base is not None:
-        samples = []
-        for i in range(2):  # one warm start, one timed
-            dt, Rc, _ = cpu_base.step()
-            samples.append(dt)
+        cpu_base.warm()
+        dt, Rc, Uc = cpu_base.step()
         Rg = R[torch.as_tensor(cpu_base.rows, device=dev)].cpu().numpy()
-        accuracy = float(np.max(np.abs(Rg - Rc)) / np.max(np.abs(Rc)))
-        cpu = {"value": cpu_base.updates() / samples[-1], "unit": "updates/s",
+        accuracy["c1_R"] = _rel(Rg, Rc)
+        if len(cpu_base.rows) == npp:  # the whole workload: the traces too
+            go = O.hermitian_traces(Uc * S, nw, decay)
+            accuracy["c1_traces"] = _rel(G.cpu().numpy(), go)
+            accuracy["c1_traces_first_30s"] = _rel(G.cpu().numpy()[:, time_axis < 30.0],
+                                                   go[:, time_axis < 30.0])
+        cpu = {"value": cpu_base.updates() / dt, "unit": "updates/s",
                "cores": cpu_base.workers, "kind": "port",
-               "sample": f"{len(cpu_base.p)} of {npp} slownesses (evenly spaced), all 2047 "
-                         f"frequencies and 100 offsets: reflectivity + J0 slowness sum, "
-                         f"multiprocessing pool of {cpu_base.workers} (oracle port)",
-               "seconds": samples[-1], "host": host_info(cpu_base.workers)}
+               "sample": f"{len(cpu_base.p)} of {npp} slownesses, all 2047 damped "
+                         f"frequencies and 100 offsets: reflectivity + J0 slowness sum (the "
+                         f"whole R grid and U of the workload), multiprocessing pool of "
+                         f"{cpu_base.workers} (oracle port)",
+               "seconds": dt, "host": host_info(cpu_base.workers)}
         cpu_base.close()
 
     extra = {}
     if world == 1 and not args.no_extra:
+        cpu_legs = not args.no_cpu_baseline
+        opool = None
+        if cpu_legs:
+            from oracle.cpu_baseline import ReflectivityPool  # checker / baseline legs only
+
+            opool = ReflectivityPool()
+            accuracy.update(accuracy_c0())
         extra["gmm"] = bench_gmm(torch, D, tab, p_t, w_t, R, max(args.steps, 3))
-        extra["inversion"] = bench_inversion(torch, dev, max(args.steps, 3))
-        extra["batched"] = bench_batched(torch, dev, max(args.steps, 2))
+        extra["inversion"] = bench_inversion(torch, dev, max(args.steps, 3), cpu=cpu_legs)
+        extra["batched"] = bench_batched(torch, dev, max(args.steps, 2), pool=opool)
         extra["training_data"] = bench_training_data(torch, dev)
         extra["published_configs"] = bench_published_configs(torch, dev)
-        extra["serving"] = bench_serving(torch, dev)
+        b = extra["batched"].get("cpu_baseline")
+        extra["serving"] = bench_serving(
+            torch, dev, pool=opool,
+            cpu_rates=(b["forward_updates_per_s"], b["gradient_updates_per_s"]) if b else None)
+        if opool is not None:
+            opool.close()
+        inv = extra["inversion"].get("max_rel_err_vs_reference", {})
+        accuracy.update({"c2_jacobian_vs_reference": inv.get("jacobian_4p_1024w"),
+                         "c2_gradient_vs_reference": inv.get("gradient_4p_1024w")})
+        for key, src in (("c3", "batched"), ("c4", "serving")):
+            for k, v in extra[src].get("max_rel_err_vs_oracle", {}).items():
+                if isinstance(v, float):
+                    accuracy[f"{key}_{k}"] = v
 
     if rank == 0:
         line = {
@@ -927,7 +1184,7 @@ def run_ours(args, rank, world, local):
             "e2e": {"value": world * upd / e2e_s, "unit": "updates/s", "seconds_per_step": e2e_s,
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": 5 * args.steps, "clocks": clocks, "kernels": kernels,
-            "max_rel_err_vs_oracle_sample": accuracy,
+            "max_rel_err_vs_oracle": accuracy,
             **extra,
         }
         print(json.dumps(line))

@@ -67,6 +67,11 @@ class GatherBaseline:
                         self.dp, self.fs))
         return out
 
+    def warm(self):
+        """Start every worker (spawn, imports) on a small task before a timed step."""
+        t = self.tasks()[:1]
+        self.pool.map(_work, t * self.workers, chunksize=1)
+
     def step(self):
         """One timed sample: returns (seconds, R rows (n_sample, nw-1), U partial)."""
         t0 = time.perf_counter()
@@ -85,23 +90,52 @@ class GatherBaseline:
         self.pool.join()
 
 
+def _warm(_):
+    import torch  # noqa: F401
+
+    from . import torch_oracle  # noqa: F401
+    return 0
+
+
 def _refl_chunk(args):
     layers, p, omega, fs = args
     return O.reflectivity(*layers, p, omega, fs)
 
 
+def _grad_chunk(args):
+    """chi and its gradient d chi / d(alpha, beta, rho, h) [4L] on a slowness subset, by
+    torch autograd through the differentiable oracle (one thread per worker)."""
+    import torch
+
+    from . import torch_oracle as T
+
+    torch.set_num_threads(1)
+    layers, p, omega, R_obs, fs = args
+    t = [torch.as_tensor(np.asarray(x, dtype=np.float64)) for x in layers]
+    for x in t[:4]:
+        x.requires_grad_(True)
+    R = T.reflectivity(*t, p, torch.as_tensor(omega), fs)
+    chi = T.misfit(R, torch.as_tensor(np.asarray(R_obs)))
+    g = torch.autograd.grad(chi, t[:4])
+    return float(chi.detach()), np.concatenate([x.numpy() for x in g])
+
+
+def _layers(model):
+    return tuple(np.asarray(getattr(model, k), dtype=np.float64) for k in
+                 ("alpha", "beta", "rho", "thickness", "Q_alpha", "Q_beta"))
+
+
 class ReflectivityPool:
-    """The oracle's reflectivity over a slowness grid, split into slowness chunks across a
-    ``spawn`` process pool (test infrastructure: full-size parity checks of the batched and
-    served paths, and CPU baselines of those workloads)."""
+    """The oracle's reflectivity (and misfit gradient) over a slowness grid, split into
+    slowness chunks across a ``spawn`` process pool (test infrastructure: full-size parity
+    checks of the batched and served paths, and CPU baselines of those workloads)."""
 
     def __init__(self, workers=None):
         self.workers = workers or len(os.sched_getaffinity(0))
         self.pool = mp.get_context("spawn").Pool(self.workers, initializer=_init_worker)
 
     def reflectivity(self, model, p, omega, free_surface=False):
-        layers = tuple(np.asarray(getattr(model, k), dtype=np.float64) for k in
-                       ("alpha", "beta", "rho", "thickness", "Q_alpha", "Q_beta"))
+        layers = _layers(model)
         p = np.asarray(p, dtype=np.float64)
         omega = np.asarray(omega, dtype=np.complex128)
         n = max(1, min(len(p), 2 * self.workers))
@@ -109,6 +143,28 @@ class ReflectivityPool:
         res = self.pool.map(_refl_chunk, [(layers, c, omega, free_surface) for c in chunks],
                             chunksize=1)
         return np.concatenate(res, axis=0)
+
+    def misfit_gradient(self, model, p, omega, R_obs, free_surface=False):
+        """(chi, gradient [4L]) of chi = sum |R - R_obs|^2, the slowness sum split across the
+        workers (torch autograd through the differentiable oracle)."""
+        layers = _layers(model)
+        p = np.asarray(p, dtype=np.float64)
+        R_obs = np.asarray(R_obs, dtype=np.complex128).reshape(len(p), -1)
+        n = max(1, min(len(p), 2 * self.workers))
+        idx = [c for c in np.array_split(np.arange(len(p)), n) if len(c)]
+        res = self.pool.map(_grad_chunk, [(layers, p[c], omega, R_obs[c], free_surface)
+                                          for c in idx], chunksize=1)
+        return sum(r[0] for r in res), sum(r[1] for r in res)
+
+    def timed_jobs(self, fn, jobs):
+        """Seconds to run ``jobs`` (argument tuples of ``fn``) across the pool."""
+        t0 = time.perf_counter()
+        self.pool.map(fn, jobs, chunksize=1)
+        return time.perf_counter() - t0
+
+    def warm(self):
+        """Start every worker (spawn, imports of the oracle and torch) before timing."""
+        self.pool.map(_warm, range(2 * self.workers), chunksize=1)
 
     def close(self):
         self.pool.close()
