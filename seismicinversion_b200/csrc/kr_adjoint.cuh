@@ -327,3 +327,135 @@ KR_HD void jacobian_pair(int L, cd w, bool free_surface, int seg, const LayerP* 
 }
 
 }  // namespace kr
+
+namespace kr {
+
+// ------------------------------------------------------------------------------------------
+// Frequency sums of the adjoint (misfit gradient, vector-Jacobian products).
+//
+// When only sum over (p, omega) of Re(seed dR/dtheta) is wanted, the contraction with the
+// frequency-independent coefficient tangents and phase-derivative factors can wait until the
+// per-step adjoints are summed over the frequencies:
+//   sum_w Re(cbar_k(w) t_kj) = Re((sum_w cbar_k(w)) t_kj),
+//   sum_w Re(fa(w) ca_alpha) = Re((sum_w fa(w)) ca_alpha),  fa = eabar ea w (likewise eb),
+// so per (omega, p) and step the sweep only hands 12 complex values (the 10 coefficient
+// adjoints of the interface and the phase terms fa, fb of the layer below it) to a summing
+// sink, and one contraction per (p, interface) replaces the per-step 10 x 6 one.
+// ------------------------------------------------------------------------------------------
+constexpr int kSumVals = 12;  // per step: 10 coefficient adjoints, fa, fb
+
+// Sum rows: row i < I holds interface i's 10 coefficient adjoints and the phase terms of
+// layer i + 1 (slots 10, 11); row I holds the top phase term of layer 0 (slot 10).
+KR_HD size_t sum_rows(int L) { return (size_t)L; }
+
+// One (omega, p) pair: forward sweep with the tape of jacobian_pair, seed, reverse sweep; per
+// step sink.step(i, cbar, fa, fb), once sink.top(f0) (the ocean phase term of layer 0).
+#ifdef __CUDACC__
+#pragma nv_exec_check_disable
+#endif
+template <class Sink, class Ph>
+KR_HD void adjoint_pair_sums(int L, cd w, bool free_surface, int seg, const Iface* coef,
+                             const Ph& ph, Sink& sink) {
+  const int I = L - 1;
+  const int nsteps = I - 1;  // step s applies interface i = I - 2 - s
+  const int ncp = nsteps > 0 ? (nsteps + seg - 1) / seg : 0;
+  const int top0 = (ncp - 1) * seg;
+  S3 cp[kCpMax];
+  S3 sg[kSegMax];
+  cd sea[kSegMax], seb[kSegMax];
+  M2 r = m2(coef[I - 1].rd11, coef[I - 1].rd12, coef[I - 1].rd12, coef[I - 1].rd22);
+  for (int s = 0; s < nsteps; ++s) {
+    if (s % seg == 0) cp[s / seg] = s3(r);
+    const int i = I - 2 - s;
+    const cd ea = ph.a(i + 1), eb = ph.b(i + 1);
+    if (s >= top0) {
+      sg[s - top0] = s3(r);
+      sea[s - top0] = ea;
+      seb[s - top0] = eb;
+    }
+    r = kennett_step(r, ea, eb, coef[i]);
+  }
+  const cd e0 = ph.a(0);
+  const cd seed = sink.reflectivity(pp_surface(r.a, e0, free_surface));
+  cd g = mk(1.0, 0.0);
+  if (free_surface) {
+    cd q = recip(1.0 + (e0 * e0) * r.a);
+    g = q * q;
+  }
+  const cd ob0 = ((e0 * e0) * g) * seed;
+  const cd f0 = (2.0 * (e0 * r.a) * g * e0 * w) * seed;
+  sink.top(f0);
+  M2 ob = m2(ob0, mk(0.0, 0.0), mk(0.0, 0.0), mk(0.0, 0.0));
+  for (int q = ncp - 1; q >= 0; --q) {
+    const int s0 = q * seg;
+    const int s1 = s0 + seg < nsteps ? s0 + seg : nsteps;
+    if (q != ncp - 1) {
+      M2 x = m2(cp[q]);
+      for (int s = s0; s < s1; ++s) {
+        const int i = I - 2 - s;
+        const cd ea = ph.a(i + 1), eb = ph.b(i + 1);
+        sg[s - s0] = s3(x);
+        sea[s - s0] = ea;
+        seb[s - s0] = eb;
+        if (s + 1 < s1) x = kennett_step(x, ea, eb, coef[i]);
+      }
+    }
+    for (int s = s1 - 1; s >= s0; --s) {
+      const int i = I - 2 - s;
+      const cd ea = sea[s - s0], eb = seb[s - s0];
+      M2 rb;
+      cd eab, ebb, cbar[10];
+      kennett_step_reverse(m2(sg[s - s0]), ea, eb, coef[i], ob, rb, eab, ebb, cbar);
+      sink.step(i, cbar, eab * ea * w, ebb * eb * w);
+      ob = rb;
+    }
+  }
+  // bottom interface I-1 initialises RRd = Rd (ob.b: the symmetric off-diagonal's adjoint)
+  cd cbar[10];
+  cbar[0] = ob.a;
+  cbar[1] = ob.b;
+  cbar[2] = ob.d;
+  for (int k = 3; k < 10; ++k) cbar[k] = mk(0.0, 0.0);
+  sink.step(I - 1, cbar, mk(0.0, 0.0), mk(0.0, 0.0));
+}
+
+// The contraction of the summed rows for layer l: out[0..3] = Re of the alpha, beta, rho, h
+// contributions (the interface above layer l contributes through its lower-layer tangents,
+// the one below through its upper-layer tangents, plus the layer's phase terms).
+KR_HD void sums_contract_layer(int l, int L, const cd* sums, const ScatTan* tan,
+                               const LayerD* dlay, double out[4]) {
+  const int I = L - 1;
+  double a = 0.0, b = 0.0, r = 0.0, h = 0.0;
+  if (l < I) {  // interface l: layer l is its upper layer (tangent columns 0..2)
+    const cd* S = sums + (size_t)l * kSumVals;
+    for (int k = 0; k < 10; ++k) {
+      acc_add(a, S[k], tan[l].t[k][0]);
+      acc_add(b, S[k], tan[l].t[k][1]);
+      acc_add(r, S[k], tan[l].t[k][2]);
+    }
+  }
+  cd A = mk(0.0, 0.0), B = mk(0.0, 0.0);
+  if (l > 0) {  // interface l - 1: layer l is its lower layer (columns 3..5)
+    const cd* S = sums + (size_t)(l - 1) * kSumVals;
+    for (int k = 0; k < 10; ++k) {
+      acc_add(a, S[k], tan[l - 1].t[k][3]);
+      acc_add(b, S[k], tan[l - 1].t[k][4]);
+      acc_add(r, S[k], tan[l - 1].t[k][5]);
+    }
+    A = S[10];
+    B = S[11];
+  } else {
+    A = sums[(size_t)I * kSumVals + 10];
+  }
+  const LayerD& d = dlay[l];
+  acc_add(a, A, d.ca_alpha);
+  acc_add(b, B, d.cb_beta);
+  acc_add(h, A, d.ca_h);
+  acc_add(h, B, d.cb_h);
+  out[0] = a;
+  out[1] = b;
+  out[2] = r;
+  out[3] = h;
+}
+
+}  // namespace kr

@@ -17,12 +17,14 @@
 // Gradient items reduce their contributions per block in a fixed order and add them to the
 // model's chi_grad with FP64 atomics (the order of those additions across blocks is not
 // fixed: results agree to rounding, ~1e-16 relative, run to run).
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
 #include <vector>
 
 #include "kr_adjoint.cuh"
+#include "kr_adjsum.cuh"
 #include "kr_internal.cuh"
 #include "kr_phase.cuh"
 
@@ -305,6 +307,92 @@ batch_gradient_kernel(unsigned char* plan, const double2* __restrict__ omega_all
   }
 }
 
+// Gradient items with the contraction moved out of the frequency loop (kr_adjsum.cuh): the
+// block's warps sum the per-step adjoints of every frequency of the item, then contract once
+// per (pair, interface).  Dynamic smem: per-warp sum rows (sized for max_layers) and staging
+// tiles, the item's [4L] result, then the item's interface coefficients and layer terms and
+// (models that tabulate) the phase table of its tiles.  Register budget: 384 threads per SM
+// (168 registers, as the gradient sweep of kr_misfit_gradient).
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 384 / THREADS)
+batch_grad_sums_kernel(unsigned char* plan, const double2* __restrict__ omega_all,
+                       const double2* __restrict__ obs_all, double2* __restrict__ R_all,
+                       double* __restrict__ chi_grad, int max_layers, int tab_entries) {
+  constexpr int W = THREADS / 32;
+  extern __shared__ __align__(16) double s_raw[];
+  __shared__ unsigned s_bad;
+  __shared__ double s_chi[W];
+  PlanHeader* h = reinterpret_cast<PlanHeader*>(plan);
+  const kr_model_desc* models = reinterpret_cast<const kr_model_desc*>(plan + h->off_models);
+  const PairRec* pairs = reinterpret_cast<const PairRec*>(plan + h->off_pairs);
+  const ItemRec* items = reinterpret_cast<const ItemRec*>(plan + h->off_grad);
+  const int n_items = h->n_grad;
+  const int warp = threadIdx.x >> 5;
+  cd* acc = reinterpret_cast<cd*>(s_raw);
+  cd* stage = acc + (size_t)W * sum_rows(max_layers) * kSumVals;
+  double* s_out = reinterpret_cast<double*>(stage + W * 32 * kSumStride);
+  unsigned char* area = reinterpret_cast<unsigned char*>(s_out) + a256(32 * (size_t)max_layers);
+  for (;;) {
+    const int it = next_item(&h->counters[1]);
+    if (it >= n_items) break;
+    const ItemRec item = items[it];
+    const PairRec pr = pairs[item.pair];
+    const kr_model_desc d = models[pr.model];
+    const PairView v = pair_view(plan, pr, d);
+    const int L = d.n_layers, I = L - 1;
+    Iface* sc = reinterpret_cast<Iface*>(area);
+    LayerP* sl = reinterpret_cast<LayerP*>(area + sizeof(Iface) * I);
+    cd* s_ph = reinterpret_cast<cd*>(area + prologue_smem_bytes(L));
+    sums_zero(acc, L, W);
+    copy16(sc, v.coef, sizeof(Iface) * I);
+    copy16(sl, v.lay, sizeof(LayerP) * L);
+    __syncthreads();
+    const double2* om = omega_all + d.omega_off;
+    const int u0 = item.w0 / kPhTile;
+    unsigned mask = 0u;
+    if (tab_entries > 0 && phase_table_model(L))
+      mask = build_phase_table(om, d.n_w, grid_line(om, d.n_w), u0,
+                               (item.w0 + item.nw - 1) / kPhTile - u0 + 1, tab_entries, L, sl,
+                               s_ph, &s_bad);
+    const int seg = checkpoint_spacing(L - 2 > 0 ? L - 2 : 1);
+    const bool fs = (d.flags & KR_FREE_SURFACE) != 0;
+    double c2 = 0.0;
+    for (int k0 = 0; k0 < item.nw; k0 += THREADS) {
+      const int iw = item.w0 + k0 + threadIdx.x;
+      const bool valid = k0 + threadIdx.x < item.nw;
+      cd w = mk(0.0, 0.0);
+      if (valid) {
+        const double2 wv = om[iw];
+        w = mk(wv.x, wv.y);
+      }
+      const size_t e = (size_t)pr.j * d.n_w + (valid ? iw : 0);
+      SumSink sink;
+      sink.valid = valid;
+      sink.vjp = false;
+      sink.obs = obs_all + d.obs_off + e;
+      sink.R_out = (d.flags & KR_BATCH_STORE_R) ? R_all + d.R_off + e : nullptr;
+      sink.acc = acc + (size_t)warp * L * kSumVals;
+      sink.stage = stage + warp * 32 * kSumStride;
+      sink.I = I;
+      const int iwt = valid ? iw : item.w0;
+      const PhaseAuto ph{((mask >> (iwt / kPhTile - u0)) & 1u) != 0,
+                         phase_at(s_ph, tab_entries, iwt, u0), PhaseDirect{w, sl}};
+      adjoint_pair_sums(L, w, fs, seg, sc, ph, sink);
+      if (valid) c2 += sink.res.x * sink.res.x + sink.res.y * sink.res.y;
+    }
+    for (int o = 16; o > 0; o >>= 1) c2 += __shfl_down_sync(0xffffffffu, c2, o);
+    if ((threadIdx.x & 31) == 0) s_chi[warp] = c2;
+    sums_finish(acc, L, W, v.tan, v.dlay, s_out);
+    __syncthreads();
+    for (int k = threadIdx.x; k < 4 * L; k += THREADS) atomicAdd(chi_grad + d.grad_off + k, s_out[k]);
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int wi = 0; wi < W; ++wi) t += s_chi[wi];
+      atomicAdd(chi_grad + d.grad_off + 4 * L, t);
+    }
+  }
+}
+
 static int occupancy_grid(const void* fn, int threads, size_t smem) {
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess ||
@@ -438,23 +526,60 @@ static size_t grad_smem(int threads, int max_layers, int tab_entries, int* stage
   return acc + area;
 }
 
+// Dynamic smem of batch_grad_sums_kernel (0 if it does not fit) and the phase-table entries it
+// uses (0: none), for blocks of THREADS threads.
+static size_t sums_smem(int threads, int max_layers, int tab_entries, int* tab) {
+  size_t area = prologue_smem_bytes(max_layers);
+  *tab = 0;
+  if (tab_entries > 0) {
+    const int lt = std::min(max_layers, phase_table_max_layers());
+    area = std::max(area, prologue_smem_bytes(lt) +
+                              sizeof(cd) * (size_t)tab_entries * 2 * (size_t)(lt - 1));
+    *tab = tab_entries;
+  }
+  const size_t smem = adjsum_smem_bytes(max_layers, threads / 32) +
+                      a256(32 * (size_t)max_layers) + area;
+  return smem <= kBatchStageMax ? smem : 0;
+}
+
+// KR_DERIV_SUMS=0 keeps the per-step contraction for gradient items (comparison runs).
+static bool batch_sums_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("KR_DERIV_SUMS");
+    v = (e && atoi(e) == 0) ? 0 : 1;
+  }
+  return v == 1;
+}
+
 template <int THREADS>
 static kr_status grids(PlanHeader& h, int max_layers, int tab_entries, size_t* fsm,
-                       size_t* gsm, int* stage, int* gtab) {
+                       size_t* gsm, int* stage, int* gtab, bool* sums) {
   const int lt = std::min(max_layers, phase_table_max_layers());
   *fsm = fwd_smem(max_layers) +
          (tab_entries ? sizeof(cd) * (size_t)tab_entries * 2 * (size_t)(lt - 1) : 0);
-  *gsm = grad_smem(THREADS, max_layers, tab_entries, stage, gtab);
+  int stab = 0;
+  const size_t ssm = batch_sums_enabled() ? sums_smem(THREADS, max_layers, tab_entries, &stab) : 0;
+  *sums = ssm > 0;
+  if (*sums) {
+    *gsm = ssm;
+    *gtab = stab;
+    *stage = 1;
+  } else {
+    *gsm = grad_smem(THREADS, max_layers, tab_entries, stage, gtab);
+  }
   if (*fsm > 48 * 1024 &&
       cudaFuncSetAttribute(batch_forward_kernel<THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)*fsm) != cudaSuccess)
     return KR_ERR_CUDA;
+  const void* gk = *sums ? (const void*)batch_grad_sums_kernel<THREADS>
+                        : (const void*)batch_gradient_kernel<THREADS>;
   if (*gsm > 48 * 1024 &&
-      cudaFuncSetAttribute(batch_gradient_kernel<THREADS>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*gsm) != cudaSuccess)
+      cudaFuncSetAttribute(gk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*gsm) !=
+          cudaSuccess)
     return KR_ERR_CUDA;
   h.grid_fwd = occupancy_grid((const void*)batch_forward_kernel<THREADS>, THREADS, *fsm);
-  h.grid_grad = occupancy_grid((const void*)batch_gradient_kernel<THREADS>, THREADS, *gsm);
+  h.grid_grad = occupancy_grid(gk, THREADS, *gsm);
   return KR_OK;
 }
 
@@ -551,7 +676,8 @@ static kr_status launch_batch(unsigned char* pl, const kr_batch_config* cfg, int
   int stage = 0;
   const int tab = fwd_table_entries(cfg->tile_w);
   int gtab = 0;
-  kr_status s = grids<THREADS>(h, max_layers, tab, &fsm, &gsm, &stage, &gtab);
+  bool sums = false;
+  kr_status s = grids<THREADS>(h, max_layers, tab, &fsm, &gsm, &stage, &gtab, &sums);
   if (s != KR_OK) {
     set_last_error_msg("kr_batch_launch: shared-memory attribute");
     return s;
@@ -567,9 +693,14 @@ static kr_status launch_batch(unsigned char* pl, const kr_batch_config* cfg, int
       pl, w, reinterpret_cast<double2*>(R), tab);
   s = check_launch("kr_batch_launch: forward");
   if (s != KR_OK) return s;
-  batch_gradient_kernel<THREADS><<<h.grid_grad, THREADS, gsm, st>>>(
-      pl, w, reinterpret_cast<const double2*>(R_obs), reinterpret_cast<double2*>(R), chi_grad,
-      stage, gtab);
+  if (sums)
+    batch_grad_sums_kernel<THREADS><<<h.grid_grad, THREADS, gsm, st>>>(
+        pl, w, reinterpret_cast<const double2*>(R_obs), reinterpret_cast<double2*>(R), chi_grad,
+        max_layers, gtab);
+  else
+    batch_gradient_kernel<THREADS><<<h.grid_grad, THREADS, gsm, st>>>(
+        pl, w, reinterpret_cast<const double2*>(R_obs), reinterpret_cast<double2*>(R), chi_grad,
+        stage, gtab);
   return check_launch("kr_batch_launch: gradient");
 }
 

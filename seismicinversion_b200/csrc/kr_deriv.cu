@@ -21,6 +21,7 @@
 #include <type_traits>
 
 #include "kr_adjoint.cuh"
+#include "kr_adjsum.cuh"
 #include "kr_internal.cuh"
 #include "kr_phase.cuh"
 
@@ -259,20 +260,88 @@ reduce_partials_kernel(const double* __restrict__ partial, int n_blocks, int str
   if (threadIdx.x == 0) out[k] = s[0];
 }
 
+// GRAD / VJP with the contraction moved out of the frequency loop (kr_adjsum.cuh): block =
+// one slowness x 128 frequencies; dynamic smem: per-warp sum rows and staging tiles, then the
+// slowness's interface coefficients and layer terms, then (table models) the phase table.
+// Writes the block's [4L] contributions and chi to partial[block][4L + 1].
+template <int MINB>
+__global__ void __launch_bounds__(kDerThreads, MINB)
+deriv_sum_kernel(int L, int n_p, const double2* __restrict__ omega, int n_w, int n_wtiles,
+                 int free_surface, int vjp, int seg, int table, const LayerP* __restrict__ lay_all,
+                 const LayerD* __restrict__ dlay_all, const Iface* __restrict__ coef_all,
+                 const ScatTan* __restrict__ tan_all, const double2* __restrict__ obs,
+                 double2* __restrict__ R_out, double* __restrict__ partial) {
+  constexpr int W = kDerThreads / 32;
+  extern __shared__ __align__(16) double s_raw[];
+  __shared__ unsigned s_bad;
+  __shared__ double s_chi[W];
+  const int I = L - 1;
+  const int ip = blockIdx.x / n_wtiles;
+  const int tile = blockIdx.x % n_wtiles;
+  const int iw = tile * kDerThreads + threadIdx.x;
+  const bool valid = iw < n_w;
+  const int warp = threadIdx.x >> 5;
+  cd* acc = reinterpret_cast<cd*>(s_raw);
+  cd* stage = acc + (size_t)W * sum_rows(L) * kSumVals;
+  unsigned char* b = reinterpret_cast<unsigned char*>(stage + W * 32 * kSumStride);
+  Iface* sc = reinterpret_cast<Iface*>(b);
+  LayerP* sl = reinterpret_cast<LayerP*>(b + sizeof(Iface) * I);
+  cd* s_ph = reinterpret_cast<cd*>(b + sizeof(Iface) * I + sizeof(LayerP) * L);
+  sums_zero(acc, L, W);
+  copy16(sc, coef_all + (size_t)ip * I, sizeof(Iface) * I);
+  copy16(sl, lay_all + (size_t)ip * L, sizeof(LayerP) * L);
+  __syncthreads();
+  cd w = mk(0.0, 0.0);
+  if (valid) {
+    const double2 wv = omega[iw];
+    w = mk(wv.x, wv.y);
+  }
+  bool use_tab = false;
+  if (table)
+    use_tab = (build_phase_table(omega, n_w, grid_line(omega, n_w), tile, 1, kPhHead + 1, L, sl,
+                                 s_ph, &s_bad) & 1u) != 0;
+  const PhaseAuto ph{use_tab, phase_at(s_ph, kPhHead + 1, valid ? iw : tile * kDerThreads, tile),
+                     PhaseDirect{w, sl}};
+  const size_t e = (size_t)ip * n_w + (valid ? iw : 0);
+  SumSink sink;
+  sink.valid = valid;
+  sink.vjp = vjp != 0;
+  sink.obs = obs + e;
+  sink.R_out = R_out ? R_out + e : nullptr;
+  sink.acc = acc + (size_t)warp * sum_rows(L) * kSumVals;
+  sink.stage = stage + warp * 32 * kSumStride;
+  sink.I = I;
+  adjoint_pair_sums(L, w, free_surface != 0, seg, sc, ph, sink);
+  double c2 = valid ? (sink.res.x * sink.res.x + sink.res.y * sink.res.y) : 0.0;
+  for (int o = 16; o > 0; o >>= 1) c2 += __shfl_down_sync(0xffffffffu, c2, o);
+  if ((threadIdx.x & 31) == 0) s_chi[warp] = c2;
+  double* dst = partial + (size_t)blockIdx.x * (4 * L + 1);
+  sums_finish(acc, L, W, tan_all + (size_t)ip * I, dlay_all + (size_t)ip * L, dst);
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int wi = 0; wi < W; ++wi) t += s_chi[wi];
+    dst[4 * L] = t;
+  }
+}
+
 // Shared memory the sweep may use for staging one slowness's data (per block).
 constexpr size_t kStageSmemMax = 160 * 1024;
 
-// Register budget of the sweep kernel: blocks of 128 threads per SM (2 -> up to 255
-// registers, 3 -> 168).  KR_DERIV_MINB or kr_set_deriv_variant; default 2.
-static int g_deriv_minb = 0;
+// Register budget of the sweep kernels: blocks of 128 threads per SM (2 -> up to 255
+// registers, 3 -> 168).  KR_DERIV_MINB or kr_set_deriv_variant; 0 (default) = automatic:
+// 3 for the frequency-sum kernel (168 registers, no spills), 2 for the per-pair kernel.
+static int g_deriv_minb = -1;
 
-static int deriv_minb() {
-  if (g_deriv_minb == 0) {
+static int deriv_minb_setting() {
+  if (g_deriv_minb < 0) {
     const char* e = getenv("KR_DERIV_MINB");
-    g_deriv_minb = (e && atoi(e) == 3) ? 3 : 2;
+    const int v = e ? atoi(e) : 0;
+    g_deriv_minb = (v == 2 || v == 3) ? v : 0;
   }
   return g_deriv_minb;
 }
+static int deriv_minb() { return deriv_minb_setting() == 3 ? 3 : 2; }
+static int sum_minb() { return deriv_minb_setting() == 2 ? 2 : 3; }
 
 template <int MODE, int MINB>
 static kr_status launch_sweep_v(unsigned blocks, size_t smem, cudaStream_t st, int L,
@@ -307,6 +376,41 @@ static kr_status launch_sweep(int minb, unsigned blocks, size_t smem, cudaStream
                                  stage, table, lay, dlay, coef, tan, R_obs, R, J, partial);
 }
 
+// Dynamic smem of deriv_sum_kernel for a model of L layers (0 if it does not fit).
+static size_t sum_kernel_smem(int L, int table) {
+  const size_t smem = adjsum_smem_bytes(L, kDerThreads / 32) + prologue_smem_bytes(L) +
+                      (table ? phase_table_bytes(L, 1) : 0);
+  return smem <= kStageSmemMax ? smem : 0;
+}
+
+// KR_DERIV_SUMS=0 keeps the per-step contraction for GRAD / VJP (comparison runs).
+static bool deriv_sums_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("KR_DERIV_SUMS");
+    v = (e && atoi(e) == 0) ? 0 : 1;
+  }
+  return v == 1;
+}
+
+template <int MINB>
+static kr_status launch_sum_v(unsigned blocks, size_t smem, cudaStream_t st, int L, int n_p,
+                              const double2* omega, int n_w, int n_wtiles, int fs, int vjp,
+                              int seg, int table, const LayerP* lay, const LayerD* dlay,
+                              const Iface* coef, const ScatTan* tan, const double2* obs,
+                              double2* R, double* partial) {
+  static SmemLimit lim;
+  if (smem > 48 * 1024) {
+    const kr_status a = raise_smem_limit((const void*)deriv_sum_kernel<MINB>, smem, lim,
+                                         "kr_deriv: smem attribute");
+    if (a != KR_OK) return a;
+  }
+  deriv_sum_kernel<MINB><<<blocks, kDerThreads, smem, st>>>(L, n_p, omega, n_w, n_wtiles, fs, vjp,
+                                                            seg, table, lay, dlay, coef, tan, obs,
+                                                            R, partial);
+  return KR_OK;
+}
+
 template <int MODE>
 static kr_status launch_deriv(const double* layers, int L, const double* p, int n_p,
                               const double* omega, int n_w, uint32_t flags, const double* R_obs,
@@ -328,6 +432,29 @@ static kr_status launch_deriv(const double* layers, int L, const double* p, int 
   s = check_launch("kr_deriv: interfaces");
   if (s != KR_OK) return s;
   const int seg = checkpoint_spacing(I - 1 > 0 ? I - 1 : 1);
+  if (GRAD && deriv_sums_enabled()) {
+    const int table = phase_table_model(L) ? 1 : 0;
+    const size_t smem = sum_kernel_smem(L, table);
+    if (smem) {
+      const int fs = (flags & KR_FREE_SURFACE) ? 1 : 0;
+      const int vjp = MODE == kModeVjp ? 1 : 0;
+      const double2* o = reinterpret_cast<const double2*>(R_obs);
+      const double2* w2 = reinterpret_cast<const double2*>(omega);
+      double2* R2 = reinterpret_cast<double2*>(R);
+      s = sum_minb() == 3
+              ? launch_sum_v<3>((unsigned)n_blocks, smem, st, L, n_p, w2, n_w, n_wtiles, fs, vjp,
+                                seg, table, w.lay, w.dlay, w.coef, w.tan, o, R2, w.partial)
+              : launch_sum_v<2>((unsigned)n_blocks, smem, st, L, n_p, w2, n_w, n_wtiles, fs, vjp,
+                                seg, table, w.lay, w.dlay, w.coef, w.tan, o, R2, w.partial);
+      if (s != KR_OK) return s;
+      s = check_launch("kr_deriv: sweep");
+      if (s != KR_OK) return s;
+      const int nv = 4 * L + 1;
+      reduce_partials_kernel<<<MODE == kModeGrad ? nv : nv - 1, 256, 0, st>>>(
+          w.partial, (int)n_blocks, nv, chi_grad);
+      return check_launch("kr_deriv: reduce");
+    }
+  }
   // accumulators: [warps][4L + 1] doubles, padded to 16 bytes
   const size_t acc = GRAD ? sizeof(double) * (((size_t)(kDerThreads / 32) * (4 * L + 1) + 1) / 2 * 2) : 0;
   const size_t pair = pair_smem_bytes(L);
@@ -366,7 +493,7 @@ static kr_status deriv_args(const double* layers, int L, const double* p, int n_
 using namespace kr;
 
 extern "C" void kr_set_deriv_variant(int32_t min_blocks_per_sm) {
-  g_deriv_minb = (min_blocks_per_sm == 3) ? 3 : 2;
+  g_deriv_minb = (min_blocks_per_sm == 2 || min_blocks_per_sm == 3) ? min_blocks_per_sm : 0;
 }
 
 extern "C" size_t kr_jacobian_workspace_bytes(int32_t n_layers, int32_t n_p, int32_t n_w) {

@@ -148,3 +148,65 @@ extern "C" void emu_hvp(const double* tab, int L, const double* p, int n_p, cons
     }
   }
 }
+
+// ---- frequency sums of the adjoint (adjoint_pair_sums + sums_contract_layer), the path of
+// the gradient / vector-Jacobian-product kernels ----
+namespace {
+struct HostSumSink {
+  cd* sums;  // [L][12] of this slowness, summed over the frequencies
+  int I;
+  bool vjp;
+  cd obs;
+  cd res;
+  cd reflectivity(cd R) {
+    if (vjp) { res = mk(0.0, 0.0); return mk(obs.x, -obs.y); }
+    res = R - obs;
+    return mk(2.0 * res.x, -2.0 * res.y);
+  }
+  void top(cd f0) { sums[(size_t)I * kSumVals + 10] = sums[(size_t)I * kSumVals + 10] + f0; }
+  void step(int i, const cd cbar[10], cd fa, cd fb) {
+    cd* row = sums + (size_t)i * kSumVals;
+    for (int k = 0; k < 10; ++k) row[k] = row[k] + cbar[k];
+    row[10] = row[10] + fa;
+    row[11] = row[11] + fb;
+  }
+};
+}  // namespace
+
+// out[4L + 1]: the misfit gradient (vjp = 0, obs = R_obs) or Re sum conj(gR) dR/dtheta
+// (vjp = 1, obs = gR) over all slownesses and frequencies, then chi.
+extern "C" void emu_gradient_sums(const double* tab, int L, const double* p, int n_p,
+                                  const double* w, int nw, int fs, int vjp, const double* obs,
+                                  double* out) {
+  static LayerP lay[512];
+  static LayerD dlay[512];
+  static Iface f[512];
+  static ScatTan t[512];
+  static cd sums[512 * kSumVals];
+  const int I = L - 1;
+  for (int q = 0; q < 4 * L + 1; ++q) out[q] = 0.0;
+  for (int j = 0; j < n_p; ++j) {
+    for (int l = 0; l < L; ++l) {
+      lay[l] = layer_terms(tab, L, l, p[j]);
+      dlay[l] = layer_derivs(tab, L, l, p[j], lay[l]);
+    }
+    for (int i = 0; i < I; ++i) {
+      f[i] = interface_coeffs(p[j], i, lay[i], lay[i + 1]);
+      interface_tangents(p[j], i, lay[i], dlay[i], lay[i + 1], dlay[i + 1], t[i]);
+    }
+    for (size_t q = 0; q < sum_rows(L) * kSumVals; ++q) sums[q] = mk(0.0, 0.0);
+    const int seg = checkpoint_spacing(I - 1 > 0 ? I - 1 : 1);
+    for (int k = 0; k < nw; ++k) {
+      const cd om = mk(w[2 * k], w[2 * k + 1]);
+      HostSumSink s{sums, I, vjp != 0, mk(obs[2 * ((size_t)j * nw + k)],
+                                          obs[2 * ((size_t)j * nw + k) + 1]), mk(0.0, 0.0)};
+      adjoint_pair_sums(L, om, fs != 0, seg, f, PhaseDirect{om, lay}, s);
+      out[4 * L] += s.res.x * s.res.x + s.res.y * s.res.y;
+    }
+    for (int l = 0; l < L; ++l) {
+      double v[4];
+      sums_contract_layer(l, L, sums, t, dlay, v);
+      for (int q = 0; q < 4; ++q) out[q * L + l] += v[q];
+    }
+  }
+}
