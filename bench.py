@@ -443,12 +443,17 @@ def bench_inversion(torch, dev, reps, cpu=True):
                              "s_per_iteration": dt / max(res.n_iterations, 1),
                              "param_err_history": list(map(float, res.param_error_history)),
                              "misfit_history": list(map(float, res.misfit_history))}
-    # the reference's own start (uniform +-10 %, seed 42) and its invert_taup trajectory on
-    # this workload (tests/golden/invert_c2.npz, the reference run on the CPU)
+    # the reference's own start (uniform +-10 %, seed 42) and its invert_taup trajectory on this
+    # model at 16 slownesses x 64 frequencies (tests/golden/invert_c2.npz, the reference run on
+    # the CPU; at 64 x 1024 the reference needs about a day)
     gold = ROOT / "tests" / "golden" / "invert_c2.npz"
-    res = invert_taup(true, list(p), nfreq=1024, perturbation=0.1, max_iter=10, seed=42,
-                      hessian="exact", tol=0.0)
-    traj = {"param_err_history": list(map(float, res.param_error_history)),
+    t0 = time.perf_counter()
+    res = invert_taup(true, list(np.linspace(0.05, 0.6, 16)), nfreq=64, perturbation=0.1,
+                      max_iter=10, seed=42, hessian="exact", tol=0.0)
+    traj = {"workload": "21 layers, 16 p on [0.05, 0.6] x 64 omega, uniform +-10 % start "
+                        "(seed 42), exact Hessian, 10 iterations",
+            "seconds": time.perf_counter() - t0,
+            "param_err_history": list(map(float, res.param_error_history)),
             "misfit_history": list(map(float, res.misfit_history))}
     if gold.exists():
         with np.load(gold) as g:

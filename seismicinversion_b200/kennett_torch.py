@@ -87,8 +87,9 @@ def _jacobian_dot(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_s
 
 def _second_derivatives(args, free_surface, L):
     """d^2 R / d theta_m d theta_k for every m: [4L, n_p, 4L, n_w] (one launch over the basis)."""
-    V = torch.eye(4 * L, dtype=_FDTYPE)
-    return _jacobian_dot(*args, free_surface, V)
+    with torch._C._DisableFuncTorch():
+        V = torch.eye(4 * L, dtype=_FDTYPE)
+        return _jacobian_dot(*args, free_surface, V)
 
 
 def _vjp(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface, gR):
@@ -98,6 +99,25 @@ def _vjp(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface, g
     p_t = torch.as_tensor(p, dtype=_FDTYPE).detach().reshape(-1)
     g, _ = D.vjp(tab, p_t, torch.as_tensor(omega).detach(), gR, free_surface)
     return g
+
+
+def _value(t, dtype=None) -> torch.Tensor:
+    """The plain value of a tensor that torch.func transforms may have wrapped (grad / jvp
+    levels), optionally converted: the kernels read raw device memory."""
+    t = torch.as_tensor(t)
+    while torch._C._functorch.is_functorch_wrapped_tensor(t):
+        t = torch._C._functorch.get_unwrapped(t)
+    with torch._C._DisableFuncTorch():
+        t = t.detach()
+        return t if dtype is None else t.to(dtype)
+
+
+def _plain_call(fn, *args):
+    """Runs a kernel wrapper outside the active torch.func transforms, so that the tensors it
+    creates are plain device memory (its result enters the transformed computation as a
+    constant)."""
+    with torch._C._DisableFuncTorch():
+        return fn(*args)
 
 
 def _split(g, L, ctx):
@@ -155,7 +175,7 @@ class _KennettFunction(torch.autograd.Function):
     @staticmethod
     def _model(saved):
         """Value-only model arguments (alpha .. omega) from the saved tensors."""
-        return [x.detach().to(_FDTYPE) for x in saved[:4]] + list(saved[4:8])
+        return [_value(x, _FDTYPE) for x in saved[:4]] + [_value(x) for x in saved[4:8]]
 
     @staticmethod
     def backward(ctx, gR, gJ):
@@ -169,7 +189,7 @@ class _KennettFunction(torch.autograd.Function):
             wrapped = torch._C._functorch.is_functorch_wrapped_tensor(gR)
             if not wrapped and not torch.is_grad_enabled():
                 # the adjoint kernel: one reverse sweep per (p, omega), no Jacobian formed
-                return _split(_vjp(*args, ctx.free_surface, gR.detach()), L, ctx)
+                return _split(_plain_call(_vjp, *args, ctx.free_surface, _value(gR)), L, ctx)
             if torch.is_grad_enabled() and not wrapped:
                 # a differentiable backward (create_graph=True): the Jacobian as a
                 # differentiable function of the layer inputs (JAC mode), so that a second
@@ -178,7 +198,7 @@ class _KennettFunction(torch.autograd.Function):
             else:
                 # a transformed backward (vmap over cotangents): contract the Jacobian with
                 # tensor operations
-                _, J = _compute(*args, ctx.free_surface, True)
+                _, J = _plain_call(_compute, *args, ctx.free_surface, True)
                 if ctx.scalar_p:
                     J = J[0]
             J = J.to(gR.device)
@@ -227,7 +247,9 @@ class _KennettFunction(torch.autograd.Function):
                 T = T[:, 0]
             dJ = (T * v.to(_CDTYPE).reshape((4 * L,) + (1,) * (T.dim() - 1))).sum(0)
         else:
-            dJ = _jacobian_dot(*args, ctx.free_surface, v.detach().reshape(1, -1))[0].to(J.device)
+            with torch._C._DisableFuncTorch():
+                dJ = _jacobian_dot(*args, ctx.free_surface, _value(v).reshape(1, -1))[0]
+            dJ = dJ.to(J.device)
             if ctx.scalar_p:
                 dJ = dJ[0]
         return dR, dJ

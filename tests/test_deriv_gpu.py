@@ -550,3 +550,27 @@ def test_c2_1024_jacobians_and_gradient_vs_reference(golden):
 
     H_ref = torch.func.hessian(chi_cpu)(m).numpy()
     assert rel_err(H, H_ref) < 1e-10
+
+
+def test_invert_taup_trajectory_vs_reference_21_layers(golden):
+    """invert_taup with the exact (tangent-of-adjoint) Hessian follows the reference's own
+    invert_taup (torch.func.hessian per slowness) on the 21-layer inversion model from the
+    same uniform +-10 % start, 16 slownesses x 64 frequencies, 10 iterations: the same start,
+    misfits and parameter errors at every iteration to 1e-6 relative."""
+    import os
+
+    from conftest import GOLDEN
+    from seismicinversion_b200.earth_models import random_layered_model
+    from seismicinversion_b200.taup_inversion import invert_taup
+
+    if not os.path.exists(GOLDEN / "invert_c2.npz"):
+        pytest.skip("reference trajectory fixture not generated")
+    g = golden("invert_c2.npz")
+    res = invert_taup(random_layered_model(20, seed=2), list(np.linspace(0.05, 0.6, 16)),
+                      nfreq=64, perturbation=0.1, max_iter=10, seed=42, tol=0.0)
+    assert np.allclose(res.initial_model.alpha, g["init_alpha"], rtol=1e-14)
+    n = int(g["n_iter"])
+    assert res.n_iterations == n
+    assert np.allclose(res.misfit_history, g["misfit"], rtol=1e-6, atol=0)
+    assert np.allclose(res.param_error_history, g["param_err"], rtol=1e-6, atol=0)
+    assert np.allclose(res.recovered_model.alpha, g["rec_alpha"], rtol=1e-6)

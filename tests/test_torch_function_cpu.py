@@ -14,8 +14,17 @@ import torch
 import seismicinversion_b200.kennett_torch as KT
 
 
+def _plain(*args):
+    """The kernels read raw device memory: like them, the stand-ins refuse tensors that a
+    torch.func transform has wrapped."""
+    for a in args:
+        if isinstance(a, torch.Tensor):
+            assert not torch._C._functorch.is_functorch_wrapped_tensor(a), "wrapped tensor"
+
+
 def _fake_compute(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface, need_jac):
     # R(w) = sum_k sum_l c[k, l](w) * x_k[l]^2  (nonlinear, known derivative)
+    _plain(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega)
     xs = [torch.as_tensor(t, dtype=torch.float64).detach() for t in (alpha, beta, rho, thickness)]
     L = xs[0].shape[0]
     w = torch.as_tensor(omega).detach().to(torch.complex128)
@@ -40,6 +49,7 @@ def _recording_compute(*args):
 
 
 def _fake_vjp(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface, gR):
+    _plain(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, gR)
     CALLS.append(("vjp", tuple(gR.shape)))
     _, J = _fake_compute(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface, True)
     g = gR.reshape(J.shape[0], -1).conj().unsqueeze(-2) * J
@@ -48,6 +58,7 @@ def _fake_vjp(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surfa
 
 def _fake_jacobian_dot(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, free_surface, V):
     # d/dv of J[k L + l] = 2 c[k, l] x_k[l]  is  2 c[k, l] v[k L + l]
+    _plain(alpha, beta, rho, thickness, Q_alpha, Q_beta, p, omega, V)
     CALLS.append(("jdot", int(V.shape[0])))
     L = torch.as_tensor(alpha).shape[0]
     w = torch.as_tensor(omega).detach().to(torch.complex128)
