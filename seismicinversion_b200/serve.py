@@ -62,6 +62,27 @@ class Request:
     error: BaseException | None = None
     cancelled: bool = False
     _lease: object = None
+    _callbacks: list = field(default_factory=list)
+    _cb_lock: threading.Lock = field(default_factory=threading.Lock)
+
+    def add_done_callback(self, fn) -> None:
+        """Calls ``fn(request)`` once the request is done (at once if it already is), on the
+        thread that completes it."""
+        with self._cb_lock:
+            if not self.done.is_set():
+                self._callbacks.append(fn)
+                return
+        fn(self)
+
+    def _finish(self) -> None:
+        with self._cb_lock:
+            self.done.set()
+            cbs, self._callbacks = self._callbacks, []
+        for fn in cbs:
+            try:
+                fn(self)
+            except Exception:  # a client callback must not stop the scheduler
+                pass
 
     def wait(self, timeout: float | None = None) -> dict:
         if not self.done.wait(timeout):
@@ -274,31 +295,32 @@ class KennettServer:
         except (ValueError, RequestRejected) as e:
             req.error = e if isinstance(e, RequestRejected) else RequestRejected(str(e))
             req.t_done = time.perf_counter()
-            req.done.set()
+            req._finish()
             return req
         with self._lock:
-            if len(self._pending) >= self.max_pending:
-                req.error = RequestRejected("queue full")
-                req.t_done = time.perf_counter()
-                req.done.set()
-                return req
-            req.id = self._next_id
-            self._next_id += 1
-            self._pending.append(req)
-            self._wake.notify()
+            full = len(self._pending) >= self.max_pending
+            if not full:
+                req.id = self._next_id
+                self._next_id += 1
+                self._pending.append(req)
+                self._wake.notify()
+        if full:
+            req.error = RequestRejected("queue full")
+            req.t_done = time.perf_counter()
+            req._finish()
         return req
 
     def cancel(self, req: Request) -> bool:
         """Cancel a request that has not been admitted yet (True if it was)."""
         with self._lock:
-            if req in self._pending:
-                self._pending.remove(req)
-                req.cancelled = True
-                req.error = RequestRejected("cancelled")
-                req.t_done = time.perf_counter()
-                req.done.set()
-                return True
-        return False
+            if req not in self._pending:
+                return False
+            self._pending.remove(req)
+        req.cancelled = True
+        req.error = RequestRejected("cancelled")
+        req.t_done = time.perf_counter()
+        req._finish()
+        return True
 
     def close(self, timeout: float = 60.0) -> None:
         with self._lock:
@@ -359,9 +381,10 @@ class KennettServer:
                             r.error = err
                             self._used -= r.nbytes
                         r.t_done = now
-                        r.done.set()
                         self.completed.append(_Record(r.t_submit, r.t_admit, r.t_launched,
                                                       r.t_done, err is None))
+                for r in reqs:  # outside the lock: completion runs client callbacks
+                    r._finish()
                 del lease, res
             else:
                 still.append((handle, reqs))
@@ -398,7 +421,8 @@ class KennettServer:
                         for r in group:
                             r.error, r.t_done = e, now
                             self._used -= r.nbytes
-                            r.done.set()
+                    for r in group:
+                        r._finish()
             elif self._inflight:
                 time.sleep(self.poll)
 
