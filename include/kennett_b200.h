@@ -349,8 +349,7 @@ void kr_set_forward_variant(int32_t min_blocks_per_sm);
 /*
  * Tuning knob (no counterpart in the reference): register budget of the kr_jacobian /
  * kr_misfit_gradient / kr_vjp sweep kernels as 128-thread blocks per SM (2 -> up to 255
- * registers, 3 -> 168; other values restore the automatic choice: 3 for the gradient and
- * vector-Jacobian sweeps, 2 for the Jacobian sweep).  Process-wide; results do not depend on it.
+ * registers, 3 -> 168; other values select 2).  Process-wide; results do not depend on it.
  */
 void kr_set_deriv_variant(int32_t min_blocks_per_sm);
 

@@ -363,6 +363,9 @@ KR_HD void adjoint_pair_sums(int L, cd w, bool free_surface, int seg, const Ifac
   S3 cp[kCpMax];
   S3 sg[kSegMax];
   cd sea[kSegMax], seb[kSegMax];
+  // tabulated phase factors are recomputed in the reverse sweep (two products each) instead of
+  // kept on the tape: 48 instead of 80 bytes of local memory per step
+  const bool keep_ph = !ph.cheap();
   M2 r = m2(coef[I - 1].rd11, coef[I - 1].rd12, coef[I - 1].rd12, coef[I - 1].rd22);
   for (int s = 0; s < nsteps; ++s) {
     if (s % seg == 0) cp[s / seg] = s3(r);
@@ -370,8 +373,10 @@ KR_HD void adjoint_pair_sums(int L, cd w, bool free_surface, int seg, const Ifac
     const cd ea = ph.a(i + 1), eb = ph.b(i + 1);
     if (s >= top0) {
       sg[s - top0] = s3(r);
-      sea[s - top0] = ea;
-      seb[s - top0] = eb;
+      if (keep_ph) {
+        sea[s - top0] = ea;
+        seb[s - top0] = eb;
+      }
     }
     r = kennett_step(r, ea, eb, coef[i]);
   }
@@ -395,14 +400,17 @@ KR_HD void adjoint_pair_sums(int L, cd w, bool free_surface, int seg, const Ifac
         const int i = I - 2 - s;
         const cd ea = ph.a(i + 1), eb = ph.b(i + 1);
         sg[s - s0] = s3(x);
-        sea[s - s0] = ea;
-        seb[s - s0] = eb;
+        if (keep_ph) {
+          sea[s - s0] = ea;
+          seb[s - s0] = eb;
+        }
         if (s + 1 < s1) x = kennett_step(x, ea, eb, coef[i]);
       }
     }
     for (int s = s1 - 1; s >= s0; --s) {
       const int i = I - 2 - s;
-      const cd ea = sea[s - s0], eb = seb[s - s0];
+      const cd ea = keep_ph ? sea[s - s0] : ph.a(i + 1);
+      const cd eb = keep_ph ? seb[s - s0] : ph.b(i + 1);
       M2 rb;
       cd eab, ebb, cbar[10];
       kennett_step_reverse(m2(sg[s - s0]), ea, eb, coef[i], ob, rb, eab, ebb, cbar);

@@ -311,10 +311,10 @@ batch_gradient_kernel(unsigned char* plan, const double2* __restrict__ omega_all
 // block's warps sum the per-step adjoints of every frequency of the item, then contract once
 // per (pair, interface).  Dynamic smem: per-warp sum rows (sized for max_layers) and staging
 // tiles, the item's [4L] result, then the item's interface coefficients and layer terms and
-// (models that tabulate) the phase table of its tiles.  Register budget: 384 threads per SM
-// (168 registers, as the gradient sweep of kr_misfit_gradient).
+// (models that tabulate) the phase table of its tiles.  Register budget: 256 threads per SM
+// (its shared memory admits two 128-thread blocks per SM; a 168-register cap only spills).
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS, 384 / THREADS)
+__global__ void __launch_bounds__(THREADS, 256 / THREADS)
 batch_grad_sums_kernel(unsigned char* plan, const double2* __restrict__ omega_all,
                        const double2* __restrict__ obs_all, double2* __restrict__ R_all,
                        double* __restrict__ chi_grad, int max_layers, int tab_entries) {

@@ -328,8 +328,9 @@ deriv_sum_kernel(int L, int n_p, const double2* __restrict__ omega, int n_w, int
 constexpr size_t kStageSmemMax = 160 * 1024;
 
 // Register budget of the sweep kernels: blocks of 128 threads per SM (2 -> up to 255
-// registers, 3 -> 168).  KR_DERIV_MINB or kr_set_deriv_variant; 0 (default) = automatic:
-// 3 for the frequency-sum kernel (168 registers, no spills), 2 for the per-pair kernel.
+// registers, 3 -> 168).  KR_DERIV_MINB or kr_set_deriv_variant; default 2.  (The
+// frequency-sum kernel fits 168 registers without spills, but three of its blocks leave too
+// little L1 for the tape: 0.154 ms vs 0.138 ms per 64 x 1024 gradient.)
 static int g_deriv_minb = -1;
 
 static int deriv_minb_setting() {
@@ -341,7 +342,7 @@ static int deriv_minb_setting() {
   return g_deriv_minb;
 }
 static int deriv_minb() { return deriv_minb_setting() == 3 ? 3 : 2; }
-static int sum_minb() { return deriv_minb_setting() == 2 ? 2 : 3; }
+static int sum_minb() { return deriv_minb(); }
 
 template <int MODE, int MINB>
 static kr_status launch_sweep_v(unsigned blocks, size_t smem, cudaStream_t st, int L,

@@ -130,6 +130,8 @@ struct PhaseDirect {
   const LayerP* lay;
   KR_HD cd a(int l) const { return cexp_(w * lay[l].ca); }
   KR_HD cd b(int l) const { return cexp_(w * lay[l].cb); }
+  // whether a factor is cheaper to recompute than to keep (a tabulated source: two products)
+  KR_HD bool cheap() const { return false; }
 };
 
 // Layer table layout (device or host): 6 rows of n_layers doubles:

@@ -74,6 +74,7 @@ struct PhaseTable {
   }
   __device__ __forceinline__ cd a(int l) const { return at(2 * l); }
   __device__ __forceinline__ cd b(int l) const { return at(2 * l + 1); }
+  __device__ __forceinline__ bool cheap() const { return true; }
 };
 
 // Either source, chosen per block (a uniform branch), so that callers compile once.
@@ -83,6 +84,7 @@ struct PhaseAuto {
   PhaseDirect d;
   __device__ __forceinline__ cd a(int l) const { return tab ? t.a(l) : d.a(l); }
   __device__ __forceinline__ cd b(int l) const { return tab ? t.b(l) : d.b(l); }
+  __device__ __forceinline__ bool cheap() const { return tab; }
 };
 
 // The same factors with the per-tile products hi[u] * mid[m] formed once per tile
