@@ -9,6 +9,8 @@ NumPy on the CPU, J0 in SciPy on the CPU and the sum in float32 on the device.
 
 from __future__ import annotations
 
+import threading
+
 import numpy as np
 import torch
 
@@ -188,8 +190,21 @@ def compute_gather_gpu(model: LayerModel, offsets, T: float = 64.0, nw: int = 20
     the reference.  ``copy_outputs=False`` instead returns the R grid as a view of this
     module's pinned receive buffer (no 268 MB host copy on the 8192 x 2047 grid), valid until
     the next call with the same grid overwrites it.  Calls share module-level staging
-    buffers, grid caches and graphs: callers on several threads must serialise them.
+    buffers, grid caches and graphs under one lock: calls from several threads run one at a
+    time.
     """
+    with _CALL_LOCK:
+        return _compute_gather_gpu(model, offsets, T, nw, np_slow, p_max, gamma, source_func,
+                                   free_surface, device, return_reflectivity, copy_chunks,
+                                   use_graph, copy_outputs)
+
+
+_CALL_LOCK = threading.RLock()
+
+
+def _compute_gather_gpu(model, offsets, T, nw, np_slow, p_max, gamma, source_func,
+                        free_surface, device, return_reflectivity, copy_chunks, use_graph,
+                        copy_outputs):
     dev = _dev.require_cuda(device)
     if gamma is None:
         gamma = np.pi / T
