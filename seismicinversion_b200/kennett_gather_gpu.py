@@ -187,9 +187,10 @@ def compute_gather_gpu(model: LayerModel, offsets, T: float = 64.0, nw: int = 20
     8192 x 2047 grid at ~57 GB/s; more blocks shorten the launches below full waves).
     With ``use_graph`` a grid seen before (same sizes, offsets, source, layer count and
     options) replays a captured CUDA graph.  Every returned array is the caller's own, as in
-    the reference.  ``copy_outputs=False`` instead returns the R grid as a view of this
-    module's pinned receive buffer (no 268 MB host copy on the 8192 x 2047 grid), valid until
-    the next call with the same grid overwrites it.  Calls share module-level staging
+    the reference.  With ``return_reflectivity``, ``copy_outputs=False`` instead returns the
+    gather and the R grid as views of this module's pinned receive buffers (no host copy of
+    the 268 MB grid on the 8192 x 2047 workload), valid until the next call with the same grid
+    overwrites them.  Calls share module-level staging
     buffers, grid caches and graphs under one lock: calls from several threads run one at a
     time.
     """
@@ -240,9 +241,10 @@ def _compute_gather_gpu(model, offsets, T, nw, np_slow, p_max, gamma, source_fun
         copy.synchronize()
     main.synchronize()
     if return_reflectivity:
-        Rn = Rh.numpy()
-        return (time.copy(), np.asarray(offsets), gh.numpy().copy(),
-                Rn.copy() if copy_outputs else Rn)
+        Rn, gn = Rh.numpy(), gh.numpy()
+        if copy_outputs:
+            Rn, gn = Rn.copy(), gn.copy()
+        return time.copy(), np.asarray(offsets), gn, Rn
     return time.copy(), np.asarray(offsets), gh.numpy().copy()
 
 

@@ -212,8 +212,8 @@ def test_graph_replay_matches_eager(return_reflectivity):
 def test_consecutive_calls_return_independent_arrays():
     """Every array compute_gather_gpu returns belongs to the caller (the reference returns
     fresh arrays): a second call on the same grid, through the replayed graph, leaves the
-    first call's R grid and gather untouched; copy_outputs=False returns the receive buffer
-    itself, which the next call overwrites."""
+    first call's R grid and gather untouched; copy_outputs=False returns the receive buffers
+    themselves, which the next call overwrites."""
     from seismicinversion_b200 import compute_gather_gpu
     from seismicinversion_b200.earth_models import random_layered_model
 
@@ -227,10 +227,11 @@ def test_consecutive_calls_return_independent_arrays():
         _, _, g2, R2 = compute_gather_gpu(m2, offs, **kw)
         assert np.array_equal(g1, keep[0]) and np.array_equal(R1, keep[1])
         assert not np.array_equal(R1, R2) and not np.shares_memory(R1, R2)
-    _, _, _, V1 = compute_gather_gpu(m1, offs, copy_outputs=False, **kw)
+    _, _, G1, V1 = compute_gather_gpu(m1, offs, copy_outputs=False, **kw)
     v1 = V1.copy()
-    _, _, _, V2 = compute_gather_gpu(m2, offs, copy_outputs=False, **kw)
+    _, _, G2, V2 = compute_gather_gpu(m2, offs, copy_outputs=False, **kw)
     assert np.shares_memory(V1, V2) and np.array_equal(V2, R2) and not np.array_equal(V1, v1)
+    assert np.shares_memory(G1, G2) and np.array_equal(G2, g2)
 
 
 def test_full_size_gather_end_to_end_vs_oracle():
