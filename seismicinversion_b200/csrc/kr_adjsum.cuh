@@ -8,32 +8,46 @@
 
 namespace kr {
 
-constexpr int kSumStride = 13;  // staging row stride in complex values (conflict-free columns)
+constexpr int kSumHalf = 6;     // values staged per round (two rounds per step)
+constexpr int kSumStride = 7;   // staging row stride in complex values
 
 // Shared memory of the sums for `warps` warps: per warp L rows of 12 complex values and a
-// 32 x 13 staging tile.
+// 32 x 7 staging tile.
 __host__ __device__ inline size_t adjsum_smem_bytes(int L, int warps) {
   return sizeof(cd) * (size_t)warps * (sum_rows(L) * kSumVals + 32 * kSumStride);
 }
 
-// acc_row[c] += sum over the warp's lanes of v[c], c < 12.  All 32 lanes call it.
+// Bytes of one warp's staging tile (the region a block may reuse once its sweeps are done).
+__host__ __device__ inline size_t adjsum_stage_bytes(int warps) {
+  return sizeof(cd) * (size_t)warps * 32 * kSumStride;
+}
+
+// acc_row[c] += sum over the warp's lanes of v[c], c < 12, in two rounds of 6 values: lanes
+// (c, g) add rows 8 g .. 8 g + 7 of column c, then the four row groups by shuffles.  All 32
+// lanes call it.
 __device__ __forceinline__ void warp_add12(const cd v[kSumVals], cd* stage, cd* acc_row) {
   const int lane = threadIdx.x & 31;
   cd* mine = stage + lane * kSumStride;
 #pragma unroll
-  for (int k = 0; k < kSumVals; ++k) mine[k] = v[k];
-  __syncwarp();
-  if (lane < 2 * kSumVals) {  // lane (c, half): column c over 16 rows
-    const int c = lane < kSumVals ? lane : lane - kSumVals;
-    const int r0 = lane < kSumVals ? 0 : 16;
-    cd s = stage[r0 * kSumStride + c];
+  for (int h = 0; h < 2; ++h) {
 #pragma unroll
-    for (int r = 1; r < 16; ++r) s = s + stage[(r0 + r) * kSumStride + c];
-    s.x += __shfl_down_sync(0x00ffffffu, s.x, kSumVals);
-    s.y += __shfl_down_sync(0x00ffffffu, s.y, kSumVals);
-    if (lane < kSumVals) acc_row[c] = acc_row[c] + s;
+    for (int k = 0; k < kSumHalf; ++k) mine[k] = v[h * kSumHalf + k];
+    __syncwarp();
+    if (lane < 4 * kSumHalf) {
+      const int c = lane % kSumHalf, g = lane / kSumHalf;
+      cd s = stage[(8 * g) * kSumStride + c];
+#pragma unroll
+      for (int r = 1; r < 8; ++r) s = s + stage[(8 * g + r) * kSumStride + c];
+      s.x += __shfl_down_sync(0x00ffffffu, s.x, 2 * kSumHalf);
+      s.y += __shfl_down_sync(0x00ffffffu, s.y, 2 * kSumHalf);
+      if (lane < 2 * kSumHalf) {
+        s.x += __shfl_down_sync(0x00000fffu, s.x, kSumHalf);
+        s.y += __shfl_down_sync(0x00000fffu, s.y, kSumHalf);
+        if (lane < kSumHalf) acc_row[h * kSumHalf + c] = acc_row[h * kSumHalf + c] + s;
+      }
+    }
+    __syncwarp();
   }
-  __syncwarp();
 }
 
 // The summing sink of one lane: seed 2 conj(R - R_obs) (misfit) or conj(gR) (cotangent gR).

@@ -310,8 +310,8 @@ batch_gradient_kernel(unsigned char* plan, const double2* __restrict__ omega_all
 // Gradient items with the contraction moved out of the frequency loop (kr_adjsum.cuh): the
 // block's warps sum the per-step adjoints of every frequency of the item, then contract once
 // per (pair, interface).  Dynamic smem: per-warp sum rows (sized for max_layers) and staging
-// tiles, the item's [4L] result, then the item's interface coefficients and layer terms and
-// (models that tabulate) the phase table of its tiles.  Register budget: 256 threads per SM
+// tiles (which then hold the item's [4L] result), then the item's interface coefficients and
+// layer terms and (models that tabulate) the phase table of its tiles.  Register budget: 256 threads per SM
 // (its shared memory admits two 128-thread blocks per SM; a 168-register cap only spills).
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, 256 / THREADS)
@@ -330,8 +330,9 @@ batch_grad_sums_kernel(unsigned char* plan, const double2* __restrict__ omega_al
   const int warp = threadIdx.x >> 5;
   cd* acc = reinterpret_cast<cd*>(s_raw);
   cd* stage = acc + (size_t)W * sum_rows(max_layers) * kSumVals;
-  double* s_out = reinterpret_cast<double*>(stage + W * 32 * kSumStride);
-  unsigned char* area = reinterpret_cast<unsigned char*>(s_out) + a256(32 * (size_t)max_layers);
+  // the item's [4L] result reuses the staging tiles once the sweeps are done
+  double* s_out = reinterpret_cast<double*>(stage);
+  unsigned char* area = reinterpret_cast<unsigned char*>(stage + W * 32 * kSumStride);
   for (;;) {
     const int it = next_item(&h->counters[1]);
     if (it >= n_items) break;
@@ -537,8 +538,9 @@ static size_t sums_smem(int threads, int max_layers, int tab_entries, int* tab) 
                               sizeof(cd) * (size_t)tab_entries * 2 * (size_t)(lt - 1));
     *tab = tab_entries;
   }
-  const size_t smem = adjsum_smem_bytes(max_layers, threads / 32) +
-                      a256(32 * (size_t)max_layers) + area;
+  // the staging tiles hold the item's [4L] result after its sweeps
+  if (adjsum_stage_bytes(threads / 32) < sizeof(double) * 4 * (size_t)max_layers) return 0;
+  const size_t smem = adjsum_smem_bytes(max_layers, threads / 32) + area;
   return smem <= kBatchStageMax ? smem : 0;
 }
 

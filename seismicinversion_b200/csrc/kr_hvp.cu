@@ -8,13 +8,17 @@
 //   hvp_ldot_kernel  : per (direction, p, layer) layer values with tangents along v
 //   hvp_idot_kernel  : per (direction, p, iface) coefficients with tangents along v and the
 //                                                 tangents of the 10x6 coefficient tangents
-//   hvp_sweep_kernel : per (direction, p, omega) forward sweep, seed and reverse sweep in dual
-//                                                 numbers; HV mode reduces Re d/dv of the
-//                                                 misfit-gradient contributions over the block,
-//                                                 JDOT mode writes d/dv of dR/dtheta
+//   hvp_sum_kernel   : per (direction, p, omega) forward sweep, seed and reverse sweep in dual
+//                                                 numbers, the per-step dual adjoints summed over
+//                                                 the block's frequencies and contracted once
+//                                                 (HV mode)
+//   hvp_sweep_kernel : the same with the contraction per (omega, p): HV mode for models whose
+//                                                 sums exceed shared memory, JDOT mode (writes
+//                                                 d/dv of dR/dtheta per frequency)
 //   hvp_reduce_kernel: per (direction, parameter) adds the block partials in a fixed order
 // Replaces torch.func.hessian of the reference's tau-p misfit (taup_inversion.py:177,
 // kennett_torch.py:644-684) and the second-order derivative graph it differentiates.
+#include "kr_adjsum.cuh"
 #include "kr_hvp.cuh"
 #include "kr_internal.cuh"
 
@@ -214,6 +218,116 @@ hvp_sweep_kernel(int L, int n_p, int n_dir, const double2* __restrict__ omega, i
   }
 }
 
+// HV mode with the contraction moved out of the frequency loop: each warp sums the value and
+// tangent parts of its lanes' per-step dual adjoints into its own rows (two row sets), the
+// block contracts the summed rows once per (direction, p, interface).  Dynamic smem: per-warp
+// value rows, tangent rows, staging tiles.
+struct DualSumSink {
+  bool valid;
+  cd robs;
+  cd* accv;  // this warp's value rows
+  cd* acct;  // this warp's tangent rows
+  cd* stage;
+  int I;
+  __device__ DC reflectivity(const DC& R) {
+    if (!valid) return dc(mk(0.0, 0.0));
+    const cd r = R.v - robs;
+    return dc(mk(2.0 * r.x, -2.0 * r.y), mk(2.0 * R.t.x, -2.0 * R.t.y));
+  }
+  __device__ void add(int row, const DC v[kSumVals]) {
+    cd x[kSumVals];
+#pragma unroll
+    for (int k = 0; k < kSumVals; ++k) x[k] = v[k].v;
+    warp_add12(x, stage, accv + (size_t)row * kSumVals);
+#pragma unroll
+    for (int k = 0; k < kSumVals; ++k) x[k] = v[k].t;
+    warp_add12(x, stage, acct + (size_t)row * kSumVals);
+  }
+  __device__ void top(const DC& f0) {
+    DC v[kSumVals];
+#pragma unroll
+    for (int k = 0; k < kSumVals; ++k) v[k] = dc(mk(0.0, 0.0));
+    v[10] = f0;
+    add(I, v);
+  }
+  __device__ void step(int i, const DC cbar[10], const DC& fa, const DC& fb) {
+    DC v[kSumVals];
+#pragma unroll
+    for (int k = 0; k < 10; ++k) v[k] = cbar[k];
+    v[10] = fa;
+    v[11] = fb;
+    add(i, v);
+  }
+};
+
+__global__ void __launch_bounds__(kHvpThreads, 1)
+hvp_sum_kernel(int L, int n_p, const double2* __restrict__ omega, int n_w, int n_wtiles,
+               int free_surface, const LayerV* __restrict__ lv_all,
+               const IfS<DC>* __restrict__ ifs_all, const ScatTan* __restrict__ tan_all,
+               const ScatTan* __restrict__ tant_all, const double2* __restrict__ R_obs,
+               double* __restrict__ partial) {
+  constexpr int W = kHvpThreads / 32;
+  extern __shared__ __align__(16) double s_raw[];
+  const int I = L - 1;
+  const int nrow = (int)sum_rows(L) * kSumVals;
+  const int tile = blockIdx.x % n_wtiles;
+  const size_t pd = blockIdx.x / n_wtiles;  // dir * n_p + p
+  const int ip = (int)(pd % n_p);
+  const int iw = tile * kHvpThreads + threadIdx.x;
+  const bool valid = iw < n_w;
+  const int warp = threadIdx.x >> 5;
+  cd* accv = reinterpret_cast<cd*>(s_raw);
+  cd* acct = accv + (size_t)W * nrow;
+  cd* stage = acct + (size_t)W * nrow;
+  for (int k = threadIdx.x; k < 2 * W * nrow; k += blockDim.x) accv[k] = mk(0.0, 0.0);
+  __syncthreads();
+  cd w = mk(0.0, 0.0);
+  if (valid) {
+    const double2 wv = omega[iw];
+    w = mk(wv.x, wv.y);
+  }
+  DualSumSink sink;
+  sink.valid = valid;
+  sink.robs = mk(0.0, 0.0);
+  if (valid) {
+    const double2 o = R_obs[(size_t)ip * n_w + iw];
+    sink.robs = mk(o.x, o.y);
+  }
+  sink.accv = accv + (size_t)warp * nrow;
+  sink.acct = acct + (size_t)warp * nrow;
+  sink.stage = stage + warp * 32 * kSumStride;
+  sink.I = I;
+  const LayerV* lv = lv_all + pd * L;
+  hvp_pair_sums(L, w, free_surface != 0, lv, ifs_all + pd * I, sink);
+  __syncthreads();
+  for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
+    cd a = accv[k], b = acct[k];
+    for (int wi = 1; wi < W; ++wi) {
+      a = a + accv[wi * nrow + k];
+      b = b + acct[wi * nrow + k];
+    }
+    accv[k] = a;
+    acct[k] = b;
+  }
+  __syncthreads();
+  double* dst = partial + (size_t)blockIdx.x * (4 * L);
+  for (int l = threadIdx.x; l < L; l += blockDim.x) {
+    double v[4];
+    hvp_sums_contract_layer(l, L, accv, acct, tan_all + (size_t)ip * I, tant_all + pd * I, lv, v);
+    dst[0 * L + l] = v[0];
+    dst[1 * L + l] = v[1];
+    dst[2 * L + l] = v[2];
+    dst[3 * L + l] = v[3];
+  }
+}
+
+// Dynamic smem of hvp_sum_kernel (0 if it does not fit).
+static size_t hvp_sum_smem(int L) {
+  const size_t smem = sizeof(cd) * (size_t)(kHvpThreads / 32) *
+                      (2 * sum_rows(L) * kSumVals + 32 * kSumStride);
+  return smem <= 160 * 1024 ? smem : 0;
+}
+
 // out[dir][k] = sum_b partial[dir][b][k]; grid (nv, n_dir), fixed-shape tree.
 __global__ void __launch_bounds__(256)
 hvp_reduce_kernel(const double* __restrict__ partial, int blocks_per_dir, int nv,
@@ -276,6 +390,24 @@ static kr_status launch_hvp(const double* layers, int L, const double* p, int n_
                                                             w.tant);
   s = check_launch("kr_hvp: interface tangents");
   if (s != KR_OK) return s;
+  if (MODE == kHvpModeHv) {
+    const size_t ssm = hvp_sum_smem(L);
+    if (ssm) {
+      static SmemLimit slim;
+      if (ssm > 48 * 1024) {
+        s = raise_smem_limit((const void*)hvp_sum_kernel, ssm, slim, "kr_hvp: smem attribute");
+        if (s != KR_OK) return s;
+      }
+      hvp_sum_kernel<<<(unsigned)blocks, kHvpThreads, ssm, st>>>(
+          L, n_p, reinterpret_cast<const double2*>(omega), n_w, n_wtiles,
+          (flags & KR_FREE_SURFACE) ? 1 : 0, w.lv, w.ifs, w.tan, w.tant,
+          reinterpret_cast<const double2*>(R_obs), w.partial);
+      s = check_launch("kr_hvp: sweep");
+      if (s != KR_OK) return s;
+      hvp_reduce_kernel<<<dim3(4 * L, n_dir), 256, 0, st>>>(w.partial, (int)per_dir, 4 * L, out);
+      return check_launch("kr_hvp: reduce");
+    }
+  }
   const size_t smem = MODE == kHvpModeHv ? sizeof(double) * (kHvpThreads / 32) * 4 * (size_t)L : 0;
   static SmemLimit lim;
   if (smem > 48 * 1024) {

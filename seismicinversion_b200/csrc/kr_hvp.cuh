@@ -517,3 +517,135 @@ KR_HD void hvp_pair(int L, cd w, bool free_surface, const LayerV* lv, const IfS<
 }
 
 }  // namespace kr
+
+namespace kr {
+
+// ------------------------------------------------------------------------------------------
+// Frequency sums of the dual adjoint (misfit Hessian-vector products): as adjoint_pair_sums,
+// the sink receives per step the dual coefficient adjoints and phase terms, and the
+// contraction with the (frequency-independent) coefficient tangents, their derivatives along
+// v and the phase-derivative factors runs once per (p, direction, interface) on the sums:
+//   (H v)_j = Re( sum_w dcbar_k(w) t_kj + sum_w cbar_k(w) dt_kj ) + phase terms alike.
+// ------------------------------------------------------------------------------------------
+#ifdef __CUDACC__
+#pragma nv_exec_check_disable
+#endif
+template <class Sink>
+KR_HD void hvp_pair_sums(int L, cd w, bool free_surface, const LayerV* lv, const IfS<DC>* ifs,
+                         Sink& sink) {
+  const int I = L - 1;
+  const int nsteps = I - 1;
+  const int seg = hvp_spacing(nsteps);
+  const int ncp = nsteps > 0 ? (nsteps + seg - 1) / seg : 0;
+  const DC W = dc(w);
+  SymS<DC> cp[kHvpCp];
+  SymS<DC> sg[kHvpSeg];
+  SymS<DC> r;
+  r.a = ifs[I - 1].rd11;
+  r.b = ifs[I - 1].rd12;
+  r.d = ifs[I - 1].rd22;
+  for (int s = 0; s < nsteps; ++s) {
+    if (s % seg == 0) cp[s / seg] = r;
+    const int i = I - 2 - s;
+    const DC ea = cexp_(W * lv[i + 1].ca), eb = cexp_(W * lv[i + 1].cb);
+    if (s >= (ncp - 1) * seg) sg[s - (ncp - 1) * seg] = r;
+    r = step_s(r, ea, eb, ifs[i]);
+  }
+  const DC e0 = cexp_(W * lv[0].ca);
+  const DC y = (e0 * e0) * r.a;
+  DC g = dc(mk(1.0, 0.0));
+  DC R = y;
+  if (free_surface) {
+    const DC q = recip(1.0 + y);
+    R = y * q;
+    g = q * q;
+  }
+  const DC seed = sink.reflectivity(R);
+  const DC ob0 = ((e0 * e0) * g) * seed;
+  const DC f0 = ((2.0 * (e0 * r.a)) * g) * ((e0 * W) * seed);
+  sink.top(f0);
+  SymS<DC> ob;
+  ob.a = ob0;
+  ob.b = ob.d = dc(mk(0.0, 0.0));
+  for (int q = ncp - 1; q >= 0; --q) {
+    const int s0 = q * seg;
+    const int s1 = s0 + seg < nsteps ? s0 + seg : nsteps;
+    if (q != ncp - 1) {
+      SymS<DC> x = cp[q];
+      for (int s = s0; s < s1; ++s) {
+        const int i = I - 2 - s;
+        sg[s - s0] = x;
+        if (s + 1 < s1) x = step_s(x, cexp_(W * lv[i + 1].ca), cexp_(W * lv[i + 1].cb), ifs[i]);
+      }
+    }
+    for (int s = s1 - 1; s >= s0; --s) {
+      const int i = I - 2 - s;
+      const DC ea = cexp_(W * lv[i + 1].ca), eb = cexp_(W * lv[i + 1].cb);
+      SymS<DC> rb;
+      DC eab, ebb, cbar[10];
+      step_reverse_s(sg[s - s0], ea, eb, ifs[i], ob, rb, eab, ebb, cbar);
+      sink.step(i, cbar, eab * (ea * W), ebb * (eb * W));
+      ob = rb;
+    }
+  }
+  DC cbar[10];
+  cbar[0] = ob.a;
+  cbar[1] = ob.b;
+  cbar[2] = ob.d;
+  for (int k = 3; k < 10; ++k) cbar[k] = dc(mk(0.0, 0.0));
+  sink.step(I - 1, cbar, dc(mk(0.0, 0.0)), dc(mk(0.0, 0.0)));
+}
+
+// Re of the tangent of the alpha, beta, rho, h contributions of layer l from the summed rows
+// (sv: value parts, st: tangent parts, the row layout of sums_contract_layer): t / tt are the
+// coefficient tangents and their derivatives along v, lv the layer's values and tangents.
+KR_HD void hvp_sums_contract_layer(int l, int L, const cd* sv, const cd* st, const ScatTan* t,
+                                   const ScatTan* tt, const LayerV* lv, double out[4]) {
+  const int I = L - 1;
+  double a = 0.0, b = 0.0, r = 0.0, h = 0.0;
+  if (l < I) {
+    const cd* V = sv + (size_t)l * kSumVals;
+    const cd* T = st + (size_t)l * kSumVals;
+    for (int k = 0; k < 10; ++k) {
+      acc_add(a, T[k], t[l].t[k][0]);
+      acc_add(b, T[k], t[l].t[k][1]);
+      acc_add(r, T[k], t[l].t[k][2]);
+      acc_add(a, V[k], tt[l].t[k][0]);
+      acc_add(b, V[k], tt[l].t[k][1]);
+      acc_add(r, V[k], tt[l].t[k][2]);
+    }
+  }
+  DC A = dc(mk(0.0, 0.0)), B = dc(mk(0.0, 0.0));
+  if (l > 0) {
+    const cd* V = sv + (size_t)(l - 1) * kSumVals;
+    const cd* T = st + (size_t)(l - 1) * kSumVals;
+    for (int k = 0; k < 10; ++k) {
+      acc_add(a, T[k], t[l - 1].t[k][3]);
+      acc_add(b, T[k], t[l - 1].t[k][4]);
+      acc_add(r, T[k], t[l - 1].t[k][5]);
+      acc_add(a, V[k], tt[l - 1].t[k][3]);
+      acc_add(b, V[k], tt[l - 1].t[k][4]);
+      acc_add(r, V[k], tt[l - 1].t[k][5]);
+    }
+    A = dc(V[10], T[10]);
+    B = dc(V[11], T[11]);
+  } else {
+    A = dc(sv[(size_t)I * kSumVals + 10], st[(size_t)I * kSumVals + 10]);
+  }
+  const LayerV& d = lv[l];
+  // Re of the tangent of A ca_alpha etc.: dA ca_alpha + A dca_alpha
+  acc_add(a, A.t, d.ca_alpha.v);
+  acc_add(a, A.v, d.ca_alpha.t);
+  acc_add(b, B.t, d.cb_beta.v);
+  acc_add(b, B.v, d.cb_beta.t);
+  acc_add(h, A.t, d.ca_h.v);
+  acc_add(h, A.v, d.ca_h.t);
+  acc_add(h, B.t, d.cb_h.v);
+  acc_add(h, B.v, d.cb_h.t);
+  out[0] = a;
+  out[1] = b;
+  out[2] = r;
+  out[3] = h;
+}
+
+}  // namespace kr

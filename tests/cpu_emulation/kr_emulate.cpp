@@ -210,3 +210,70 @@ extern "C" void emu_gradient_sums(const double* tab, int L, const double* p, int
     }
   }
 }
+
+// ---- frequency sums of the dual adjoint (hvp_pair_sums + hvp_sums_contract_layer), the path
+// of the misfit Hessian-vector-product kernel ----
+namespace {
+struct HostDualSumSink {
+  cd* sv;  // [L][12] value parts, summed over frequency
+  cd* st;  // [L][12] tangent parts
+  int I;
+  cd robs;
+  DC reflectivity(const DC& R) {
+    const cd r = R.v - robs;
+    return dc(mk(2.0 * r.x, -2.0 * r.y), mk(2.0 * R.t.x, -2.0 * R.t.y));
+  }
+  void add(int row, int k, const DC& x) {
+    sv[(size_t)row * kSumVals + k] = sv[(size_t)row * kSumVals + k] + x.v;
+    st[(size_t)row * kSumVals + k] = st[(size_t)row * kSumVals + k] + x.t;
+  }
+  void top(const DC& f0) { add(I, 10, f0); }
+  void step(int i, const DC cbar[10], const DC& fa, const DC& fb) {
+    for (int k = 0; k < 10; ++k) add(i, k, cbar[k]);
+    add(i, 10, fa);
+    add(i, 11, fb);
+  }
+};
+}  // namespace
+
+// hv[4L] = H v of chi = sum |R - R_obs|^2 by the frequency-sum dual path.
+extern "C" void emu_hvp_sums(const double* tab, int L, const double* p, int n_p, const double* w,
+                             int nw, int fs, const double* v, const double* R_obs, double* hv) {
+  static LayerP lay[512];
+  static LayerD dlay[512];
+  static LayerD2 d2[512];
+  static LayerV lv[512];
+  static Iface f[512];
+  static IfS<DC> ifs[512];
+  static ScatTan t[512], tt[512];
+  static cd sv[512 * kSumVals], st[512 * kSumVals];
+  const int I = L - 1;
+  for (int q = 0; q < 4 * L; ++q) hv[q] = 0.0;
+  for (int j = 0; j < n_p; ++j) {
+    for (int l = 0; l < L; ++l) {
+      lay[l] = layer_terms(tab, L, l, p[j]);
+      dlay[l] = layer_derivs(tab, L, l, p[j], lay[l]);
+      d2[l] = layer_derivs2(tab, L, l, lay[l], dlay[l]);
+      const double vl[4] = {v[l], v[L + l], v[2 * L + l], v[3 * L + l]};
+      lv[l] = layer_dot(tab, L, l, lay[l], dlay[l], d2[l], vl);
+    }
+    for (int i = 0; i < I; ++i) {
+      f[i] = interface_coeffs(p[j], i, lay[i], lay[i + 1]);
+      interface_tangents(p[j], i, lay[i], dlay[i], lay[i + 1], dlay[i + 1], t[i]);
+      IfS<DC> c;
+      interface_dot(p[j], i, lv[i], lv[i + 1], c, tt[i]);
+      ifs[i] = iface_dual(f[i], c);
+    }
+    for (size_t q = 0; q < (size_t)L * kSumVals; ++q) sv[q] = st[q] = mk(0.0, 0.0);
+    for (int k = 0; k < nw; ++k) {
+      HostDualSumSink s{sv, st, I, mk(R_obs[2 * ((size_t)j * nw + k)],
+                                      R_obs[2 * ((size_t)j * nw + k) + 1])};
+      hvp_pair_sums(L, mk(w[2 * k], w[2 * k + 1]), fs != 0, lv, ifs, s);
+    }
+    for (int l = 0; l < L; ++l) {
+      double o[4];
+      hvp_sums_contract_layer(l, L, sv, st, t, tt, lv, o);
+      for (int q = 0; q < 4; ++q) hv[q * L + l] += o[q];
+    }
+  }
+}
