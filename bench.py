@@ -65,7 +65,8 @@ def parse():
                     help="device steps only (no e2e, CPU baseline or peak probe): for ncu")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the inversion / batching / serving measurements")
-    ap.add_argument("--profile-kernel", choices=["inversion", "batch", "gmm"], default=None,
+    ap.add_argument("--profile-kernel", choices=["inversion", "batch", "gmm", "gather512"],
+                    default=None,
                     help="run only a small case of that workload (for ncu), no JSON line")
     return ap.parse_args()
 
@@ -1241,8 +1242,10 @@ def run_reference(args, rank, world):
 
 
 def profile_case(kind):
-    """Small cases for ncu captures: the inversion gradient / Jacobian (64 p x 1024 omega,
-    21 layers) or a 256-model uneven batch (seed 3, half gradient)."""
+    """Small cases for ncu captures: the inversion gradient / Jacobian / Hessian-vector
+    products (64 p x 1024 omega, 21 layers), a 256-model uneven batch (seed 3, half gradient),
+    the GMM forward, or the 21-layer gather at 512 of its 8192 slownesses (every 16th; all 2047
+    damped frequencies and 100 offsets: R grid 17 MB, Bessel sum, traces)."""
     import torch
 
     from seismicinversion_b200 import device as D
@@ -1257,9 +1260,27 @@ def profile_case(kind):
         w = torch.as_tensor(np.arange(1, 1025) * (2 * np.pi / 64), device=dev).to(torch.complex128)
         R_obs = D.reflectivity(D.layer_table(true, dev), p, w)
         tab = D.layer_table(start, dev)
+        from seismicinversion_b200.kennett_torch import packed_index
+
+        V = torch.eye(84, dtype=torch.float64, device=dev)[torch.as_tensor(packed_index(21))]
         for _ in range(3):
             D.misfit_gradient(tab, p, w, R_obs)
             D.jacobian(tab, p, w, want_R=False)
+        D.misfit_hvp(tab, p, w, R_obs, V)
+    elif kind == "gather512":
+        from seismicinversion_b200.earth_models import damped_gather_grid, random_layered_model
+
+        om, omd, p, dp, taper, _ = damped_gather_grid(64.0, 2048, 8192, 1.2)
+        tab = D.layer_table(random_layered_model(20, seed=1), dev)
+        sel = slice(15, 8192, 16)
+        p_t = torch.as_tensor(p[sel], device=dev)
+        pw_t = torch.as_tensor((taper * p)[sel], device=dev)
+        w_t, wr_t = torch.as_tensor(omd, device=dev), torch.as_tensor(om, device=dev)
+        off_t = torch.as_tensor(np.arange(1, 101) * 0.5, device=dev)
+        for _ in range(2):
+            R = D.reflectivity(tab, p_t, w_t, True)
+            U = D.bessel_sum(R, p_t, pw_t, 16 * dp, wr_t, off_t)
+            D.traces(U, 2048)
     elif kind == "gmm":
         from seismicinversion_b200.earth_models import damped_gather_grid, random_layered_model
 
