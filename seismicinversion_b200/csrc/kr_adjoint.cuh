@@ -208,13 +208,17 @@ KR_HD void contract(const ScatTan& t, const cd cbar[10], AccT& up, AccT& lo) {
 }
 
 // Tape of one (omega, p) pair, in local memory: up to kSegMax steps of inputs (the three
-// entries of the symmetric state) and phase factors (80 B per step) plus kCpMax
-// checkpoints.  64 steps hold every model of up to 66
-// layers outright, so those run without any recomputation; measured on an uneven batch of
-// 3-64-layer models, the larger per-thread stack (~7 KB) costs far less than recomputing
-// segments did (24 steps: 1080 ms, 40: 1049 ms, 64: 963 ms per batch).
-constexpr int kSegMax = 64;
-constexpr int kCpMax = 4;  // segments of the deepest model (kr_deriv.cu checks the bound)
+// entries of the symmetric state) and phase factors (80 B per step; 48 B where the phases
+// come from a table) plus kCpMax checkpoints.  64 steps hold every model of up to 66 layers
+// outright, so those run without any recomputation; measured on an uneven batch of 3-64-layer
+// models with the per-step contraction, the larger per-thread stack (~7 KB) cost far less
+// than recomputing segments did (24 steps: 1080 ms, 40: 1049 ms, 64: 963 ms per batch).
+// KR_TAPE_STEPS changes the length at build time.
+#ifndef KR_TAPE_STEPS
+#define KR_TAPE_STEPS 64
+#endif
+constexpr int kSegMax = KR_TAPE_STEPS;
+constexpr int kCpMax = (256 - 2 + kSegMax - 1) / kSegMax;  // segments of the deepest model
 
 // Steps per segment: one segment (a full tape, no recomputation) when the pair's steps fit
 // the buffer, else the fewest segments of at most kSegMax steps, of balanced length.
