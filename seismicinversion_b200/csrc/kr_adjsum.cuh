@@ -8,42 +8,51 @@
 
 namespace kr {
 
-constexpr int kSumHalf = 6;     // values staged per round (two rounds per step)
-constexpr int kSumStride = 7;   // staging row stride in complex values
+// Staging of the warp sums: ROUNDS = 1 stages all 12 values in one 32 x 13 tile (fewest
+// instructions); ROUNDS = 2 stages 6 at a time in a 32 x 7 tile (half the shared memory, for
+// kernels whose residency shared memory limits).  Tile row stride in complex values:
+template <int ROUNDS>
+__host__ __device__ constexpr int stage_stride() { return kSumVals / ROUNDS + 1; }
 
-// Shared memory of the sums for `warps` warps: per warp L rows of 12 complex values and a
-// 32 x 7 staging tile.
-__host__ __device__ inline size_t adjsum_smem_bytes(int L, int warps) {
-  return sizeof(cd) * (size_t)warps * (sum_rows(L) * kSumVals + 32 * kSumStride);
+// Shared memory of the sums for `warps` warps: per warp L rows of 12 complex values and its
+// staging tile.
+__host__ __device__ inline size_t adjsum_smem_bytes(int L, int warps, int rounds) {
+  const int stride = kSumVals / rounds + 1;
+  return sizeof(cd) * (size_t)warps * (sum_rows(L) * kSumVals + 32 * (size_t)stride);
 }
 
-// Bytes of one warp's staging tile (the region a block may reuse once its sweeps are done).
-__host__ __device__ inline size_t adjsum_stage_bytes(int warps) {
-  return sizeof(cd) * (size_t)warps * 32 * kSumStride;
+// Bytes of the warps' staging tiles (the region a block may reuse once its sweeps are done).
+__host__ __device__ inline size_t adjsum_stage_bytes(int warps, int rounds) {
+  return sizeof(cd) * (size_t)warps * 32 * (size_t)(kSumVals / rounds + 1);
 }
 
-// acc_row[c] += sum over the warp's lanes of v[c], c < 12, in two rounds of 6 values: lanes
-// (c, g) add rows 8 g .. 8 g + 7 of column c, then the four row groups by shuffles.  All 32
-// lanes call it.
+// acc_row[c] += sum over the warp's lanes of v[c], c < 12.  Per round, lanes (c, g) add the
+// rows of row group g in column c (2 groups of 16 rows for one round, 4 of 8 for two), then
+// shuffles combine the groups; a fixed order (deterministic).  All 32 lanes call it.
+template <int ROUNDS>
 __device__ __forceinline__ void warp_add12(const cd v[kSumVals], cd* stage, cd* acc_row) {
+  constexpr int P = kSumVals / ROUNDS, S = P + 1, G = 2 * ROUNDS, RG = 32 / G;
   const int lane = threadIdx.x & 31;
-  cd* mine = stage + lane * kSumStride;
+  cd* mine = stage + lane * S;
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
+  for (int h = 0; h < ROUNDS; ++h) {
 #pragma unroll
-    for (int k = 0; k < kSumHalf; ++k) mine[k] = v[h * kSumHalf + k];
+    for (int k = 0; k < P; ++k) mine[k] = v[h * P + k];
     __syncwarp();
-    if (lane < 4 * kSumHalf) {
-      const int c = lane % kSumHalf, g = lane / kSumHalf;
-      cd s = stage[(8 * g) * kSumStride + c];
+    if (lane < G * P) {  // 24 lanes
+      const int c = lane % P, g = lane / P;
+      cd s = stage[(RG * g) * S + c];
 #pragma unroll
-      for (int r = 1; r < 8; ++r) s = s + stage[(8 * g + r) * kSumStride + c];
-      s.x += __shfl_down_sync(0x00ffffffu, s.x, 2 * kSumHalf);
-      s.y += __shfl_down_sync(0x00ffffffu, s.y, 2 * kSumHalf);
-      if (lane < 2 * kSumHalf) {
-        s.x += __shfl_down_sync(0x00000fffu, s.x, kSumHalf);
-        s.y += __shfl_down_sync(0x00000fffu, s.y, kSumHalf);
-        if (lane < kSumHalf) acc_row[h * kSumHalf + c] = acc_row[h * kSumHalf + c] + s;
+      for (int r = 1; r < RG; ++r) s = s + stage[(RG * g + r) * S + c];
+      if (G == 4) {
+        s.x += __shfl_down_sync(0x00ffffffu, s.x, 2 * P);
+        s.y += __shfl_down_sync(0x00ffffffu, s.y, 2 * P);
+      }
+      if (lane < 2 * P) {
+        const unsigned m = (2 * P == 24) ? 0x00ffffffu : 0x00000fffu;
+        s.x += __shfl_down_sync(m, s.x, P);
+        s.y += __shfl_down_sync(m, s.y, P);
+        if (lane < P) acc_row[h * P + c] = acc_row[h * P + c] + s;
       }
     }
     __syncwarp();
@@ -51,6 +60,7 @@ __device__ __forceinline__ void warp_add12(const cd v[kSumVals], cd* stage, cd* 
 }
 
 // The summing sink of one lane: seed 2 conj(R - R_obs) (misfit) or conj(gR) (cotangent gR).
+template <int ROUNDS>
 struct SumSink {
   bool valid;
   bool vjp;          // seed with conj(gR) instead of 2 conj(R - R_obs)
@@ -74,7 +84,7 @@ struct SumSink {
 #pragma unroll
     for (int k = 0; k < kSumVals; ++k) v[k] = mk(0.0, 0.0);
     v[10] = f0;
-    warp_add12(v, stage, acc + (size_t)I * kSumVals);
+    warp_add12<ROUNDS>(v, stage, acc + (size_t)I * kSumVals);
   }
   __device__ void step(int i, const cd cbar[10], cd fa, cd fb) {
     cd v[kSumVals];
@@ -82,7 +92,7 @@ struct SumSink {
     for (int k = 0; k < 10; ++k) v[k] = cbar[k];
     v[10] = fa;
     v[11] = fb;
-    warp_add12(v, stage, acc + (size_t)i * kSumVals);
+    warp_add12<ROUNDS>(v, stage, acc + (size_t)i * kSumVals);
   }
 };
 

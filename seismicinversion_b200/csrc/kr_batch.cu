@@ -328,11 +328,12 @@ batch_grad_sums_kernel(unsigned char* plan, const double2* __restrict__ omega_al
   const ItemRec* items = reinterpret_cast<const ItemRec*>(plan + h->off_grad);
   const int n_items = h->n_grad;
   const int warp = threadIdx.x >> 5;
+  constexpr int RS = 2;  // two staging rounds: half the tile, two blocks per SM
   cd* acc = reinterpret_cast<cd*>(s_raw);
   cd* stage = acc + (size_t)W * sum_rows(max_layers) * kSumVals;
   // the item's [4L] result reuses the staging tiles once the sweeps are done
   double* s_out = reinterpret_cast<double*>(stage);
-  unsigned char* area = reinterpret_cast<unsigned char*>(stage + W * 32 * kSumStride);
+  unsigned char* area = reinterpret_cast<unsigned char*>(stage + W * 32 * stage_stride<RS>());
   for (;;) {
     const int it = next_item(&h->counters[1]);
     if (it >= n_items) break;
@@ -367,13 +368,13 @@ batch_grad_sums_kernel(unsigned char* plan, const double2* __restrict__ omega_al
         w = mk(wv.x, wv.y);
       }
       const size_t e = (size_t)pr.j * d.n_w + (valid ? iw : 0);
-      SumSink sink;
+      SumSink<RS> sink;
       sink.valid = valid;
       sink.vjp = false;
       sink.obs = obs_all + d.obs_off + e;
       sink.R_out = (d.flags & KR_BATCH_STORE_R) ? R_all + d.R_off + e : nullptr;
       sink.acc = acc + (size_t)warp * L * kSumVals;
-      sink.stage = stage + warp * 32 * kSumStride;
+      sink.stage = stage + warp * 32 * stage_stride<RS>();
       sink.I = I;
       const int iwt = valid ? iw : item.w0;
       const PhaseAuto ph{((mask >> (iwt / kPhTile - u0)) & 1u) != 0,
@@ -539,8 +540,8 @@ static size_t sums_smem(int threads, int max_layers, int tab_entries, int* tab) 
     *tab = tab_entries;
   }
   // the staging tiles hold the item's [4L] result after its sweeps
-  if (adjsum_stage_bytes(threads / 32) < sizeof(double) * 4 * (size_t)max_layers) return 0;
-  const size_t smem = adjsum_smem_bytes(max_layers, threads / 32) + area;
+  if (adjsum_stage_bytes(threads / 32, 2) < sizeof(double) * 4 * (size_t)max_layers) return 0;
+  const size_t smem = adjsum_smem_bytes(max_layers, threads / 32, 2) + area;
   return smem <= kBatchStageMax ? smem : 0;
 }
 

@@ -281,9 +281,10 @@ deriv_sum_kernel(int L, int n_p, const double2* __restrict__ omega, int n_w, int
   const int iw = tile * kDerThreads + threadIdx.x;
   const bool valid = iw < n_w;
   const int warp = threadIdx.x >> 5;
+  constexpr int RS = 1;  // one staging round: registers, not shared memory, bound residency
   cd* acc = reinterpret_cast<cd*>(s_raw);
   cd* stage = acc + (size_t)W * sum_rows(L) * kSumVals;
-  unsigned char* b = reinterpret_cast<unsigned char*>(stage + W * 32 * kSumStride);
+  unsigned char* b = reinterpret_cast<unsigned char*>(stage + W * 32 * stage_stride<RS>());
   Iface* sc = reinterpret_cast<Iface*>(b);
   LayerP* sl = reinterpret_cast<LayerP*>(b + sizeof(Iface) * I);
   cd* s_ph = reinterpret_cast<cd*>(b + sizeof(Iface) * I + sizeof(LayerP) * L);
@@ -303,13 +304,13 @@ deriv_sum_kernel(int L, int n_p, const double2* __restrict__ omega, int n_w, int
   const PhaseAuto ph{use_tab, phase_at(s_ph, kPhHead + 1, valid ? iw : tile * kDerThreads, tile),
                      PhaseDirect{w, sl}};
   const size_t e = (size_t)ip * n_w + (valid ? iw : 0);
-  SumSink sink;
+  SumSink<RS> sink;
   sink.valid = valid;
   sink.vjp = vjp != 0;
   sink.obs = obs + e;
   sink.R_out = R_out ? R_out + e : nullptr;
   sink.acc = acc + (size_t)warp * sum_rows(L) * kSumVals;
-  sink.stage = stage + warp * 32 * kSumStride;
+  sink.stage = stage + warp * 32 * stage_stride<RS>();
   sink.I = I;
   adjoint_pair_sums(L, w, free_surface != 0, seg, sc, ph, sink);
   double c2 = valid ? (sink.res.x * sink.res.x + sink.res.y * sink.res.y) : 0.0;
@@ -379,7 +380,7 @@ static kr_status launch_sweep(int minb, unsigned blocks, size_t smem, cudaStream
 
 // Dynamic smem of deriv_sum_kernel for a model of L layers (0 if it does not fit).
 static size_t sum_kernel_smem(int L, int table) {
-  const size_t smem = adjsum_smem_bytes(L, kDerThreads / 32) + prologue_smem_bytes(L) +
+  const size_t smem = adjsum_smem_bytes(L, kDerThreads / 32, 1) + prologue_smem_bytes(L) +
                       (table ? phase_table_bytes(L, 1) : 0);
   return smem <= kStageSmemMax ? smem : 0;
 }

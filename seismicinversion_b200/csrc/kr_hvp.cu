@@ -238,10 +238,10 @@ struct DualSumSink {
     cd x[kSumVals];
 #pragma unroll
     for (int k = 0; k < kSumVals; ++k) x[k] = v[k].v;
-    warp_add12(x, stage, accv + (size_t)row * kSumVals);
+    warp_add12<1>(x, stage, accv + (size_t)row * kSumVals);
 #pragma unroll
     for (int k = 0; k < kSumVals; ++k) x[k] = v[k].t;
-    warp_add12(x, stage, acct + (size_t)row * kSumVals);
+    warp_add12<1>(x, stage, acct + (size_t)row * kSumVals);
   }
   __device__ void top(const DC& f0) {
     DC v[kSumVals];
@@ -295,7 +295,7 @@ hvp_sum_kernel(int L, int n_p, const double2* __restrict__ omega, int n_w, int n
   }
   sink.accv = accv + (size_t)warp * nrow;
   sink.acct = acct + (size_t)warp * nrow;
-  sink.stage = stage + warp * 32 * kSumStride;
+  sink.stage = stage + warp * 32 * stage_stride<1>();
   sink.I = I;
   const LayerV* lv = lv_all + pd * L;
   hvp_pair_sums(L, w, free_surface != 0, lv, ifs_all + pd * I, sink);
@@ -324,7 +324,7 @@ hvp_sum_kernel(int L, int n_p, const double2* __restrict__ omega, int n_w, int n
 // Dynamic smem of hvp_sum_kernel (0 if it does not fit).
 static size_t hvp_sum_smem(int L) {
   const size_t smem = sizeof(cd) * (size_t)(kHvpThreads / 32) *
-                      (2 * sum_rows(L) * kSumVals + 32 * kSumStride);
+                      (2 * sum_rows(L) * kSumVals + 32 * stage_stride<1>());
   return smem <= 160 * 1024 ? smem : 0;
 }
 
