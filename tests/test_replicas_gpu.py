@@ -1,6 +1,9 @@
-"""Replicas on the GPU (one device standing in for two): the router over two GPU servers and
-the two ranks' shards of a batch give every model exactly the single-batch result (forward
-bit-identical; gradients to 1e-12, the batch adds block partials with FP64 atomics)."""
+"""Replicas on the GPU (one device standing in for two): the two ranks' shards of a batch give
+every model the single-batch result (forward bit-identical; gradients to 1e-12, the batch
+adds block partials with FP64 atomics), and the router over two GPU servers gives every
+request the single-call result (forward bit-identical; gradients to 1e-11: the batch and the
+single call sum the same per-frequency terms in different orders, and these gradients are
+sums with cancellation, so their rounding differs at ~1e-12 of max |g|)."""
 
 import numpy as np
 import pytest
@@ -65,7 +68,7 @@ def test_router_over_two_gpu_servers():
         if it.gradient:
             out, R = D.misfit_gradient(tab, it.p, it.omega, it.R_obs, want_R=True)
             L = it.model.n_layers
-            assert rel_err(r["grad"].cpu().numpy(), out[:4 * L].cpu().numpy()) < 1e-12
+            assert rel_err(r["grad"].cpu().numpy(), out[:4 * L].cpu().numpy()) < 1e-11
             assert torch.equal(r["R"], R)
         else:
             assert torch.equal(r["R"], D.reflectivity(tab, it.p, it.omega))
