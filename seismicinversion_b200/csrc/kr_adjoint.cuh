@@ -78,30 +78,49 @@ struct ScatTan {
   cd t[10][6];
 };
 
-KR_HD void interface_tangents(double p, int iface, const LayerP& up, const LayerD& dup,
-                              const LayerP& lo, const LayerD& dlo, ScatTan& out) {
-  typedef Dual<6> D;
-  D eta1 = dconst<6>(up.eta), neta1 = dconst<6>(up.neta), rho1 = dconst<6>(to_c(up.rho));
-  D betac1 = dconst<6>(up.betac);
-  D eta2 = dconst<6>(lo.eta), neta2 = dconst<6>(lo.neta), rho2 = dconst<6>(to_c(lo.rho));
-  D betac2 = dconst<6>(lo.betac);
-  eta1.d[0] = dup.eta_alpha;
-  neta1.d[1] = dup.neta_beta;
-  betac1.d[1] = dup.betac_beta;
-  rho1.d[2] = mk(1.0, 0.0);
-  eta2.d[3] = dlo.eta_alpha;
-  neta2.d[4] = dlo.neta_beta;
-  betac2.d[4] = dlo.betac_beta;
-  rho2.d[5] = mk(1.0, 0.0);
+// Column j of t (one tangent direction: forward mode with a single dual component).  The dual
+// arithmetic acts on each tangent component separately, so the column is the one a pass over
+// all six directions computes, with a sixth of the live state: the kernels run one thread per
+// (slowness, interface, column) and nothing spills.
+KR_HD void interface_tangent_col(double p, int iface, const LayerP& up, const LayerD& dup,
+                                 const LayerP& lo, const LayerD& dlo, int j, cd col[10]) {
+  typedef Dual<1> D;
+  D eta1 = dconst<1>(up.eta), neta1 = dconst<1>(up.neta), rho1 = dconst<1>(to_c(up.rho));
+  D betac1 = dconst<1>(up.betac);
+  D eta2 = dconst<1>(lo.eta), neta2 = dconst<1>(lo.neta), rho2 = dconst<1>(to_c(lo.rho));
+  D betac2 = dconst<1>(lo.betac);
+  switch (j) {
+    case 0: eta1.d[0] = dup.eta_alpha; break;
+    case 1: neta1.d[0] = dup.neta_beta; betac1.d[0] = dup.betac_beta; break;
+    case 2: rho1.d[0] = mk(1.0, 0.0); break;
+    case 3: eta2.d[0] = dlo.eta_alpha; break;
+    case 4: neta2.d[0] = dlo.neta_beta; betac2.d[0] = dlo.betac_beta; break;
+    default: rho2.d[0] = mk(1.0, 0.0); break;
+  }
   IfaceT<D> f;
   if (iface == 0)
     ocean_bottom<D>(p, eta1, rho1, eta2, neta2, rho2, betac2, f);
   else
     solid_solid<D>(p, eta1, neta1, rho1, betac1, eta2, neta2, rho2, betac2, f);
-  const D* c[10] = {&f.rd11, &f.rd12, &f.rd22, &f.ru11, &f.ru12,
-                    &f.ru22, &f.td11, &f.td12, &f.td21, &f.td22};
-  for (int k = 0; k < 10; ++k)
-    for (int j = 0; j < 6; ++j) out.t[k][j] = c[k]->d[j];
+  col[0] = f.rd11.d[0];
+  col[1] = f.rd12.d[0];
+  col[2] = f.rd22.d[0];
+  col[3] = f.ru11.d[0];
+  col[4] = f.ru12.d[0];
+  col[5] = f.ru22.d[0];
+  col[6] = f.td11.d[0];
+  col[7] = f.td12.d[0];
+  col[8] = f.td21.d[0];
+  col[9] = f.td22.d[0];
+}
+
+KR_HD void interface_tangents(double p, int iface, const LayerP& up, const LayerD& dup,
+                              const LayerP& lo, const LayerD& dlo, ScatTan& out) {
+  for (int j = 0; j < 6; ++j) {
+    cd col[10];
+    interface_tangent_col(p, iface, up, dup, lo, dlo, j, col);
+    for (int k = 0; k < 10; ++k) out.t[k][j] = col[k];
+  }
 }
 
 // Reverse of kennett_step, differentiating its symmetric adjugate form.  States and their

@@ -106,9 +106,15 @@ __global__ void batch_prep_kernel(unsigned char* plan, const double* __restrict_
       if (grad) dlay[l] = layer_derivs(tab, L, l, pj, lay[l]);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < I; i += blockDim.x) {
+    for (int i = threadIdx.x; i < I; i += blockDim.x)
       coef[i] = interface_coeffs(pj, i, lay[i], lay[i + 1]);
-      if (grad) interface_tangents(pj, i, lay[i], dlay[i], lay[i + 1], dlay[i + 1], tan[i]);
+    if (grad) {  // one thread per (interface, tangent column)
+      for (int t = threadIdx.x; t < 6 * I; t += blockDim.x) {
+        const int i = t / 6, col = t % 6;
+        cd c[10];
+        interface_tangent_col(pj, i, lay[i], dlay[i], lay[i + 1], dlay[i + 1], col, c);
+        for (int k = 0; k < 10; ++k) tan[i].t[k][col] = c[k];
+      }
     }
     __syncthreads();
   }

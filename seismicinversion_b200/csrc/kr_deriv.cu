@@ -3,7 +3,7 @@
 //
 // Three kernels (JAC, GRAD and VJP modes of the sweep):
 //   deriv_layer_kernel : per (p, layer)      layer terms + derivative factors  -> workspace
-//   deriv_iface_kernel : per (p, interface)  coefficients + 10x6 tangents      -> workspace
+//   deriv_iface_kernel : per (p, interface, tangent column) coefficients + 10x6 tangents -> workspace
 //   deriv_sweep_kernel : per (omega, p)      forward sweep with checkpoints every <= 64 steps, then the
 //                        reverse sweep segment by segment (each segment recomputed from its
 //                        checkpoint: per-layer recomputation instead of a full tape), giving
@@ -72,16 +72,23 @@ __global__ void deriv_layer_kernel(const double* __restrict__ tab, int L,
   dlay[idx] = layer_derivs(tab, L, l, p[j], lp);
 }
 
+// One thread per (slowness, interface, tangent column); column 0's thread also writes the
+// coefficients.
 __global__ void deriv_iface_kernel(const double* __restrict__ p, int n_p, int L,
                                    const LayerP* __restrict__ lay,
                                    const LayerD* __restrict__ dlay, Iface* coef, ScatTan* tan) {
   const int I = L - 1;
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= n_p * I) return;
-  const int j = idx / I, i = idx % I;
-  const LayerP up = lay[j * L + i], lo = lay[j * L + i + 1];
-  coef[idx] = interface_coeffs(p[j], i, up, lo);
-  interface_tangents(p[j], i, up, dlay[j * L + i], lo, dlay[j * L + i + 1], tan[idx]);
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)n_p * I * 6) return;
+  const int col = (int)(t % 6);
+  const size_t idx = t / 6;
+  const int j = (int)(idx / I), i = (int)(idx % I);
+  const size_t e = (size_t)j * L + i;
+  const LayerP up = lay[e], lo = lay[e + 1];
+  if (col == 0) coef[idx] = interface_coeffs(p[j], i, up, lo);
+  cd c[10];
+  interface_tangent_col(p[j], i, up, dlay[e], lo, dlay[e + 1], col, c);
+  for (int k = 0; k < 10; ++k) tan[idx].t[k][col] = c[k];
 }
 
 // Jacobian mode: writes dR/dtheta of layer l.
@@ -429,8 +436,8 @@ static kr_status launch_deriv(const double* layers, int L, const double* p, int 
   deriv_layer_kernel<<<nb, 128, 0, st>>>(layers, L, p, n_p, w.lay, w.dlay);
   kr_status s = check_launch("kr_deriv: layers");
   if (s != KR_OK) return s;
-  nb = (n_p * I + 63) / 64;
-  deriv_iface_kernel<<<nb, 64, 0, st>>>(p, n_p, L, w.lay, w.dlay, w.coef, w.tan);
+  const unsigned nbi = (unsigned)(((size_t)n_p * I * 6 + 127) / 128);
+  deriv_iface_kernel<<<nbi, 128, 0, st>>>(p, n_p, L, w.lay, w.dlay, w.coef, w.tan);
   s = check_launch("kr_deriv: interfaces");
   if (s != KR_OK) return s;
   const int seg = checkpoint_spacing(I - 1 > 0 ? I - 1 : 1);

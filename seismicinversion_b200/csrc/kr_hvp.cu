@@ -4,9 +4,9 @@
 // Kernels (all stream-ordered, no host synchronisation):
 //   hvp_layer_kernel : per (p, layer)            layer terms, first and second derivative
 //                                                 factors -> workspace
-//   hvp_iface_kernel : per (p, interface)        coefficients + 10x6 tangents
+//   hvp_iface_kernel : per (p, interface, column) coefficients + 10x6 tangents
 //   hvp_ldot_kernel  : per (direction, p, layer) layer values with tangents along v
-//   hvp_idot_kernel  : per (direction, p, iface) coefficients with tangents along v and the
+//   hvp_idot_kernel  : per (direction, p, iface, column) coefficients with tangents along v and the
 //                                                 tangents of the 10x6 coefficient tangents
 //   hvp_sum_kernel   : per (direction, p, omega) forward sweep, seed and reverse sweep in dual
 //                                                 numbers, the per-step dual adjoints summed over
@@ -88,12 +88,17 @@ __global__ void hvp_iface_kernel(const double* __restrict__ p, int n_p, int L,
                                  const LayerP* __restrict__ lay, const LayerD* __restrict__ dlay,
                                  Iface* coef, ScatTan* tan) {
   const int I = L - 1;
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= n_p * I) return;
-  const int j = idx / I, i = idx % I;
-  const LayerP up = lay[j * L + i], lo = lay[j * L + i + 1];
-  coef[idx] = interface_coeffs(p[j], i, up, lo);
-  interface_tangents(p[j], i, up, dlay[j * L + i], lo, dlay[j * L + i + 1], tan[idx]);
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)n_p * I * 6) return;
+  const int col = (int)(t % 6);
+  const size_t idx = t / 6;
+  const int j = (int)(idx / I), i = (int)(idx % I);
+  const size_t e = (size_t)j * L + i;
+  const LayerP up = lay[e], lo = lay[e + 1];
+  if (col == 0) coef[idx] = interface_coeffs(p[j], i, up, lo);
+  cd c[10];
+  interface_tangent_col(p[j], i, up, dlay[e], lo, dlay[e + 1], col, c);
+  for (int k = 0; k < 10; ++k) tan[idx].t[k][col] = c[k];
 }
 
 // V: [n_dir][4L] directions, theta order k*L + l (alpha, beta, rho, h)
@@ -117,15 +122,19 @@ __global__ void hvp_idot_kernel(const double* __restrict__ p, int L, int n_p, in
                                 const Iface* __restrict__ coef, const LayerV* __restrict__ lv,
                                 IfS<DC>* ifs, ScatTan* tant) {
   const int I = L - 1;
-  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (size_t)n_dir * n_p * I) return;
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)n_dir * n_p * I * 6) return;
+  const int col = (int)(t % 6);
+  const size_t idx = t / 6;
   const int i = (int)(idx % I);
   const size_t jd = idx / I;
   const int j = (int)(jd % n_p);
   const LayerV* l0 = lv + jd * L;
   IfS<DC> c;
-  interface_dot(p[j], i, l0[i], l0[i + 1], c, tant[idx]);
-  ifs[idx] = iface_dual(coef[(size_t)j * I + i], c);
+  cd tc[10];
+  interface_dot_col(p[j], i, l0[i], l0[i + 1], col, col == 0 ? &c : nullptr, tc);
+  for (int k = 0; k < 10; ++k) tant[idx].t[k][col] = tc[k];
+  if (col == 0) ifs[idx] = iface_dual(coef[(size_t)j * I + i], c);
 }
 
 template <int MODE>
@@ -376,8 +385,8 @@ static kr_status launch_hvp(const double* layers, int L, const double* p, int n_
   hvp_layer_kernel<<<nb, 128, 0, st>>>(layers, L, p, n_p, w.lay, w.dlay, w.d2);
   kr_status s = check_launch("kr_hvp: layers");
   if (s != KR_OK) return s;
-  nb = (n_p * I + 63) / 64;
-  hvp_iface_kernel<<<nb, 64, 0, st>>>(p, n_p, L, w.lay, w.dlay, w.coef, w.tan);
+  const unsigned nbi = (unsigned)(((size_t)n_p * I * 6 + 127) / 128);
+  hvp_iface_kernel<<<nbi, 128, 0, st>>>(p, n_p, L, w.lay, w.dlay, w.coef, w.tan);
   s = check_launch("kr_hvp: interfaces");
   if (s != KR_OK) return s;
   size_t n = (size_t)n_dir * n_p * L;
@@ -385,8 +394,8 @@ static kr_status launch_hvp(const double* layers, int L, const double* p, int n_
                                                                w.dlay, w.d2, w.lv);
   s = check_launch("kr_hvp: layer tangents");
   if (s != KR_OK) return s;
-  n = (size_t)n_dir * n_p * I;
-  hvp_idot_kernel<<<(unsigned)((n + 63) / 64), 64, 0, st>>>(p, L, n_p, n_dir, w.coef, w.lv, w.ifs,
+  n = (size_t)n_dir * n_p * I * 6;
+  hvp_idot_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(p, L, n_p, n_dir, w.coef, w.lv, w.ifs,
                                                             w.tant);
   s = check_launch("kr_hvp: interface tangents");
   if (s != KR_OK) return s;

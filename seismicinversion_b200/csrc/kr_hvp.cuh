@@ -331,21 +331,23 @@ KR_HD LayerV layer_dot(const double* tab, int n_layers, int l, const LayerP& lp,
 // Coefficient tangents along v and their own derivatives: out_c[k] = coefficient k as DC
 // (value, d/dv), out_t.t[k][j] = d coefficient_k / d theta_j along v (the tangent of the
 // ScatTan entry), for the interface between layers `iface` (upper) and iface + 1 (lower).
-KR_HD void interface_dot(double p, int iface, const LayerV& up, const LayerV& lo, IfS<DC>& out_c,
-                         ScatTan& out_t) {
-  typedef DualG<6, DC> G;
-  G eta1 = gconst<6>(up.eta), neta1 = gconst<6>(up.neta), rho1 = gconst<6>(up.rho);
-  G betac1 = gconst<6>(up.betac);
-  G eta2 = gconst<6>(lo.eta), neta2 = gconst<6>(lo.neta), rho2 = gconst<6>(lo.rho);
-  G betac2 = gconst<6>(lo.betac);
-  eta1.d[0] = up.eta_alpha;
-  neta1.d[1] = up.neta_beta;
-  betac1.d[1] = up.betac_beta;
-  rho1.d[2] = dc(mk(1.0, 0.0));
-  eta2.d[3] = lo.eta_alpha;
-  neta2.d[4] = lo.neta_beta;
-  betac2.d[4] = lo.betac_beta;
-  rho2.d[5] = dc(mk(1.0, 0.0));
+// interface_dot_col computes column j alone (nested duals with one outer direction, the
+// component-wise arithmetic of the six-direction pass) and, given out_c, the coefficients.
+KR_HD void interface_dot_col(double p, int iface, const LayerV& up, const LayerV& lo, int j,
+                             IfS<DC>* out_c, cd col[10]) {
+  typedef DualG<1, DC> G;
+  G eta1 = gconst<1>(up.eta), neta1 = gconst<1>(up.neta), rho1 = gconst<1>(up.rho);
+  G betac1 = gconst<1>(up.betac);
+  G eta2 = gconst<1>(lo.eta), neta2 = gconst<1>(lo.neta), rho2 = gconst<1>(lo.rho);
+  G betac2 = gconst<1>(lo.betac);
+  switch (j) {
+    case 0: eta1.d[0] = up.eta_alpha; break;
+    case 1: neta1.d[0] = up.neta_beta; betac1.d[0] = up.betac_beta; break;
+    case 2: rho1.d[0] = dc(mk(1.0, 0.0)); break;
+    case 3: eta2.d[0] = lo.eta_alpha; break;
+    case 4: neta2.d[0] = lo.neta_beta; betac2.d[0] = lo.betac_beta; break;
+    default: rho2.d[0] = dc(mk(1.0, 0.0)); break;
+  }
   IfaceT<G> f;
   if (iface == 0)
     ocean_bottom<G>(p, eta1, rho1, eta2, neta2, rho2, betac2, f);
@@ -353,13 +355,22 @@ KR_HD void interface_dot(double p, int iface, const LayerV& up, const LayerV& lo
     solid_solid<G>(p, eta1, neta1, rho1, betac1, eta2, neta2, rho2, betac2, f);
   const G* c[10] = {&f.rd11, &f.rd12, &f.rd22, &f.ru11, &f.ru12,
                     &f.ru22, &f.td11, &f.td12, &f.td21, &f.td22};
-  DC* oc[10] = {&out_c.rd11, &out_c.rd12, &out_c.rd22, &out_c.ru11, &out_c.ru12,
-                &out_c.ru22, &out_c.td11, &out_c.td12, &out_c.td21, &out_c.td22};
-  for (int k = 0; k < 10; ++k) {
-    *oc[k] = c[k]->v;
-    for (int j = 0; j < 6; ++j) out_t.t[k][j] = c[k]->d[j].t;
+  for (int k = 0; k < 10; ++k) col[k] = c[k]->d[0].t;
+  if (out_c) {
+    DC* oc[10] = {&out_c->rd11, &out_c->rd12, &out_c->rd22, &out_c->ru11, &out_c->ru12,
+                  &out_c->ru22, &out_c->td11, &out_c->td12, &out_c->td21, &out_c->td22};
+    for (int k = 0; k < 10; ++k) *oc[k] = c[k]->v;
+    iface_derived(*out_c);
   }
-  iface_derived(out_c);
+}
+
+KR_HD void interface_dot(double p, int iface, const LayerV& up, const LayerV& lo, IfS<DC>& out_c,
+                         ScatTan& out_t) {
+  for (int j = 0; j < 6; ++j) {
+    cd col[10];
+    interface_dot_col(p, iface, up, lo, j, j == 0 ? &out_c : nullptr, col);
+    for (int k = 0; k < 10; ++k) out_t.t[k][j] = col[k];
+  }
 }
 
 // The interface as IfS<DC> from the value coefficients and the value-plus-tangent ones
