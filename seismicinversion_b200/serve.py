@@ -11,7 +11,8 @@ gradient requests the observed R) from any thread; each returns a ``Request`` wh
 * launches each admitted group as one persistent batched launch (``ModelBatch``) on one of
   ``n_streams`` streams, keeping up to ``max_inflight`` batches on the GPU at once, so
   requests that arrive while others run are batched into the next launch and their work
-  overlaps on the device;
+  overlaps on the device; a group of one request (a lightly loaded server) runs the
+  single-model kernels instead, which skip the batch plan's host-side build;
 * polls completion events and marks requests done.  Results stay on the device as tensors
   (views of the batch's single device block), so the budget keeps a batch's bytes charged
   until every request of that batch has released its results: ``Request.release()``, or
@@ -166,14 +167,22 @@ class _Record:
 
 
 class GpuBatchExecutor:
-    """Runs an admitted group as one ModelBatch launch on a stream; ``ready`` polls its event."""
+    """Runs an admitted group as one ModelBatch launch on a stream; ``ready`` polls its event.
 
-    def __init__(self, device=None, n_streams: int = 2, schedule=(128, 256)):
+    Groups of at most ``direct_max_requests`` requests (default 1) run the single-model
+    entry points (``kr_reflectivity``, ``kr_misfit_gradient`` with R) on the stream instead:
+    the same R bit for bit, the gradient to rounding (the batch adds per-block partials in
+    another order), without the plan build."""
+
+    def __init__(self, device=None, n_streams: int = 2, schedule=(128, 256),
+                 direct_max_requests: int = 1):
         import torch
 
         from . import device as D
 
         self.torch = torch
+        self.D = D
+        self.direct_max = int(direct_max_requests)
         self.dev = D.require_cuda(device)
         self.streams = [torch.cuda.Stream(self.dev) for _ in range(n_streams)]
         # every batch's device block comes from this stream's allocator pool, so cached
@@ -207,6 +216,12 @@ class GpuBatchExecutor:
         torch = self.torch
         s = self.streams[self._k % len(self.streams)]
         self._k += 1
+        if len(reqs) <= self.direct_max:
+            with torch.cuda.stream(s):
+                res = [self._direct(r) for r in reqs]
+                ev = torch.cuda.Event()
+                ev.record(s)
+            return (None, ev, res)
         with torch.cuda.stream(s):
             items = [BatchItem(r.model, r.p, r.omega, gradient=r.gradient, R_obs=r.R_obs,
                                free_surface=r.free_surface, store_R=r.gradient) for r in reqs]
@@ -215,13 +230,24 @@ class GpuBatchExecutor:
             batch.launch()
             ev = torch.cuda.Event()
             ev.record(s)
-        return (batch, ev)
+        return (batch, ev, None)
+
+    def _direct(self, r: Request) -> dict:
+        D = self.D
+        tab = D.layer_table(r.model, self.dev)
+        if r.gradient:
+            out, R = D.misfit_gradient(tab, r.p, r.omega, r.R_obs, r.free_surface, want_R=True)
+            L = tab.shape[1]
+            return {"R": R, "chi": out[4 * L], "grad": out[:4 * L]}
+        return {"R": D.reflectivity(tab, r.p, r.omega, r.free_surface)}
 
     def ready(self, handle) -> bool:
         return handle[1].query()
 
     def results(self, handle, reqs: list[Request]) -> list[dict]:
-        batch, _ = handle
+        batch, _, direct = handle
+        if direct is not None:
+            return direct
         out = []
         for b, r in enumerate(reqs):
             res = {"R": batch.reflectivity(b)}

@@ -63,3 +63,22 @@ def test_mix_matches_single_calls_and_alone_vs_mix():
         assert torch.equal(mixed.result["R"], a["R"])
         st = srv.stats()
         assert st["completed"] == 61 and st["batches"] >= 2
+
+
+def test_single_request_group_runs_the_single_model_kernels():
+    """A group of one request runs the single-model entry points: results identical to the
+    direct call, bit for bit (gradient included)."""
+    from seismicinversion_b200 import device as D
+    from seismicinversion_b200.serve import GpuBatchExecutor, KennettServer
+
+    (m, p, w, _, _), (m1, p1, w1, g1, o1) = _requests(2, seed=9)
+    ex = GpuBatchExecutor(n_streams=2)
+    with KennettServer(executor=ex, max_batch_requests=16) as srv:
+        res = srv.submit(m1, p1, w1, gradient=g1, R_obs=o1).wait(60)
+        fwd = srv.submit(m, p, w).wait(60)
+    tab = D.layer_table(m1)
+    out, R = D.misfit_gradient(tab, p1, w1, o1, want_R=True)
+    L = m1.n_layers
+    assert g1 and torch.equal(res["grad"], out[:4 * L]) and torch.equal(res["R"], R)
+    assert float(res["chi"]) == float(out[4 * L])
+    assert torch.equal(fwd["R"], D.reflectivity(D.layer_table(m), p, w))
