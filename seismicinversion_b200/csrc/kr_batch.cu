@@ -11,9 +11,11 @@
 // and uploads them into the caller's plan buffer.  kr_batch_launch (device only, capturable
 // in a CUDA graph) then runs:
 //   1. batch_prep_kernel: one block per pair -> layer terms and interface coefficients (and,
-//      for gradient models, layer derivative factors and coefficient tangents) into the plan;
-//   2. batch_forward_kernel and batch_gradient_kernel: persistent grids (resident blocks
-//      only) that pull items with an atomic counter until the list is exhausted.
+//      for gradient models, layer derivative factors and coefficient tangents, one thread per
+//      interface and tangent column) into the plan;
+//   2. batch_forward_kernel and batch_grad_sums_kernel (batch_gradient_kernel where a model's
+//      frequency sums exceed shared memory): persistent grids (resident blocks only) that
+//      pull items with an atomic counter until the list is exhausted.
 // Gradient items reduce their contributions per block in a fixed order and add them to the
 // model's chi_grad with FP64 atomics (the order of those additions across blocks is not
 // fixed: results agree to rounding, ~1e-16 relative, run to run).

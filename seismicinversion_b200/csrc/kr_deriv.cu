@@ -1,18 +1,19 @@
 // Jacobian and misfit gradient of the reflectivity with respect to every layer's
 // (alpha, beta, rho, h): the hand-written adjoint of the Kennett recursion.
 //
-// Three kernels (JAC, GRAD and VJP modes of the sweep):
-//   deriv_layer_kernel : per (p, layer)      layer terms + derivative factors  -> workspace
-//   deriv_iface_kernel : per (p, interface, tangent column) coefficients + 10x6 tangents -> workspace
-//   deriv_sweep_kernel : per (omega, p)      forward sweep with checkpoints every <= 64 steps, then the
-//                        reverse sweep segment by segment (each segment recomputed from its
-//                        checkpoint: per-layer recomputation instead of a full tape), giving
-//                        dR/d(theta) for all 4L parameters.  JAC mode writes them
-//                        (J[p][k*L + l][omega], k = alpha, beta, rho, h); GRAD mode contracts
-//                        them with the residual, 2 Re(conj(R - R_obs) dR/dtheta), VJP mode
-//                        with a caller's cotangent, Re(conj(gR) dR/dtheta); both reduce over
-//                        the block in a fixed order and a last kernel adds the block partials
-//                        in order (deterministic).
+// Kernels (stream-ordered, no host synchronisation):
+//   deriv_prep_kernel  : per (p, interface, tangent column or coefficients): layer terms and
+//                        derivative factors, interface coefficients and their 10 x 6 tangents
+//                        -> workspace
+//   deriv_sum_kernel   : GRAD / VJP, per (omega, p): forward sweep with a tape of up to 64
+//                        steps (deeper models checkpoint and recompute segments), seed
+//                        2 conj(R - R_obs) (GRAD) or conj(gR) (VJP), reverse sweep; the per-step
+//                        adjoints are summed over the block's frequencies and contracted with
+//                        the tangents once per (p, interface) -> per-block partials
+//   deriv_sweep_kernel : the same sweep with the contraction per (omega, p): JAC mode writes
+//                        dR/dtheta (J[p][k*L + l][omega], k = alpha, beta, rho, h); GRAD / VJP
+//                        for models whose frequency sums exceed shared memory
+//   reduce_partials_kernel : adds the block partials in a fixed order (deterministic)
 // Replaces the torch autograd graph of kennett_reflectivity_torch (kennett_torch.py:312-480),
 // jacobian (:611-641), its reverse pass under torch.autograd.grad, and the per-slowness
 // gradient of taup_misfit_grad_hessian (taup_inversion.py:112-187).
@@ -61,34 +62,53 @@ static DerivWs deriv_ws(void* base, int L, int n_p, size_t n_blocks) {
   return w;
 }
 
-__global__ void deriv_layer_kernel(const double* __restrict__ tab, int L,
-                                   const double* __restrict__ p, int n_p, LayerP* lay,
-                                   LayerD* dlay) {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= n_p * L) return;
-  const int j = idx / L, l = idx % L;
-  LayerP lp = layer_terms(tab, L, l, p[j]);
-  lay[idx] = lp;
-  dlay[idx] = layer_derivs(tab, L, l, p[j], lp);
-}
+// One block per (slowness, chunk of kPrepThreads interface items): the layer terms and
+// derivative factors of the chunk's layers go to shared memory, then one thread per
+// (interface, item): items 0..5 form one tangent column each, item 6 the interface's
+// coefficients and the workspace copy of its upper layer (and of the half-space, for the last
+// interface), so no lane of a warp waits on another's extra work.  The coefficients read the
+// layer terms back from shared memory after a barrier, as the forward kernel's prologue
+// does, so they round exactly as there (R bit-identical across entry points).
+constexpr int kPrepThreads = 128;
+constexpr int kPrepItems = 7;                                  // per interface
+constexpr int kPrepLayers = kPrepThreads / kPrepItems + 3;     // layers one chunk touches
 
-// One thread per (slowness, interface, tangent column); column 0's thread also writes the
-// coefficients.
-__global__ void deriv_iface_kernel(const double* __restrict__ p, int n_p, int L,
-                                   const LayerP* __restrict__ lay,
-                                   const LayerD* __restrict__ dlay, Iface* coef, ScatTan* tan) {
+__global__ void __launch_bounds__(kPrepThreads)
+deriv_prep_kernel(const double* __restrict__ tab, int L, const double* __restrict__ p,
+                  int n_chunks, LayerP* lay, LayerD* dlay, Iface* coef, ScatTan* tan) {
+  __shared__ LayerP s_lp[kPrepLayers];
+  __shared__ LayerD s_ld[kPrepLayers];
   const int I = L - 1;
-  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (size_t)n_p * I * 6) return;
-  const int col = (int)(t % 6);
-  const size_t idx = t / 6;
-  const int j = (int)(idx / I), i = (int)(idx % I);
-  const size_t e = (size_t)j * L + i;
-  const LayerP up = lay[e], lo = lay[e + 1];
-  if (col == 0) coef[idx] = interface_coeffs(p[j], i, up, lo);
+  const int j = blockIdx.x / n_chunks;
+  const int t0 = (blockIdx.x % n_chunks) * kPrepThreads;
+  const int t1 = min(t0 + kPrepThreads, kPrepItems * I);
+  const int l0 = t0 / kPrepItems, l1 = (t1 - 1) / kPrepItems + 1;  // the chunk's layers
+  const double pj = p[j];
+  for (int l = l0 + threadIdx.x; l <= l1; l += blockDim.x) {
+    const LayerP lp = layer_terms(tab, L, l, pj);
+    s_lp[l - l0] = lp;
+    s_ld[l - l0] = layer_derivs(tab, L, l, pj, lp);
+  }
+  __syncthreads();
+  const int t = t0 + threadIdx.x;
+  if (t >= t1) return;
+  const int i = t / kPrepItems, item = t % kPrepItems;
+  const size_t idx = (size_t)j * I + i, e = (size_t)j * L + i;
+  const LayerP& up = s_lp[i - l0];
+  const LayerP& lo = s_lp[i + 1 - l0];
+  if (item == 6) {
+    lay[e] = up;
+    dlay[e] = s_ld[i - l0];
+    if (i == I - 1) {
+      lay[e + 1] = lo;
+      dlay[e + 1] = s_ld[i + 1 - l0];
+    }
+    coef[idx] = interface_coeffs(pj, i, up, lo);
+    return;
+  }
   cd c[10];
-  interface_tangent_col(p[j], i, up, dlay[e], lo, dlay[e + 1], col, c);
-  for (int k = 0; k < 10; ++k) tan[idx].t[k][col] = c[k];
+  interface_tangent_col(pj, i, up, s_ld[i - l0], lo, s_ld[i + 1 - l0], item, c);
+  for (int k = 0; k < 10; ++k) tan[idx].t[k][item] = c[k];
 }
 
 // Jacobian mode: writes dR/dtheta of layer l.
@@ -432,13 +452,11 @@ static kr_status launch_deriv(const double* layers, int L, const double* p, int 
   DerivWs w = deriv_ws(ws, L, n_p, GRAD ? n_blocks : 0);
   if (!ws || ws_bytes < w.bytes) return KR_ERR_WORKSPACE;
   const int I = L - 1;
-  int nb = (n_p * L + 127) / 128;
-  deriv_layer_kernel<<<nb, 128, 0, st>>>(layers, L, p, n_p, w.lay, w.dlay);
-  kr_status s = check_launch("kr_deriv: layers");
-  if (s != KR_OK) return s;
-  const unsigned nbi = (unsigned)(((size_t)n_p * I * 6 + 127) / 128);
-  deriv_iface_kernel<<<nbi, 128, 0, st>>>(p, n_p, L, w.lay, w.dlay, w.coef, w.tan);
-  s = check_launch("kr_deriv: interfaces");
+  const int n_chunks = (kPrepItems * I + kPrepThreads - 1) / kPrepThreads;
+  if ((size_t)n_p * n_chunks > 0x7fffffffULL) return KR_ERR_TOO_LARGE;
+  deriv_prep_kernel<<<(unsigned)(n_p * n_chunks), kPrepThreads, 0, st>>>(
+      layers, L, p, n_chunks, w.lay, w.dlay, w.coef, w.tan);
+  kr_status s = check_launch("kr_deriv: layers and interfaces");
   if (s != KR_OK) return s;
   const int seg = checkpoint_spacing(I - 1 > 0 ? I - 1 : 1);
   if (GRAD && deriv_sums_enabled()) {
