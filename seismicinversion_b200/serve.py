@@ -192,14 +192,23 @@ class GpuBatchExecutor:
         self.schedule = schedule
         self._k = 0
 
-    def prewarm(self, device_bytes: int, host_bytes: int = 16 << 20) -> None:
+    def prewarm(self, device_bytes: int, host_bytes: int = 16 << 20,
+                stream_bytes: int = 256 << 20) -> None:
         """Reserve a caching-allocator segment on the allocation stream (and pinned host blocks) so
         that steady-state batches reuse cached memory instead of calling cudaMalloc /
-        cudaHostAlloc, which are slow and (cudaMalloc) synchronise the device."""
+        cudaHostAlloc, which are slow and (cudaMalloc) synchronise the device.  Each execution
+        stream also gets ``stream_bytes`` of large blocks and a few small-pool segments: groups
+        of one request allocate their outputs and workspaces there."""
         torch = self.torch
         with torch.cuda.stream(self.alloc_stream):
             x = torch.empty(int(device_bytes), dtype=torch.uint8, device=self.dev)
             del x
+        for s in self.streams:
+            with torch.cuda.stream(s):
+                xs = [torch.empty(int(stream_bytes), dtype=torch.uint8, device=self.dev)]
+                xs += [torch.empty(512 << 10, dtype=torch.uint8, device=self.dev)
+                       for _ in range(16)]
+                del xs
         # one pinned block per power-of-two size class from 1 KB up (the host caching
         # allocator serves plan images and staging copies from these)
         sizes, b = [], 1024
