@@ -111,8 +111,9 @@ def _enqueue_gather(dev, stage, off, sizes, L, nwm, nw, np_slow, dp, free_surfac
                     return_reflectivity, copy_chunks):
     """Enqueues one gather on the current stream (and the copy stream): upload of the pinned
     staging buffer, the reflectivity grid in slowness blocks with each block's host copy,
-    the Bessel sum, the traces and their host copy.  No synchronisation; returns the pinned
-    host outputs (gather, R or None) and the device R."""
+    the Bessel sum, the traces and (with the reflectivity) their host copy.  No
+    synchronisation; returns (pinned host gather or None, pinned host R or None, device R,
+    device gather)."""
     main = torch.cuda.current_stream(dev)
     dbuf = torch.empty(stage.shape, dtype=torch.float64, device=dev)
     dbuf.copy_(stage, non_blocking=True)
@@ -138,9 +139,11 @@ def _enqueue_gather(dev, stage, off, sizes, L, nwm, nw, np_slow, dp, free_surfac
                 Rh[a:b].copy_(R[a:b], non_blocking=True)
     U = _dev.bessel_sum(R, p_t, pw_t, dp, wr_t, off_t)
     g = _dev.traces(U, nw, S=S_t, decay=dec_t)
-    gh = _pinned(tuple(g.shape), g.dtype)
-    gh.copy_(g, non_blocking=True)
-    return gh, Rh, R
+    gh = None
+    if return_reflectivity:
+        gh = _pinned(tuple(g.shape), g.dtype)
+        gh.copy_(g, non_blocking=True)
+    return gh, Rh, R, g
 
 
 # Gathers replayed from CUDA graphs, keyed by grid, layer count and options: a repeated call
@@ -187,12 +190,12 @@ def compute_gather_gpu(model: LayerModel, offsets, T: float = 64.0, nw: int = 20
     8192 x 2047 grid at ~57 GB/s; more blocks shorten the launches below full waves).
     With ``use_graph`` a grid seen before (same sizes, offsets, source, layer count and
     options) replays a captured CUDA graph.  Every returned array is the caller's own, as in
-    the reference.  With ``return_reflectivity``, ``copy_outputs=False`` instead returns the
-    gather and the R grid as views of this module's pinned receive buffers (no host copy of
-    the 268 MB grid on the 8192 x 2047 workload), valid until the next call with the same grid
-    overwrites them.  Calls share module-level staging
-    buffers, grid caches and graphs under one lock: calls from several threads run one at a
-    time.
+    the reference (without the R grid, the gather is a new page-locked host block that the
+    device copies into directly).  With ``return_reflectivity``, ``copy_outputs=False``
+    instead returns the gather and the R grid as views of this module's pinned receive
+    buffers (no host copy of the 268 MB grid on the 8192 x 2047 workload), valid until the
+    next call with the same grid overwrites them.  Calls share module-level staging buffers,
+    grid caches and graphs under one lock: calls from several threads run one at a time.
     """
     with _CALL_LOCK:
         return _compute_gather_gpu(model, offsets, T, nw, np_slow, p_max, gamma, source_func,
@@ -231,21 +234,25 @@ def _compute_gather_gpu(model, offsets, T, nw, np_slow, p_max, gamma, source_fun
     if use_graph:
         entry = _gather_graph((dev, grid_key) + args[3:], dev, args, copy)
     if entry is not None:
-        graph, (gh, Rh, _) = entry
+        graph, (gh, Rh, _, g) = entry
         graph.replay()
     else:
-        gh, Rh, R = _enqueue_gather(dev, *args)
+        gh, Rh, R, g = _enqueue_gather(dev, *args)
         if return_reflectivity:
             R.record_stream(copy)
     if return_reflectivity:
         copy.synchronize()
-    main.synchronize()
-    if return_reflectivity:
+        main.synchronize()
         Rn, gn = Rh.numpy(), gh.numpy()
         if copy_outputs:
             Rn, gn = Rn.copy(), gn.copy()
         return time.copy(), np.asarray(offsets), gn, Rn
-    return time.copy(), np.asarray(offsets), gh.numpy().copy()
+    # the traces go straight into a new page-locked block from torch's caching host allocator:
+    # the caller's own array, no host-side copy (freed blocks are reused without new faults)
+    out = torch.empty(tuple(g.shape), dtype=g.dtype, pin_memory=True)
+    out.copy_(g, non_blocking=True)
+    main.synchronize()
+    return time.copy(), np.asarray(offsets), out.numpy()
 
 
 _COPY_STREAMS: dict = {}

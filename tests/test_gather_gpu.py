@@ -232,6 +232,14 @@ def test_consecutive_calls_return_independent_arrays():
     _, _, G2, V2 = compute_gather_gpu(m2, offs, copy_outputs=False, **kw)
     assert np.shares_memory(V1, V2) and np.array_equal(V2, R2) and not np.array_equal(V1, v1)
     assert np.shares_memory(G1, G2) and np.array_equal(G2, g2)
+    # the reference's signature (gather only): a new page-locked block per call
+    kw0 = {k: v for k, v in kw.items() if k != "return_reflectivity"}
+    for _ in range(3):  # eager, capture, replay
+        _, _, h1 = compute_gather_gpu(m1, offs, **kw0)
+        k1 = h1.copy()
+        _, _, h2 = compute_gather_gpu(m2, offs, **kw0)
+        assert np.array_equal(h1, k1) and not np.shares_memory(h1, h2)
+        assert np.array_equal(h1, g1) and np.array_equal(h2, g2)
 
 
 def test_full_size_gather_end_to_end_vs_oracle():
