@@ -574,3 +574,70 @@ def test_invert_taup_trajectory_vs_reference_21_layers(golden):
     assert np.allclose(res.misfit_history, g["misfit"], rtol=1e-6, atol=0)
     assert np.allclose(res.param_error_history, g["param_err"], rtol=1e-6, atol=0)
     assert np.allclose(res.recovered_model.alpha, g["rec_alpha"], rtol=1e-6)
+
+
+@pytest.mark.parametrize("n_sub,fs", [(60, False), (120, True)])
+def test_deep_model_hvp_vs_gradient_differences(n_sub, fs):
+    """kr_misfit_hvp on models deeper than one 32-step dual tape: 62 layers (the frequency-sum
+    kernel, two recomputed segments) and 122 layers with the free surface (per-step fallback:
+    its sums exceed shared memory; four segments).  H v against central differences of the
+    exact gradient along v, to their truncation error."""
+    from seismicinversion_b200 import device as D
+    from seismicinversion_b200.earth_models import random_layered_model
+
+    m = random_layered_model(n_sub, seed=70 + n_sub)
+    tab = D.layer_table(m)
+    L = tab.shape[1]
+    p = torch.tensor([0.1, 0.35], dtype=torch.float64, device=tab.device)
+    w = (torch.arange(1, 49, dtype=torch.float64, device=tab.device) * (2 * np.pi / 64)
+         + 1j * (np.pi / 64))
+    R_obs = 0.95 * D.reflectivity(tab, p, w, fs)
+    gen = torch.Generator(device="cpu").manual_seed(n_sub)
+    scale = torch.cat([tab[0], tab[1], tab[2], torch.cat([tab[3, :-1],
+                                                          torch.zeros(1, device=tab.device)])])
+    V = torch.randn(2, 4 * L, dtype=torch.float64, generator=gen).to(tab.device) * scale
+    V[:, L] = 0.0  # the ocean's beta stays 0
+    HV = D.misfit_hvp(tab, p, w, R_obs, V, fs)
+    for d in range(2):
+        eps = 1e-6
+
+        def grad(s):
+            t = tab.clone()
+            t[0] += s * V[d, :L]
+            t[1] += s * V[d, L:2 * L]
+            t[2] += s * V[d, 2 * L:3 * L]
+            t[3, :-1] += s * V[d, 3 * L:4 * L - 1]
+            return D.misfit_gradient(t, p, w, R_obs, fs)[0][:4 * L]
+
+        fd = (grad(eps) - grad(-eps)) / (2 * eps)
+        assert rel_err(HV[d].cpu().numpy(), fd.cpu().numpy()) < 1e-6, d
+
+
+def test_derivative_entry_points_with_empty_grids():
+    """Empty slowness or frequency grids and zero directions: gradients, VJPs and H v are
+    zeros, Jacobians and their directional derivatives are empty, nothing raises."""
+    from seismicinversion_b200 import device as D
+    from seismicinversion_b200.earth_models import random_layered_model
+
+    m = random_layered_model(4, seed=3)
+    tab = D.layer_table(m)
+    L = tab.shape[1]
+    V = torch.ones((3, 4 * L), dtype=torch.float64, device=tab.device)
+    w = np.arange(1, 9) * 0.3 + 0.05j
+    for p, om in ((np.zeros(0), w), (np.array([0.2, 0.3]), np.zeros(0, complex))):
+        n_p, n_w = len(p), len(om)
+        zeros = np.zeros((n_p, n_w), complex)
+        out, R = D.misfit_gradient(tab, p, om, zeros, want_R=True)
+        assert torch.count_nonzero(out) == 0 and out.shape == (4 * L + 1,)
+        assert tuple(R.shape) == (n_p, n_w)
+        g, _ = D.vjp(tab, p, om, zeros)
+        assert torch.count_nonzero(g) == 0 and g.shape == (4 * L,)
+        _, J = D.jacobian(tab, p, om, want_R=False)
+        assert tuple(J.shape) == (n_p, 4 * L, n_w)
+        HV = D.misfit_hvp(tab, p, om, zeros, V)
+        assert torch.count_nonzero(HV) == 0 and tuple(HV.shape) == (3, 4 * L)
+        assert tuple(D.jacobian_dot(tab, p, om, V).shape) == (3, n_p, 4 * L, n_w)
+    p = np.array([0.2])
+    R_obs = D.reflectivity(tab, p, w)
+    assert tuple(D.misfit_hvp(tab, p, w, R_obs, V[:0]).shape) == (0, 4 * L)
+    assert tuple(D.jacobian_dot(tab, p, w, V[:0]).shape) == (0, 1, 4 * L, len(w))
