@@ -218,7 +218,9 @@ static size_t gmm_smem(int L, bool table) {
          (table ? phase_table_bytes(L, kGmmTabTiles) : 0);
 }
 
-__global__ void __launch_bounds__(kGmmThreads)
+// Four blocks of 128 threads per SM (128 registers): 13.34 ms on the 21-layer gather grid
+// against 13.47 at the compiler's 134 registers (three blocks) and 13.59 at five (96).
+__global__ void __launch_bounds__(kGmmThreads, 4)
 gmm_kernel(const double* __restrict__ tab, int L, const double* __restrict__ p, int n_p,
            const double2* __restrict__ omega, int n_w, int n_wtiles, int tiles_per_block,
            int free_surface, int use_table, double2* __restrict__ R) {
