@@ -567,8 +567,14 @@ template <int THREADS>
 static kr_status grids(PlanHeader& h, int max_layers, int tab_entries, size_t* fsm,
                        size_t* gsm, int* stage, int* gtab, bool* sums) {
   const int lt = std::min(max_layers, phase_table_max_layers());
-  *fsm = fwd_smem(max_layers) +
-         (tab_entries ? sizeof(cd) * (size_t)tab_entries * 2 * (size_t)(lt - 1) : 0);
+  // a model's table sits right after its own layer terms and coefficients, so the block needs
+  // the larger of the deepest model's prologue and the deepest tabulating model's prologue
+  // plus table (not their sum: 51 instead of 66 KB for 64- and 30-layer models, four blocks
+  // per SM instead of three)
+  *fsm = std::max(fwd_smem(max_layers),
+                  fwd_smem(lt) + (tab_entries ? sizeof(cd) * (size_t)tab_entries * 2 *
+                                                    (size_t)(lt - 1)
+                                              : 0));
   int stab = 0;
   const size_t ssm = batch_sums_enabled() ? sums_smem(THREADS, max_layers, tab_entries, &stab) : 0;
   *sums = ssm > 0;
