@@ -5,6 +5,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "../../include/kennett_b200.h"
 #include "kr_math.cuh"
 
@@ -36,6 +38,15 @@ constexpr int kMaxDevices = 64;
 struct SmemLimit {
   int bytes[kMaxDevices];
 };
+// One lock for every kernel's limit: host threads that launch concurrently (two servers, a
+// server and a direct call) must not interleave the check, the attribute call and the
+// record, or one could lower a limit another thread's launch relies on.  Under the lock a
+// limit only ever rises.
+inline std::mutex& smem_limit_mutex() {
+  static std::mutex m;
+  return m;
+}
+
 inline kr_status raise_smem_limit(const void* fn, size_t bytes, SmemLimit& lim,
                                   const char* where) {
   int dev = -1;
@@ -45,6 +56,7 @@ inline kr_status raise_smem_limit(const void* fn, size_t bytes, SmemLimit& lim,
     return KR_ERR_CUDA;
   }
   const bool known = dev >= 0 && dev < kMaxDevices;
+  std::lock_guard<std::mutex> g(smem_limit_mutex());
   if (known && lim.bytes[dev] >= (int)bytes) return KR_OK;
   e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   if (e != cudaSuccess) {
