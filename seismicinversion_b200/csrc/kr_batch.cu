@@ -143,15 +143,15 @@ __device__ __forceinline__ int next_item(int* counter) {
 }
 
 // Forward items: one (model, slowness) pair and a frequency range [w0, w0 + nw).  With
-// tab_entries > 0 the block tabulates the phase factors of the 128-frequency tiles the range
-// touches (kr_phase.cuh; same tiles and verdicts as kr_reflectivity, so the results are
-// bit-identical to a per-model call).
+// tab_entries > 0 (kPhHead + 2: lo, mid and two hi slots) models that tabulate take their
+// phase factors from a table holding one tile's hi entry at a time (kr_phase.cuh; same
+// entries and verdicts as kr_reflectivity, so the results are bit-identical to a per-model
+// call): ~37 KB of shared memory for the deepest such model, six blocks per SM.
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS)
 batch_forward_kernel(unsigned char* plan, const double2* __restrict__ omega_all,
                      double2* __restrict__ R_all, int tab_entries) {
   extern __shared__ __align__(16) unsigned char s_pair[];  // layer terms + coefficients + table
-  __shared__ unsigned s_bad;
   PlanHeader* h = reinterpret_cast<PlanHeader*>(plan);
   const kr_model_desc* models = reinterpret_cast<const kr_model_desc*>(plan + h->off_models);
   const PairRec* pairs = reinterpret_cast<const PairRec*>(plan + h->off_pairs);
@@ -172,23 +172,29 @@ batch_forward_kernel(unsigned char* plan, const double2* __restrict__ omega_all,
     copy16(coef, v.coef, sizeof(Iface) * (d.n_layers - 1));
     __syncthreads();
     const double2* om = omega_all + d.omega_off;
-    const int u0 = item.w0 / kPhTile;
-    unsigned mask = 0u;
-    if (tab_entries > 0 && phase_table_model(d.n_layers))
-      mask = build_phase_table(om, d.n_w, grid_line(om, d.n_w), u0,
-                               (item.w0 + item.nw - 1) / kPhTile - u0 + 1, tab_entries,
-                               d.n_layers, lay, s_ph, &s_bad);
-    for (int k = threadIdx.x; k < item.nw; k += THREADS) {
-      const int iw = item.w0 + k;
-      cd e0, rpp;
-      if ((mask >> (iw / kPhTile - u0)) & 1u) {
-        rpp = sweep_ph(d.n_layers, coef, phase_at(s_ph, tab_entries, iw, u0), &e0);
-      } else {
-        const double2 wv = om[iw];
-        rpp = sweep(mk(wv.x, wv.y), d.n_layers, lay, coef, &e0);
+    const GridLine g = grid_line(om, d.n_w);
+    // block-uniform conditions: every thread takes the same branches through the barriers
+    const bool tab = tab_entries > 0 && phase_table_model(d.n_layers);
+    const bool lomid = tab && build_phase_lomid(g, tab_entries, d.n_layers, lay, s_ph);
+    const int u_end = (item.w0 + item.nw - 1) / kPhTile;
+    for (int u = item.w0 / kPhTile; u <= u_end; ++u) {
+      // tile u's hi entry goes to slot u & 1, last read by tile u - 2, whose readers passed
+      // the barrier inside phase_hi_tile for tile u - 1
+      const bool tile_tab =
+          lomid && phase_hi_tile(om, d.n_w, g, u, u & 1, tab_entries, d.n_layers, lay, s_ph);
+      const int k_lo = max(item.w0, u * kPhTile);
+      const int k_hi = min(item.w0 + item.nw, (u + 1) * kPhTile);
+      for (int iw = k_lo + threadIdx.x; iw < k_hi; iw += THREADS) {
+        cd e0, rpp;
+        if (tile_tab) {
+          rpp = sweep_ph(d.n_layers, coef, phase_at(s_ph, tab_entries, iw, u - (u & 1)), &e0);
+        } else {
+          const double2 wv = om[iw];
+          rpp = sweep(mk(wv.x, wv.y), d.n_layers, lay, coef, &e0);
+        }
+        const cd out = pp_surface(rpp, e0, fs);
+        R_all[d.R_off + (size_t)pr.j * d.n_w + iw] = make_double2(out.x, out.y);
       }
-      const cd out = pp_surface(rpp, e0, fs);
-      R_all[d.R_off + (size_t)pr.j * d.n_w + iw] = make_double2(out.x, out.y);
     }
   }
 }
@@ -564,7 +570,7 @@ static bool batch_sums_enabled() {
 }
 
 template <int THREADS>
-static kr_status grids(PlanHeader& h, int max_layers, int tab_entries, size_t* fsm,
+static kr_status grids(PlanHeader& h, int max_layers, int tab_entries, int ftab, size_t* fsm,
                        size_t* gsm, int* stage, int* gtab, bool* sums) {
   const int lt = std::min(max_layers, phase_table_max_layers());
   // a model's table sits right after its own layer terms and coefficients, so the block needs
@@ -572,9 +578,7 @@ static kr_status grids(PlanHeader& h, int max_layers, int tab_entries, size_t* f
   // plus table (not their sum: 51 instead of 66 KB for 64- and 30-layer models, four blocks
   // per SM instead of three)
   *fsm = std::max(fwd_smem(max_layers),
-                  fwd_smem(lt) + (tab_entries ? sizeof(cd) * (size_t)tab_entries * 2 *
-                                                    (size_t)(lt - 1)
-                                              : 0));
+                  fwd_smem(lt) + (ftab ? sizeof(cd) * (size_t)ftab * 2 * (size_t)(lt - 1) : 0));
   int stab = 0;
   const size_t ssm = batch_sums_enabled() ? sums_smem(THREADS, max_layers, tab_entries, &stab) : 0;
   *sums = ssm > 0;
@@ -585,15 +589,16 @@ static kr_status grids(PlanHeader& h, int max_layers, int tab_entries, size_t* f
   } else {
     *gsm = grad_smem(THREADS, max_layers, tab_entries, stage, gtab);
   }
-  if (*fsm > 48 * 1024 &&
-      cudaFuncSetAttribute(batch_forward_kernel<THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)*fsm) != cudaSuccess)
+  // limits only ever rise (raise_smem_limit), so batches of different shapes launched from
+  // several host threads at once never find a kernel's limit lowered under them
+  static SmemLimit flim, slim, glim;
+  if (*fsm > 48 * 1024 && raise_smem_limit((const void*)batch_forward_kernel<THREADS>, *fsm, flim,
+                                           "kr_batch_launch: forward smem") != KR_OK)
     return KR_ERR_CUDA;
   const void* gk = *sums ? (const void*)batch_grad_sums_kernel<THREADS>
                         : (const void*)batch_gradient_kernel<THREADS>;
-  if (*gsm > 48 * 1024 &&
-      cudaFuncSetAttribute(gk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*gsm) !=
-          cudaSuccess)
+  if (*gsm > 48 * 1024 && raise_smem_limit(gk, *gsm, *sums ? slim : glim,
+                                           "kr_batch_launch: gradient smem") != KR_OK)
     return KR_ERR_CUDA;
   h.grid_fwd = occupancy_grid((const void*)batch_forward_kernel<THREADS>, THREADS, *fsm);
   h.grid_grad = occupancy_grid(gk, THREADS, *gsm);
@@ -692,9 +697,11 @@ static kr_status launch_batch(unsigned char* pl, const kr_batch_config* cfg, int
   size_t fsm = 0, gsm = 0;
   int stage = 0;
   const int tab = fwd_table_entries(cfg->tile_w);
+  // the forward kernel holds lo / mid and two tiles' hi entries per phase (kPhHead + 2)
+  const int ftab = kPhHead + 2;
   int gtab = 0;
   bool sums = false;
-  kr_status s = grids<THREADS>(h, max_layers, tab, &fsm, &gsm, &stage, &gtab, &sums);
+  kr_status s = grids<THREADS>(h, max_layers, tab, ftab, &fsm, &gsm, &stage, &gtab, &sums);
   if (s != KR_OK) {
     set_last_error_msg("kr_batch_launch: shared-memory attribute");
     return s;
@@ -707,7 +714,7 @@ static kr_status launch_batch(unsigned char* pl, const kr_batch_config* cfg, int
   if (s != KR_OK) return s;
   const double2* w = reinterpret_cast<const double2*>(omega);
   batch_forward_kernel<THREADS><<<h.grid_fwd, THREADS, fsm, st>>>(
-      pl, w, reinterpret_cast<double2*>(R), tab);
+      pl, w, reinterpret_cast<double2*>(R), ftab);
   s = check_launch("kr_batch_launch: forward");
   if (s != KR_OK) return s;
   if (sums)

@@ -170,4 +170,51 @@ __device__ inline unsigned build_phase_table(const double2* __restrict__ omega, 
   return (b >> 31) ? 0u : ~b;
 }
 
+// The same table built in two block-cooperative pieces, for kernels that hold the hi entries
+// of one or two tiles at a time (kPhHead + slots entries per phase): build_phase_lomid fills
+// the lo and mid entries of every phase and returns whether all of them are usable;
+// phase_hi_tile fills tile u's hi entry in hi slot `slot` and returns whether tile u uses
+// the table.  Every entry and every verdict is formed exactly as build_phase_table forms it,
+// so the phase factors are bit-identical to it.  Each contains a block barrier and reads
+// omega / lay only; all threads must call them.
+__device__ inline bool build_phase_lomid(const GridLine& g, int entries, int n_layers,
+                                         const LayerP* lay, cd* s_ph) {
+  bool bad = false;
+  const int n_phase = 2 * (n_layers - 1);
+  for (int e = threadIdx.x; e < n_phase * kPhHead; e += blockDim.x) {
+    const int id = e / kPhHead, j = e - id * kPhHead;
+    const LayerP& lp = lay[id >> 1];
+    const cd c = (id & 1) ? lp.cb : lp.ca;
+    const cd z = j < kPhLo ? (double)j * g.d : (double)((j - kPhLo) * kPhLo) * g.d;
+    const cd v = cexp_(z * c);
+    if (!(fabs(v.x) <= kPhMaxMag && fabs(v.y) <= kPhMaxMag)) bad = true;
+    s_ph[id * entries + j] = v;
+  }
+  return __syncthreads_or(bad) == 0;
+}
+
+__device__ inline bool phase_hi_tile(const double2* __restrict__ omega, int n_w,
+                                     const GridLine& g, int u, int slot, int entries,
+                                     int n_layers, const LayerP* lay, cd* s_ph) {
+  bool bad = false;
+  const int k_end = min(n_w, (u + 1) * kPhTile);
+  for (int k = u * kPhTile + threadIdx.x; k < k_end; k += blockDim.x) {
+    const double2 w = omega[k];
+    const double m = (double)k;
+    const bool ok = fabs(w.x - fma(m, g.d.x, g.w0.x)) <= g.tol &&
+                    fabs(w.y - fma(m, g.d.y, g.w0.y)) <= g.tol;
+    if (!ok) bad = true;
+  }
+  const int n_phase = 2 * (n_layers - 1);
+  const double2 ws = omega[u * kPhTile];
+  for (int id = threadIdx.x; id < n_phase; id += blockDim.x) {
+    const LayerP& lp = lay[id >> 1];
+    const cd c = (id & 1) ? lp.cb : lp.ca;
+    const cd v = cexp_(mk(ws.x, ws.y) * c);
+    if (!(fabs(v.x) <= kPhMaxMag && fabs(v.y) <= kPhMaxMag)) bad = true;
+    s_ph[id * entries + kPhHead + slot] = v;
+  }
+  return __syncthreads_or(bad) == 0;
+}
+
 }  // namespace kr
