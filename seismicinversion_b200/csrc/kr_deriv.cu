@@ -4,7 +4,10 @@
 // Kernels (stream-ordered, no host synchronisation):
 //   deriv_prep_kernel  : per (p, interface, tangent column or coefficients): layer terms and
 //                        derivative factors, interface coefficients and their 10 x 6 tangents
-//                        -> workspace
+//                        -> workspace (JAC, and GRAD / VJP on the per-step path)
+//   deriv_coef_kernel, deriv_tan_kernel : the same in two kernels for the frequency-sum sweep,
+//                        which is launched as the tangent kernel's programmatic dependent and
+//                        waits for the tangents only before its contraction
 //   deriv_sum_kernel   : GRAD / VJP, per (omega, p): forward sweep with a tape of up to 64
 //                        steps (deeper models checkpoint and recompute segments), seed
 //                        2 conj(R - R_obs) (GRAD) or conj(gR) (VJP), reverse sweep; the per-step
@@ -109,6 +112,51 @@ deriv_prep_kernel(const double* __restrict__ tab, int L, const double* __restric
   cd c[10];
   interface_tangent_col(pj, i, up, s_ld[i - l0], lo, s_ld[i + 1 - l0], item, c);
   for (int k = 0; k < 10; ++k) tan[idx].t[k][item] = c[k];
+}
+
+// The same preparation in two kernels, for the frequency-sum sweep, which needs the
+// coefficients from its first step but the tangents only in its final contraction:
+// deriv_coef_kernel (block per slowness and chunk of kPrepThreads interfaces: layer terms
+// staged in shared memory, then one thread per interface for the coefficients, exactly as in
+// deriv_prep_kernel) and deriv_tan_kernel (one thread per (slowness, interface, tangent
+// column), from the layer terms deriv_coef_kernel wrote), which lets the sweep launch at once
+// (griddepcontrol.launch_dependents) so that the tangents overlap the sweep.
+__global__ void __launch_bounds__(kPrepThreads)
+deriv_coef_kernel(const double* __restrict__ tab, int L, const double* __restrict__ p,
+                  int n_chunks, LayerP* lay, LayerD* dlay, Iface* coef) {
+  __shared__ LayerP s_lp[kPrepThreads + 1];
+  const int I = L - 1;
+  const int j = blockIdx.x / n_chunks;
+  const int i0 = (blockIdx.x % n_chunks) * kPrepThreads;
+  const int i1 = min(i0 + kPrepThreads, I);  // the chunk's interfaces [i0, i1), layers i0 .. i1
+  const double pj = p[j];
+  for (int l = i0 + threadIdx.x; l <= i1; l += blockDim.x) {
+    const LayerP lp = layer_terms(tab, L, l, pj);
+    s_lp[l - i0] = lp;
+    if (l < i1 || i1 == I) {  // each layer written by one block
+      lay[(size_t)j * L + l] = lp;
+      dlay[(size_t)j * L + l] = layer_derivs(tab, L, l, pj, lp);
+    }
+  }
+  __syncthreads();
+  const int i = i0 + threadIdx.x;
+  if (i < i1) coef[(size_t)j * I + i] = interface_coeffs(pj, i, s_lp[i - i0], s_lp[i + 1 - i0]);
+}
+
+__global__ void __launch_bounds__(kPrepThreads)
+deriv_tan_kernel(const double* __restrict__ p, int n_p, int L, const LayerP* __restrict__ lay,
+                 const LayerD* __restrict__ dlay, ScatTan* tan) {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  const int I = L - 1;
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)n_p * I * 6) return;
+  const int col = (int)(t % 6);
+  const size_t idx = t / 6;
+  const int j = (int)(idx / I), i = (int)(idx % I);
+  const size_t e = (size_t)j * L + i;
+  cd c[10];
+  interface_tangent_col(p[j], i, lay[e], dlay[e], lay[e + 1], dlay[e + 1], col, c);
+  for (int k = 0; k < 10; ++k) tan[idx].t[k][col] = c[k];
 }
 
 // Jacobian mode: writes dR/dtheta of layer l.
@@ -344,6 +392,10 @@ deriv_sum_kernel(int L, int n_p, const double2* __restrict__ omega, int n_w, int
   for (int o = 16; o > 0; o >>= 1) c2 += __shfl_down_sync(0xffffffffu, c2, o);
   if ((threadIdx.x & 31) == 0) s_chi[warp] = c2;
   double* dst = partial + (size_t)blockIdx.x * (4 * L + 1);
+  // the tangents may still be in the making (deriv_tan_kernel, launched ahead of this kernel
+  // as its programmatic prerequisite): wait for that grid's completion and its writes; a
+  // no-op when the kernel was launched without the dependency
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   sums_finish(acc, L, W, tan_all + (size_t)ip * I, dlay_all + (size_t)ip * L, dst);
   if (threadIdx.x == 0) {
     double t = 0.0;
@@ -434,9 +486,25 @@ static kr_status launch_sum_v(unsigned blocks, size_t smem, cudaStream_t st, int
                                          "kr_deriv: smem attribute");
     if (a != KR_OK) return a;
   }
-  deriv_sum_kernel<MINB><<<blocks, kDerThreads, smem, st>>>(L, n_p, omega, n_w, n_wtiles, fs, vjp,
-                                                            seg, table, lay, dlay, coef, tan, obs,
-                                                            R, partial);
+  // programmatic dependent launch: the sweep may start while the tangent kernel ahead of it
+  // on the stream still runs; it waits for it (griddepcontrol.wait) only before contracting
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(kDerThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, deriv_sum_kernel<MINB>, L, n_p, omega, n_w,
+                                           n_wtiles, fs, vjp, seg, table, lay, dlay, coef, tan,
+                                           obs, R, partial);
+  if (e != cudaSuccess) {
+    set_last_error("kr_deriv: sweep launch", e);
+    return KR_ERR_CUDA;
+  }
   return KR_OK;
 }
 
@@ -452,35 +520,50 @@ static kr_status launch_deriv(const double* layers, int L, const double* p, int 
   DerivWs w = deriv_ws(ws, L, n_p, GRAD ? n_blocks : 0);
   if (!ws || ws_bytes < w.bytes) return KR_ERR_WORKSPACE;
   const int I = L - 1;
-  const int n_chunks = (kPrepItems * I + kPrepThreads - 1) / kPrepThreads;
-  if ((size_t)n_p * n_chunks > 0x7fffffffULL) return KR_ERR_TOO_LARGE;
-  deriv_prep_kernel<<<(unsigned)(n_p * n_chunks), kPrepThreads, 0, st>>>(
-      layers, L, p, n_chunks, w.lay, w.dlay, w.coef, w.tan);
-  kr_status s = check_launch("kr_deriv: layers and interfaces");
-  if (s != KR_OK) return s;
   const int seg = checkpoint_spacing(I - 1 > 0 ? I - 1 : 1);
-  if (GRAD && deriv_sums_enabled()) {
-    const int table = phase_table_model(L) ? 1 : 0;
-    const size_t smem = sum_kernel_smem(L, table);
-    if (smem) {
-      const int fs = (flags & KR_FREE_SURFACE) ? 1 : 0;
-      const int vjp = MODE == kModeVjp ? 1 : 0;
-      const double2* o = reinterpret_cast<const double2*>(R_obs);
-      const double2* w2 = reinterpret_cast<const double2*>(omega);
-      double2* R2 = reinterpret_cast<double2*>(R);
-      s = sum_minb() == 3
-              ? launch_sum_v<3>((unsigned)n_blocks, smem, st, L, n_p, w2, n_w, n_wtiles, fs, vjp,
-                                seg, table, w.lay, w.dlay, w.coef, w.tan, o, R2, w.partial)
-              : launch_sum_v<2>((unsigned)n_blocks, smem, st, L, n_p, w2, n_w, n_wtiles, fs, vjp,
-                                seg, table, w.lay, w.dlay, w.coef, w.tan, o, R2, w.partial);
-      if (s != KR_OK) return s;
-      s = check_launch("kr_deriv: sweep");
-      if (s != KR_OK) return s;
-      const int nv = 4 * L + 1;
-      reduce_partials_kernel<<<MODE == kModeGrad ? nv : nv - 1, 256, 0, st>>>(
-          w.partial, (int)n_blocks, nv, chi_grad);
-      return check_launch("kr_deriv: reduce");
-    }
+  const int sum_table = phase_table_model(L) ? 1 : 0;
+  const size_t sum_smem = (GRAD && deriv_sums_enabled()) ? sum_kernel_smem(L, sum_table) : 0;
+  kr_status s = KR_OK;
+  if (sum_smem) {
+    // coefficients first; the tangents then overlap the frequency-sum sweep
+    const int n_cc = (I + kPrepThreads - 1) / kPrepThreads;
+    const size_t n_tan = (size_t)n_p * I * 6;
+    if ((size_t)n_p * n_cc > 0x7fffffffULL || (n_tan + kPrepThreads - 1) / kPrepThreads > 0x7fffffffULL)
+      return KR_ERR_TOO_LARGE;
+    deriv_coef_kernel<<<(unsigned)(n_p * n_cc), kPrepThreads, 0, st>>>(layers, L, p, n_cc, w.lay,
+                                                                       w.dlay, w.coef);
+    s = check_launch("kr_deriv: layers and coefficients");
+    if (s != KR_OK) return s;
+    deriv_tan_kernel<<<(unsigned)((n_tan + kPrepThreads - 1) / kPrepThreads), kPrepThreads, 0,
+                       st>>>(p, n_p, L, w.lay, w.dlay, w.tan);
+    s = check_launch("kr_deriv: tangents");
+    if (s != KR_OK) return s;
+  } else {
+    const int n_chunks = (kPrepItems * I + kPrepThreads - 1) / kPrepThreads;
+    if ((size_t)n_p * n_chunks > 0x7fffffffULL) return KR_ERR_TOO_LARGE;
+    deriv_prep_kernel<<<(unsigned)(n_p * n_chunks), kPrepThreads, 0, st>>>(
+        layers, L, p, n_chunks, w.lay, w.dlay, w.coef, w.tan);
+    s = check_launch("kr_deriv: layers and interfaces");
+    if (s != KR_OK) return s;
+  }
+  if (sum_smem) {
+    const int fs = (flags & KR_FREE_SURFACE) ? 1 : 0;
+    const int vjp = MODE == kModeVjp ? 1 : 0;
+    const double2* o = reinterpret_cast<const double2*>(R_obs);
+    const double2* w2 = reinterpret_cast<const double2*>(omega);
+    double2* R2 = reinterpret_cast<double2*>(R);
+    s = sum_minb() == 3
+            ? launch_sum_v<3>((unsigned)n_blocks, sum_smem, st, L, n_p, w2, n_w, n_wtiles, fs,
+                              vjp, seg, sum_table, w.lay, w.dlay, w.coef, w.tan, o, R2, w.partial)
+            : launch_sum_v<2>((unsigned)n_blocks, sum_smem, st, L, n_p, w2, n_w, n_wtiles, fs,
+                              vjp, seg, sum_table, w.lay, w.dlay, w.coef, w.tan, o, R2, w.partial);
+    if (s != KR_OK) return s;
+    s = check_launch("kr_deriv: sweep");
+    if (s != KR_OK) return s;
+    const int nv = 4 * L + 1;
+    reduce_partials_kernel<<<MODE == kModeGrad ? nv : nv - 1, 256, 0, st>>>(
+        w.partial, (int)n_blocks, nv, chi_grad);
+    return check_launch("kr_deriv: reduce");
   }
   // accumulators: [warps][4L + 1] doubles, padded to 16 bytes
   const size_t acc = GRAD ? sizeof(double) * (((size_t)(kDerThreads / 32) * (4 * L + 1) + 1) / 2 * 2) : 0;
