@@ -11,9 +11,10 @@
 // and uploads them into the caller's plan buffer.  kr_batch_launch (device only, capturable
 // in a CUDA graph) then runs:
 //   1. batch_prep_kernel: one block per pair -> layer terms and interface coefficients (and,
-//      for gradient models, layer derivative factors and coefficient tangents, one thread per
-//      interface and tangent column) into the plan;
-//   2. batch_forward_kernel and batch_grad_sums_kernel (batch_gradient_kernel where a model's
+//      for gradient models, layer derivative factors) into the plan;
+//   2. batch_tan_kernel: the gradient models' coefficient tangents, one thread per interface
+//      and tangent column, alongside the forward kernel (its programmatic dependent);
+//   3. batch_forward_kernel and batch_grad_sums_kernel (batch_gradient_kernel where a model's
 //      frequency sums exceed shared memory): persistent grids (resident blocks only) that
 //      pull items with an atomic counter until the list is exhausted.
 // Gradient items reduce their contributions per block in a fixed order and add them to the
@@ -100,8 +101,6 @@ __global__ void batch_prep_kernel(unsigned char* plan, const double* __restrict_
     Iface* coef = reinterpret_cast<Iface*>(b);
     b += a256(sizeof(Iface) * I);
     LayerD* dlay = reinterpret_cast<LayerD*>(b);
-    b += a256(sizeof(LayerD) * L);
-    ScatTan* tan = reinterpret_cast<ScatTan*>(b);
     const bool grad = (d.flags & KR_BATCH_GRADIENT) != 0;
     for (int l = threadIdx.x; l < L; l += blockDim.x) {
       lay[l] = layer_terms(tab, L, l, pj);
@@ -110,15 +109,39 @@ __global__ void batch_prep_kernel(unsigned char* plan, const double* __restrict_
     __syncthreads();
     for (int i = threadIdx.x; i < I; i += blockDim.x)
       coef[i] = interface_coeffs(pj, i, lay[i], lay[i + 1]);
-    if (grad) {  // one thread per (interface, tangent column)
-      for (int t = threadIdx.x; t < 6 * I; t += blockDim.x) {
-        const int i = t / 6, col = t % 6;
-        cd c[10];
-        interface_tangent_col(pj, i, lay[i], dlay[i], lay[i + 1], dlay[i + 1], col, c);
-        for (int k = 0; k < 10; ++k) tan[i].t[k][col] = c[k];
-      }
-    }
     __syncthreads();
+  }
+}
+
+// Coefficient tangents of the gradient models' pairs, one thread per (interface, tangent
+// column), from the layer terms and derivative factors batch_prep_kernel left in the plan.
+// Only the gradient kernel reads them, so the forward kernel is launched as this kernel's
+// programmatic dependent (released on entry) and runs alongside it; the forward kernel
+// waits for this grid before it exits, so the gradient kernel after it sees the tangents.
+__global__ void __launch_bounds__(64)
+batch_tan_kernel(unsigned char* plan, const double* __restrict__ p_all) {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  const PlanHeader* h = reinterpret_cast<const PlanHeader*>(plan);
+  const kr_model_desc* models = reinterpret_cast<const kr_model_desc*>(plan + h->off_models);
+  const PairRec* pairs = reinterpret_cast<const PairRec*>(plan + h->off_pairs);
+  for (int q = blockIdx.x; q < h->n_pairs; q += gridDim.x) {
+    const PairRec pr = pairs[q];
+    const kr_model_desc d = models[pr.model];
+    if (!(d.flags & KR_BATCH_GRADIENT)) continue;
+    const int L = d.n_layers, I = L - 1;
+    const double pj = p_all[d.p_off + pr.j];
+    unsigned char* b = plan + pr.coef_off;
+    const LayerP* lay = reinterpret_cast<const LayerP*>(b);
+    b += a256(sizeof(LayerP) * L) + a256(sizeof(Iface) * I);
+    const LayerD* dlay = reinterpret_cast<const LayerD*>(b);
+    b += a256(sizeof(LayerD) * L);
+    ScatTan* tan = reinterpret_cast<ScatTan*>(b);
+    for (int t = threadIdx.x; t < 6 * I; t += blockDim.x) {
+      const int i = t / 6, col = t % 6;
+      cd c[10];
+      interface_tangent_col(pj, i, lay[i], dlay[i], lay[i + 1], dlay[i + 1], col, c);
+      for (int k = 0; k < 10; ++k) tan[i].t[k][col] = c[k];
+    }
   }
 }
 
@@ -197,6 +220,9 @@ batch_forward_kernel(unsigned char* plan, const double2* __restrict__ omega_all,
       }
     }
   }
+  // launched as batch_tan_kernel's programmatic dependent: this grid completes only after
+  // that one has, so the gradient kernel launched after it reads finished tangents
+  asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 // Per-thread sink for gradient items: 2 Re(conj(res) dR/dtheta) per layer, reduced over the
@@ -712,11 +738,30 @@ static kr_status launch_batch(unsigned char* pl, const kr_batch_config* cfg, int
   batch_prep_kernel<<<148 * 16, 64, 0, st>>>(pl, layers, p);
   s = check_launch("kr_batch_launch: prep");
   if (s != KR_OK) return s;
-  const double2* w = reinterpret_cast<const double2*>(omega);
-  batch_forward_kernel<THREADS><<<h.grid_fwd, THREADS, fsm, st>>>(
-      pl, w, reinterpret_cast<double2*>(R), ftab);
-  s = check_launch("kr_batch_launch: forward");
+  // tangents on a resident-sized grid (every block starts at once and releases the forward
+  // kernel), the forward kernel as its programmatic dependent
+  batch_tan_kernel<<<148 * 4, 64, 0, st>>>(pl, p);
+  s = check_launch("kr_batch_launch: tangents");
   if (s != KR_OK) return s;
+  const double2* w = reinterpret_cast<const double2*>(omega);
+  {
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(h.grid_fwd);
+    lc.blockDim = dim3(THREADS);
+    lc.dynamicSmemBytes = fsm;
+    lc.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&lc, batch_forward_kernel<THREADS>, pl, w,
+                                             reinterpret_cast<double2*>(R), ftab);
+    if (e != cudaSuccess) {
+      set_last_error("kr_batch_launch: forward", e);
+      return KR_ERR_CUDA;
+    }
+  }
   if (sums)
     batch_grad_sums_kernel<THREADS><<<h.grid_grad, THREADS, gsm, st>>>(
         pl, w, reinterpret_cast<const double2*>(R_obs), reinterpret_cast<double2*>(R), chi_grad,
