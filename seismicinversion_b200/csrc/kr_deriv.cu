@@ -322,6 +322,9 @@ deriv_sweep_kernel(int L, const double* __restrict__ p, int n_p,
 __global__ void __launch_bounds__(256)
 reduce_partials_kernel(const double* __restrict__ partial, int n_blocks, int stride,
                        double* __restrict__ out) {
+  // after the frequency-sum sweep this kernel is launched as the sweep's programmatic
+  // dependent: wait for that grid and its partials (a no-op after an ordinary launch)
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   __shared__ double s[256];
   const int k = blockIdx.x;
   double t = 0.0;
@@ -346,6 +349,8 @@ deriv_sum_kernel(int L, int n_p, const double2* __restrict__ omega, int n_w, int
                  const LayerD* __restrict__ dlay_all, const Iface* __restrict__ coef_all,
                  const ScatTan* __restrict__ tan_all, const double2* __restrict__ obs,
                  double2* __restrict__ R_out, double* __restrict__ partial) {
+  // the reduction after this kernel may launch as soon as every block of it has started
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   constexpr int W = kDerThreads / 32;
   extern __shared__ __align__(16) double s_raw[];
   __shared__ unsigned s_bad;
@@ -561,9 +566,22 @@ static kr_status launch_deriv(const double* layers, int L, const double* p, int 
     s = check_launch("kr_deriv: sweep");
     if (s != KR_OK) return s;
     const int nv = 4 * L + 1;
-    reduce_partials_kernel<<<MODE == kModeGrad ? nv : nv - 1, 256, 0, st>>>(
-        w.partial, (int)n_blocks, nv, chi_grad);
-    return check_launch("kr_deriv: reduce");
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(MODE == kModeGrad ? nv : nv - 1);
+    lc.blockDim = dim3(256);
+    lc.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&lc, reduce_partials_kernel,
+                                             (const double*)w.partial, (int)n_blocks, nv, chi_grad);
+    if (e != cudaSuccess) {
+      set_last_error("kr_deriv: reduce launch", e);
+      return KR_ERR_CUDA;
+    }
+    return KR_OK;
   }
   // accumulators: [warps][4L + 1] doubles, padded to 16 bytes
   const size_t acc = GRAD ? sizeof(double) * (((size_t)(kDerThreads / 32) * (4 * L + 1) + 1) / 2 * 2) : 0;
