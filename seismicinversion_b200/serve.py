@@ -11,8 +11,8 @@ gradient requests the observed R) from any thread; each returns a ``Request`` wh
 * launches each admitted group as one persistent batched launch (``ModelBatch``) on one of
   ``n_streams`` streams, keeping up to ``max_inflight`` batches on the GPU at once, so
   requests that arrive while others run are batched into the next launch and their work
-  overlaps on the device; a group of one request (a lightly loaded server) runs the
-  single-model kernels instead, which skip the batch plan's host-side build;
+  overlaps on the device; a group of up to four requests (a lightly or moderately loaded
+  server) runs the single-model kernels instead, which skip the batch machinery;
 * polls completion events and marks requests done.  Results stay on the device as tensors
   (views of the batch's single device block), so the budget keeps a batch's bytes charged
   until every request of that batch has released its results: ``Request.release()``, or
@@ -169,13 +169,13 @@ class _Record:
 class GpuBatchExecutor:
     """Runs an admitted group as one ModelBatch launch on a stream; ``ready`` polls its event.
 
-    Groups of at most ``direct_max_requests`` requests (default 1) run the single-model
+    Groups of at most ``direct_max_requests`` requests (default 4) run the single-model
     entry points (``kr_reflectivity``, ``kr_misfit_gradient`` with R) on the stream instead:
     the same R bit for bit, the gradient to rounding (the batch adds per-block partials in
     another order), without the plan build."""
 
     def __init__(self, device=None, n_streams: int = 2, schedule=(128, 256),
-                 direct_max_requests: int = 1):
+                 direct_max_requests: int = 4):
         import torch
 
         from . import device as D

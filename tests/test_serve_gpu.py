@@ -82,3 +82,27 @@ def test_single_request_group_runs_the_single_model_kernels():
     assert g1 and torch.equal(res["grad"], out[:4 * L]) and torch.equal(res["R"], R)
     assert float(res["chi"]) == float(out[4 * L])
     assert torch.equal(fwd["R"], D.reflectivity(D.layer_table(m), p, w))
+
+
+def test_small_groups_run_the_single_model_kernels():
+    """A group of up to four requests (the default threshold) runs each request through the
+    single-model entry points, one after another on the group's stream: no batch plan, and
+    every result equals the direct call bit for bit."""
+    from seismicinversion_b200 import device as D
+    from seismicinversion_b200.serve import GpuBatchExecutor, Request
+
+    reqs = [Request(m, np.asarray(p, dtype=np.float64), np.asarray(w, dtype=np.complex128), g, o)
+            for (m, p, w, g, o) in _requests(4, seed=11)]
+    ex = GpuBatchExecutor(n_streams=1)
+    handle = ex.launch(reqs)
+    handle[1].synchronize()
+    assert handle[0] is None  # no ModelBatch was built
+    res = ex.results(handle, reqs)
+    for r, x in zip(reqs, res):
+        tab = D.layer_table(r.model)
+        if r.gradient:
+            out, R = D.misfit_gradient(tab, r.p, r.omega, r.R_obs, want_R=True)
+            L = r.model.n_layers
+            assert torch.equal(x["grad"], out[:4 * L]) and torch.equal(x["R"], R)
+        else:
+            assert torch.equal(x["R"], D.reflectivity(tab, r.p, r.omega))
