@@ -455,6 +455,7 @@ KR_HD void hvp_pair(int L, cd w, bool free_surface, const LayerV* lv, const IfS<
   const DC W = dc(w);
   SymS<DC> cp[kHvpCp];
   SymS<DC> sg[kHvpSeg];
+  DC sea[kHvpSeg], seb[kHvpSeg];  // the steps' phase factors, kept for the reverse sweep
   SymS<DC> r;
   r.a = ifs[I - 1].rd11;
   r.b = ifs[I - 1].rd12;
@@ -463,7 +464,12 @@ KR_HD void hvp_pair(int L, cd w, bool free_surface, const LayerV* lv, const IfS<
     if (s % seg == 0) cp[s / seg] = r;
     const int i = I - 2 - s;
     const DC ea = cexp_(W * lv[i + 1].ca), eb = cexp_(W * lv[i + 1].cb);
-    if (s >= (ncp - 1) * seg) sg[s - (ncp - 1) * seg] = r;
+    if (s >= (ncp - 1) * seg) {
+      const int k = s - (ncp - 1) * seg;
+      sg[k] = r;
+      sea[k] = ea;
+      seb[k] = eb;
+    }
     r = step_s(r, ea, eb, ifs[i]);
   }
   const DC e0 = cexp_(W * lv[0].ca);
@@ -494,13 +500,16 @@ KR_HD void hvp_pair(int L, cd w, bool free_surface, const LayerV* lv, const IfS<
       SymS<DC> x = cp[q];
       for (int s = s0; s < s1; ++s) {
         const int i = I - 2 - s;
+        const DC ea = cexp_(W * lv[i + 1].ca), eb = cexp_(W * lv[i + 1].cb);
         sg[s - s0] = x;
-        if (s + 1 < s1) x = step_s(x, cexp_(W * lv[i + 1].ca), cexp_(W * lv[i + 1].cb), ifs[i]);
+        sea[s - s0] = ea;
+        seb[s - s0] = eb;
+        if (s + 1 < s1) x = step_s(x, ea, eb, ifs[i]);
       }
     }
     for (int s = s1 - 1; s >= s0; --s) {
       const int i = I - 2 - s;
-      const DC ea = cexp_(W * lv[i + 1].ca), eb = cexp_(W * lv[i + 1].cb);
+      const DC ea = sea[s - s0], eb = seb[s - s0];
       SymS<DC> rb;
       DC eab, ebb, cbar[10];
       step_reverse_s(sg[s - s0], ea, eb, ifs[i], ob, rb, eab, ebb, cbar);
