@@ -271,6 +271,9 @@ KR_HD void jacobian_pair(int L, cd w, bool free_surface, int seg, const LayerP* 
   S3 cp[kCpMax];
   S3 sg[kSegMax];
   cd sea[kSegMax], seb[kSegMax];
+  // tabulated phase factors are recomputed in the reverse sweep (two products each) instead of
+  // kept on the tape, as in adjoint_pair_sums
+  const bool keep_ph = !ph.cheap();
   M2 r = m2(coef[I - 1].rd11, coef[I - 1].rd12, coef[I - 1].rd12, coef[I - 1].rd22);
   for (int s = 0; s < nsteps; ++s) {
     if (s % seg == 0) cp[s / seg] = s3(r);
@@ -278,8 +281,10 @@ KR_HD void jacobian_pair(int L, cd w, bool free_surface, int seg, const LayerP* 
     const cd ea = ph.a(i + 1), eb = ph.b(i + 1);
     if (s >= top0) {  // the top segment is recorded now and never recomputed
       sg[s - top0] = s3(r);
-      sea[s - top0] = ea;
-      seb[s - top0] = eb;
+      if (keep_ph) {
+        sea[s - top0] = ea;
+        seb[s - top0] = eb;
+      }
     }
     r = kennett_step(r, ea, eb, coef[i]);
   }
@@ -314,14 +319,17 @@ KR_HD void jacobian_pair(int L, cd w, bool free_surface, int seg, const LayerP* 
         const int i = I - 2 - s;
         const cd ea = ph.a(i + 1), eb = ph.b(i + 1);
         sg[s - s0] = s3(x);
-        sea[s - s0] = ea;
-        seb[s - s0] = eb;
+        if (keep_ph) {
+          sea[s - s0] = ea;
+          seb[s - s0] = eb;
+        }
         if (s + 1 < s1) x = kennett_step(x, ea, eb, coef[i]);
       }
     }
     for (int s = s1 - 1; s >= s0; --s) {
       const int i = I - 2 - s;  // interface i, lower layer i + 1
-      const cd ea = sea[s - s0], eb = seb[s - s0];
+      const cd ea = keep_ph ? sea[s - s0] : ph.a(i + 1);
+      const cd eb = keep_ph ? seb[s - s0] : ph.b(i + 1);
       M2 rb;
       cd eab, ebb, cbar[10];
       kennett_step_reverse(m2(sg[s - s0]), ea, eb, coef[i], ob, rb, eab, ebb, cbar);
