@@ -99,7 +99,7 @@ __device__ __forceinline__ double j0_table(const double* s_j0, double x) {
 // Slowness steps between exact sincos anchors when p is an arithmetic progression.
 constexpr int kRotSteps = 32;
 // Slownesses staged per shared-memory chunk: (p_j, pw_j dp) and (1 / p_j, pw_j dp / sqrt p_j).
-constexpr int kChunk = 256;
+constexpr int kChunk = 128;
 
 // R rows are staged through shared memory in tiles of kSub slownesses x 32 frequencies
 // (16 KB) in a ring of three with cp.async: the 8 offset warps of a block read each R
@@ -181,10 +181,12 @@ __device__ __forceinline__ void fast_tile(const double2* s_pf, const double2* s_
 // progression (to 4.5 ulp); inside such a chunk cos / sin of x_j = (omega p_j) r advance by
 // one rotation per slowness, with an exact sincos anchor every kRotSteps.  R arrives in
 // tiles through a ring of three buffers (stage_R).  omega is factored out of the weight:
-// U = omega * sum_j J0(x_j) (pw_j dp) R_j.  Three blocks of 256 threads per SM (80 registers,
-// 16 bytes of spills): 24 warps hide the per-term dependency chains and the tile barriers
-// better than 16 at 124 registers (2.74 vs 2.98 ms on the 21-layer gather grid, same U).
-__global__ void __launch_bounds__(kBsW * kBsR, 3)
+// U = omega * sum_j J0(x_j) (pw_j dp) R_j.  Four blocks of 256 threads per SM (64 registers,
+// 72 bytes of spills; 128-slowness chunks keep four blocks' shared memory within the SM's
+// 228 KB): the kernel is bound by each warp's dependency chains, so more resident warps
+// help despite the spills (21-layer gather grid: 2.98 ms at two blocks and 124 registers,
+// 2.65 at three and 80, 2.635 at four, U bit-identical).
+__global__ void __launch_bounds__(kBsW * kBsR, 4)
 bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ p,
                       const double* __restrict__ pw, int n_p, double dp,
                       const double* __restrict__ omega, int n_w,
@@ -321,7 +323,7 @@ __global__ void reduce_slices_kernel(const double2* __restrict__ partial, int n_
 }
 
 // The R ring lives in dynamic shared memory above the 48 KB default (with the static arrays
-// ~59 KB per block, three blocks per SM); the limit is raised once per device.
+// ~56 KB per block, four blocks per SM); the limit is raised once per device.
 static SmemLimit g_ring_limit;
 static kr_status bessel_ring_attribute(const char* where) {
   return raise_smem_limit((const void*)bessel_partial_kernel, kRingBytes, g_ring_limit, where);
@@ -336,7 +338,7 @@ struct BesselPlan {
 static BesselPlan bessel_plan(int n_p, int n_w, int n_r) {
   BesselPlan b;
   const long long tiles = (long long)((n_w + kBsW - 1) / kBsW) * ((n_r + kBsR - 1) / kBsR);
-  // About 64 blocks of 256 threads per SM in total (~21 waves at 3 resident blocks per SM:
+  // About 64 blocks of 256 threads per SM in total (~16 waves at 4 resident blocks per SM:
   // shorter blocks even out the slow low-frequency tiles; 2.65 ms on the 21-layer gather
   // grid against 2.73 at 32 and 2.85 at 16, flat up to 128), but no slice shorter than 64
   // slownesses.
