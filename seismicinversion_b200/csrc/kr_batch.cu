@@ -168,7 +168,7 @@ __device__ __forceinline__ int next_item(int* counter) {
 // Forward items: one (model, slowness) pair and a frequency range [w0, w0 + nw).  With
 // tab_entries > 0 (kPhHead + 2: lo, mid and two hi slots) models that tabulate take their
 // phase factors from a table holding one tile's hi entry at a time (kr_phase.cuh; same
-// entries and verdicts as kr_reflectivity, so the results are bit-identical to a per-model
+// entries and decisions as kr_reflectivity, so the results are bit-identical to a per-model
 // call): ~37 KB of shared memory for the deepest such model, six blocks per SM.
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS)

@@ -12,7 +12,7 @@
 // each entry one direct exp of an exactly formed argument: two complex products and three
 // shared-memory reads replace an exp and a sincos per layer, phase and frequency.  A tile
 // whose frequencies leave the line, or whose entries exceed 1e100 in magnitude (so that no
-// product can overflow), evaluates its phases directly.  The per-tile verdict depends only
+// product can overflow), evaluates its phases directly.  The per-tile decision depends only
 // on the grid, so every kernel that uses this table gives bit-identical results.
 #pragma once
 
@@ -174,7 +174,7 @@ __device__ inline unsigned build_phase_table(const double2* __restrict__ omega, 
 // of one or two tiles at a time (kPhHead + slots entries per phase): build_phase_lomid fills
 // the lo and mid entries of every phase and returns whether all of them are usable;
 // phase_hi_tile fills tile u's hi entry in hi slot `slot` and returns whether tile u uses
-// the table.  Every entry and every verdict is formed exactly as build_phase_table forms it,
+// the table.  Every entry and every decision is formed exactly as build_phase_table forms it,
 // so the phase factors are bit-identical to it.  Each contains a block barrier and reads
 // omega / lay only; all threads must call them.
 __device__ inline bool build_phase_lomid(const GridLine& g, int entries, int n_layers,

@@ -44,7 +44,7 @@ def _check(batch, items):
         tab = D.layer_table(it.model)
         R1 = D.reflectivity(tab, it.p, it.omega, it.free_surface)
         if not it.gradient:
-            # same phase tiles and verdicts as the per-model forward kernel: identical bits
+            # same phase tiles and decisions as the per-model forward kernel: identical bits
             assert torch.equal(batch.reflectivity(b), R1), b
         if it.gradient:
             out, Rg = D.misfit_gradient(tab, it.p, it.omega, it.R_obs, it.free_surface,
