@@ -338,11 +338,11 @@ struct BesselPlan {
 static BesselPlan bessel_plan(int n_p, int n_w, int n_r) {
   BesselPlan b;
   const long long tiles = (long long)((n_w + kBsW - 1) / kBsW) * ((n_r + kBsR - 1) / kBsR);
-  // About 64 blocks of 256 threads per SM in total (~16 waves at 4 resident blocks per SM:
-  // shorter blocks even out the slow low-frequency tiles; 2.65 ms on the 21-layer gather
-  // grid against 2.73 at 32 and 2.85 at 16, flat up to 128), but no slice shorter than 64
-  // slownesses.
-  const long long target = 148LL * 64;
+  // About 96 blocks of 256 threads per SM in total (~24 waves at 4 resident blocks per SM:
+  // shorter blocks even out the slow low-frequency tiles; on the 21-layer gather grid
+  // 2.612 ms against 2.633 at 64 and 2.623 at 128; with three resident blocks 2.65 at 64,
+  // 2.73 at 32, 2.85 at 16), but no slice shorter than 64 slownesses.
+  const long long target = 148LL * 96;
   long long s = (target + tiles - 1) / (tiles > 0 ? tiles : 1);
   long long smax = (n_p + 63) / 64;
   if (s > smax) s = smax;
