@@ -182,7 +182,7 @@ __device__ __forceinline__ void fast_tile(const double2* s_pf, const double2* s_
 // one rotation per slowness, with an exact sincos anchor every kRotSteps.  R arrives in
 // tiles through a ring of three buffers (stage_R).  omega is factored out of the weight:
 // U = omega * sum_j J0(x_j) (pw_j dp) R_j.  Four blocks of 256 threads per SM (64 registers,
-// 72 bytes of spills; 128-slowness chunks keep four blocks' shared memory within the SM's
+// 40 bytes of spills; 128-slowness chunks keep four blocks' shared memory within the SM's
 // 228 KB): the kernel is bound by each warp's dependency chains, so more resident warps
 // help despite the spills (21-layer gather grid: 2.98 ms at two blocks and 124 registers,
 // 2.65 at three and 80, 2.635 at four, U bit-identical).
@@ -275,7 +275,9 @@ bessel_partial_kernel(const double2* __restrict__ R, const double* __restrict__ 
           default: fast_tile<7>(s_pf, s_ig, tile, k0, m, lane, om, r, inv_omr, cdl, sd, ax, ay); break;
         }
       } else if (active) {
-#pragma unroll 4
+        // not unrolled: fewer spills at 64 registers, 2.593 vs 2.615 ms (unroll 4) and
+        // 2.723 (unroll 8) on the 21-layer gather grid, U bit-identical
+#pragma unroll 1
         for (int k = 0; k < m; ++k) {
           const double2 pf = s_pf[k0 + k];
           const double2 rv = tile[k][lane];
